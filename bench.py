@@ -1,0 +1,387 @@
+"""BSOF/I benchmark: FP64 inversion of the DQMC block p-cyclic matrix.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (default): one plain-FP64 inversion per step of the Hubbard matrix on
+a 16x16 periodic lattice (n = 256), p = 32 time slices, U = 4, dtau = 0.125
+(N = 8192), seeded synthetic fields.  A step is BSOF + BSTRI + BSOI on one
+matrix already resident in HBM; every step inverts a different 537 MB buffer
+(inputs larger than L2, no reuse between steps).
+
+Multi-GPU: independent replicas (one process per GPU, no collective on the
+data path); value = inversions by all ranks / max-over-ranks device time.
+
+Printed JSON line (rank 0): value (device-resident inversions/s), tflops
+(flop model of include/bsofi_flops.h), roofline of the dominant kernel (the
+BSOI step GEMM, FP64 DMMA, against cuBLAS DGEMM measured in the same run),
+e2e (the reference handle API hybridxbsoftrih_ + hybridxbsoih_ on host
+buffers, copies included), cpu_baseline (the reference's CPU path,
+oracle/_ref, on the host cores), clocks sampled during the timed region.
+
+--impl reference times the reference's own CPU implementation (the compiled
+reference library in oracle/_ref, OpenBLAS with all host threads) on the same
+workload and prints the same JSON line with "impl": "reference".
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from bsofi_b200.flops import bsofi_flops, flops_bsoi  # noqa: E402
+from bsofi_b200.hubbard import hubbard_blocks  # noqa: E402
+
+METRIC = "inversions/s (FP64 BSOF/I, n=256, p=32)"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=30)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--side", type=int, default=16)
+    p.add_argument("--L", type=int, default=32)
+    p.add_argument("--U", type=float, default=4.0)
+    p.add_argument("--e2e-steps", type=int, default=5)
+    p.add_argument("--cpu-sample", type=int, default=2, help="reference inversions in cpu_baseline")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def config(args, n, N):
+    return {"workload": "single FP64 inversion of the Hubbard DQMC p-cyclic matrix, "
+                        "%dx%d lattice, n=%d, p=%d, N=%d, U=%g, dtau=0.125"
+                        % (args.side, args.side, n, args.L, N, args.U),
+            "n": n, "p": args.L, "N": N, "U": args.U,
+            "l2": "inputs larger than L2: %d MB per matrix, a fresh buffer every step"
+                  % (8 * N * N // 2 ** 20),
+            "parallelism": "replicas" if args.gpus > 1 else "single"}
+
+
+def pcyclic_device(torch, diag, sub, ldd, dev):
+    """Column-major (ldd x N) device buffer of the p-cyclic matrix."""
+    L, n, _ = diag.shape
+    N = n * L
+    t = torch.zeros((N, ldd), dtype=torch.float64, device=dev)  # t[col, row]
+    D = torch.from_numpy(diag).to(dev)
+    S = torch.from_numpy(sub).to(dev)
+    for k in range(L):
+        t[k * n:(k + 1) * n, k * n:(k + 1) * n] = D[k].T
+        r = (k + 1) % L
+        t[k * n:(k + 1) * n, r * n:(r + 1) * n] = S[k].T
+    return t
+
+
+def hubbard_pcyclic(side, L, U, seed):
+    B = hubbard_blocks(side, L, U, seed=seed)
+    n = side * side
+    diag = np.broadcast_to(np.eye(n), (L, n, n)).copy()
+    sub = -B
+    sub[L - 1] = B[L - 1]
+    return diag, sub
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def measure_dgemm_peak(torch, dev, size=8192, reps=6):
+    """cuBLAS FP64 GEMM throughput (TFLOP/s), best of `reps` (the FP64
+    denominator; the driver's peak file carries only HBM and BF16 figures)."""
+    a = torch.randn(size, size, dtype=torch.float64, device=dev)
+    b = torch.randn(size, size, dtype=torch.float64, device=dev)
+    c = a @ b
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b, out=c)
+        e1.record()
+        e1.synchronize()
+        best = max(best, 2.0 * size ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b, c
+    return best
+
+
+def traffic_per_launch():
+    """DRAM bytes per BSOI GEMM launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "bsoi_gemm_traffic.json")
+    if os.path.exists(path):
+        try:
+            return json.load(open(path)).get("dram_bytes_per_launch")
+        except ValueError:
+            return None
+    return None
+
+
+def cpu_reference(side, L, U, steps, threads=None):
+    """Time the reference's CPU path (oracle/_ref) on `steps` inversions."""
+    import oracle
+    from bsofi_b200.hubbard import hubbard_matrix
+    if not oracle.ref_available():
+        return None
+    cores = threads or os.cpu_count()
+    oracle.set_ref_threads(cores)
+    n = side * side
+    M = hubbard_matrix(side, L, U, seed=12345)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        A, tau, info = oracle.ref_bsoftri(M, n, L)
+        oracle.ref_bsoi(A, tau, n, L)
+        times.append(time.perf_counter() - t0)
+    return {"times": times, "cores": cores}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    n = args.side * args.side
+    N = n * args.L
+    out = cpu_reference(args.side, args.L, args.U, args.warmup + args.steps)
+    if out is None:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference CPU library oracle/_ref/libbsofi_ref.so not built"}))
+        return
+    t = out["times"][args.warmup:]
+    tot = sum(t)
+    value = len(t) / tot
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "inversions/s",
+            "n_gpus": args.gpus, "steps": len(t), "warmup": args.warmup,
+            "ms_per_step": 1e3 * tot / len(t), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded Hubbard DQMC matrix",
+            "config": config(args, n, N),
+            "tflops": bsofi_flops(n, args.L) * value / 1e12,
+            "cpu_baseline": {"value": value, "unit": "inversions/s", "cores": out["cores"],
+                             "kind": "reference",
+                             "sample": "%d full inversions (lapackXbsof+lapackXbstri+"
+                                       "lapackXbsoi_ormqr, OpenBLAS)" % len(t)},
+            "e2e": {"value": value, "unit": "inversions/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from bsofi_b200 import api
+
+    api.load()  # the CUDA library is the only path; fail loudly if missing
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=dev)
+
+    side, L, U = args.side, args.L, args.U
+    n = side * side
+    N = n * L
+    ldd = (N + 31) // 32 * 32
+    nbuf = args.warmup + args.steps
+    nseeds = 4
+    blocks = [hubbard_pcyclic(side, L, U, seed=1000 * rank + s) for s in range(nseeds)]
+    bufs = [pcyclic_device(torch, *blocks[i % nseeds], ldd, dev) for i in range(nbuf)]
+    dtau = torch.zeros(N, dtype=torch.float64, device=dev)
+    ws = torch.zeros(api.workspace_bytes(n, L, ldd) // 8 + 32, dtype=torch.float64, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    sp = stream.cuda_stream
+
+    def step(i):
+        rc = api.device_invert(n, L, bufs[i].data_ptr(), ldd, dtau.data_ptr(), ws.data_ptr(), sp)
+        if rc != 0:
+            raise RuntimeError("bsofi_device_invert failed: %d" % rc)
+
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup):
+            step(i)
+    torch.cuda.synchronize()
+    launches_per_step = api.last_launches()
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    api.timing(True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for i in range(args.warmup, nbuf):
+            step(i)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    gemm_ms, gemm_launches = api.timing_read()
+    api.timing(False)
+    clk = clocks.stop()
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * args.steps / (ms_max * 1e-3)
+
+    # Check the last output: ||M X - I||_F / ||X||_F on the device.
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from gpu_util import block_residual_gpu
+    Xlast = bufs[nbuf - 1][:, :N].T  # row-major view of the column-major result
+    resid = block_residual_gpu(torch, *blocks[(nbuf - 1) % nseeds], Xlast.contiguous())
+    del bufs
+    torch.cuda.empty_cache()
+
+    peak = measure_dgemm_peak(torch, dev)
+    achieved = flops_bsoi(n, L) * args.steps / (gemm_ms * 1e-3) / 1e12 if gemm_ms > 0 else None
+    roofline = {"kernel": "BSOI step GEMM (gemm_kernel, FP64 DMMA m16n8k4)",
+                "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": (achieved / peak) if achieved else None,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor)",
+                "launches": gemm_launches,
+                "avg_launch_ms": gemm_ms / max(gemm_launches, 1),
+                "algorithmic_flops_per_launch": flops_bsoi(n, L) / (L - 1),
+                "traffic": traffic_per_launch()}
+
+    e2e = None
+    if not args.no_e2e and args.e2e_steps > 0:
+        e2e = run_e2e(api, torch, dist, world, side, L, U, rank, args.e2e_steps)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu and args.cpu_sample > 0:
+        out = cpu_reference(side, L, U, args.cpu_sample)
+        if out is not None:
+            cpu = {"value": len(out["times"]) / sum(out["times"]), "unit": "inversions/s",
+                   "cores": out["cores"], "kind": "reference",
+                   "sample": "%d inversions of the same workload through oracle/_ref "
+                             "(reference CPU path, OpenBLAS, %d threads)"
+                             % (len(out["times"]), out["cores"])}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "inversions/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64",
+                "data": "synthetic: seeded Hubbard DQMC matrices (random +-1 fields)",
+                "config": config(args, n, N),
+                "tflops": bsofi_flops(n, L) * value / world / 1e12,
+                "residual": resid,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": launches_per_step * args.steps,
+                "clocks": clk}
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_e2e(api, torch, dist, world, side, L, U, rank, steps):
+    """The reference-facing handle API on host buffers: hybridxbsoftrih_ +
+    hybridxbsoih_ per step, every copy between host and device included."""
+    from bsofi_b200.hubbard import hubbard_matrix
+    n = side * side
+    N = n * L
+    M = hubbard_matrix(side, L, U, seed=777 + rank)
+    A = np.empty_like(M, order="F")
+    tau = np.zeros(N)
+    h = api.Handle(n, L)
+    times = []
+    for i in range(steps + 1):
+        np.copyto(A, M)
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        info = h.bsoftri(A, tau)
+        info2 = h.bsoi(A, tau)
+        dt = time.perf_counter() - t0
+        if info or info2:
+            raise RuntimeError("handle API info %d %d" % (info, info2))
+        if i > 0:
+            times.append(dt)
+    h.close()
+    tot = sum(times)
+    t = torch.tensor([tot], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    tot = float(t.item())
+    state_bytes = sum(min(N, (k + 2) * n) * n for k in range(L)) * 8
+    h2d = 2 * L * n * n * 8 + state_bytes + N * 8
+    d2h = state_bytes + N * 8 + N * N * 8
+    return {"value": world * len(times) / tot, "unit": "inversions/s",
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "api": "hybridxbsoftrih_ + hybridxbsoih_ (host pageable buffers)",
+            "steps": len(times)}
+
+
+if __name__ == "__main__":
+    main()

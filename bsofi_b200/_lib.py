@@ -1,0 +1,92 @@
+"""ctypes binding of libbsofi_b200.so (the C ABI in include/bsofi_b200.h).
+
+The library is the product: there is no Python or CPU fallback.  Loading fails
+loudly when the shared library has not been built.
+"""
+import ctypes
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbsofi_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "bsofi_b200.h")
+
+_c_int_p = ctypes.POINTER(ctypes.c_int)
+_c_dbl_p = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+
+# (restype, argtypes) per exported symbol.
+_SIGS = {
+    "hybridxinith_": (ctypes.c_int, [_c_int_p, _c_int_p, _c_int_p, _c_int_p]),
+    "hybridxbsofilworkh_": (ctypes.c_int, [_c_int_p, _c_int_p, _c_int_p, _c_int_p]),
+    "hybridxbsoftrih_": (ctypes.c_int, [_c_int_p, _c_int_p, _c_int_p, _c_dbl_p, _c_int_p,
+                                        _c_dbl_p, _c_dbl_p, _c_int_p, _c_int_p]),
+    "hybridxbsoih_": (ctypes.c_int, [_c_int_p, _c_int_p, _c_int_p, _c_dbl_p, _c_int_p,
+                                     _c_dbl_p, _c_dbl_p, _c_int_p, _c_int_p]),
+    "hybridxfinalizeh_": (ctypes.c_int, [_c_int_p]),
+    "fgetwalltime_": (None, [_c_dbl_p]),
+    "felapsed_": (ctypes.c_double, [_c_dbl_p, _c_dbl_p]),
+    "lapackXbsofiLWork": (ctypes.c_int, [ctypes.c_int] * 3),
+    "lapackXbsof": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _c_dbl_p, ctypes.c_int, _c_dbl_p,
+                                   _c_dbl_p, ctypes.c_int, _c_int_p]),
+    "lapackXbstri": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _c_dbl_p, ctypes.c_int, _c_int_p]),
+    "lapackXbsoi_ormqr": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _c_dbl_p, ctypes.c_int,
+                                         _c_dbl_p, _c_dbl_p, ctypes.c_int, _c_int_p]),
+    "lapackXbsoi_orgqr": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _c_dbl_p, ctypes.c_int,
+                                         _c_dbl_p, _c_dbl_p, ctypes.c_int, _c_int_p]),
+    "hybridXbsofiLWork": (ctypes.c_int, [ctypes.c_int] * 4),
+    "hybridXbsoftri": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _c_dbl_p,
+                                      ctypes.c_int, _c_dbl_p, _c_dbl_p, ctypes.c_int, _c_dbl_p,
+                                      ctypes.c_int, _c_int_p]),
+    "hybridXbsoi": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _c_dbl_p,
+                                   ctypes.c_int, _c_dbl_p, _c_dbl_p, ctypes.c_int, _c_dbl_p,
+                                   ctypes.c_int, _c_int_p]),
+    "gpuXbsof": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _c_dbl_p,
+                                _c_dbl_p, ctypes.c_int, _vp, _c_int_p]),
+    "gpuXbstri_rseq": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp,
+                                      ctypes.c_int, _c_int_p]),
+    "gpuXbsoi_batched": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _c_dbl_p,
+                                        _c_dbl_p, ctypes.c_int, _vp, _vp, ctypes.c_int,
+                                        _c_int_p]),
+    "bsofi_device_workspace_bytes": (ctypes.c_ulonglong, [ctypes.c_int] * 3),
+    "bsofi_device_invert": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp,
+                                           _vp, _vp]),
+    "bsofi_device_bsoftri": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp,
+                                            _vp, _vp]),
+    "bsofi_device_bsoi": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp,
+                                         _vp, _vp]),
+    "bsofi_device_info": (_vp, [_vp]),
+    "bsofi_device_last_launches": (ctypes.c_longlong, []),
+    "bsofi_device_timing": (None, [ctypes.c_int]),
+    "bsofi_device_timing_read": (ctypes.c_int, [_c_dbl_p, ctypes.POINTER(ctypes.c_longlong)]),
+    "bsofi_selftest_gemm": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_double, _vp, ctypes.c_int, ctypes.c_int,
+                                           _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                           _vp, ctypes.c_int, ctypes.c_int, _vp]),
+}
+
+_lib = None
+
+
+def declared_symbols(header=HEADER):
+    """Function names declared in include/bsofi_b200.h."""
+    text = open(header).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:unsigned\s+long\s+long|long\s+long|int\s*\*?|double|void)\s+\*?\s*(\w+)\s*\(",
+                                 text, flags=re.M)))
+
+
+def load():
+    """Load the library (once).  Raises if it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libbsofi_b200.so is not built (python -m bsofi_b200.build); "
+                               "the BSOF/I path has no fallback")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+    return _lib

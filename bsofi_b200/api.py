@@ -1,0 +1,149 @@
+"""Python view of the BSOF/I C ABI (numpy host buffers and raw device pointers).
+
+Every function calls libbsofi_b200.so; the numerical work runs in the sm_100a
+kernels.  Host matrices are column-major float64 (numpy Fortran order).
+"""
+import ctypes
+
+import numpy as np
+
+from ._lib import load
+
+INFO_CUDA = -1000
+_ip = ctypes.POINTER(ctypes.c_int)
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def _iref(v):
+    return ctypes.byref(ctypes.c_int(int(v)))
+
+
+def _dptr(a):
+    return a.ctypes.data_as(_dp)
+
+
+class Handle:
+    """The reference's integer handler(10) managed by hybridxinith_ /
+    hybridxfinalizeh_ (src/bsofi_callback.c:101-168)."""
+
+    def __init__(self, n, L, lda=None):
+        self.n, self.L = int(n), int(L)
+        self.lda = int(lda) if lda is not None else self.n * self.L
+        self.words = np.zeros(10, dtype=np.int32)
+        rc = load().hybridxinith_(self.words.ctypes.data_as(_ip), _iref(self.n), _iref(self.L),
+                                  _iref(self.lda))
+        if rc != 0:
+            raise RuntimeError("hybridxinith_ failed (%d)" % rc)
+
+    @property
+    def ptr(self):
+        return self.words.ctypes.data_as(_ip)
+
+    def lwork(self):
+        return load().hybridxbsofilworkh_(self.ptr, _iref(self.n), _iref(self.L), _iref(self.lda))
+
+    def bsoftri(self, A, tau, work=None, lwork=None):
+        """hybridxbsoftrih_ in place on A (Fortran-ordered float64); returns info."""
+        _check_host(A, self.lda)
+        if work is None:
+            work = np.zeros(max(1, self.lwork()))
+        lw = len(work) if lwork is None else lwork
+        info = ctypes.c_int(0)
+        load().hybridxbsoftrih_(self.ptr, _iref(self.n), _iref(self.L), _dptr(A), _iref(self.lda),
+                                _dptr(tau), _dptr(work), _iref(lw), ctypes.byref(info))
+        return info.value
+
+    def bsoi(self, A, tau, work=None, lwork=None):
+        _check_host(A, self.lda)
+        if work is None:
+            work = np.zeros(max(1, self.lwork()))
+        lw = len(work) if lwork is None else lwork
+        info = ctypes.c_int(0)
+        load().hybridxbsoih_(self.ptr, _iref(self.n), _iref(self.L), _dptr(A), _iref(self.lda),
+                             _dptr(tau), _dptr(work), _iref(lw), ctypes.byref(info))
+        return info.value
+
+    def close(self):
+        if self.words is not None:
+            load().hybridxfinalizeh_(self.ptr)
+            self.words = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _check_host(A, lda):
+    if not (isinstance(A, np.ndarray) and A.dtype == np.float64 and A.flags.f_contiguous):
+        raise TypeError("A must be a Fortran-ordered float64 numpy array")
+    if A.shape[0] != lda:
+        raise ValueError("A.shape[0] must equal lda")
+
+
+def invert(M, n, L):
+    """M^{-1} through the handle API (XbsoftriH + XbsoiH).  Returns
+    (X, A_after_bsoftri, tau, info)."""
+    A = np.asfortranarray(np.array(M, dtype=np.float64, copy=True))
+    tau = np.zeros(n * L)
+    with Handle(n, L) as h:
+        info = h.bsoftri(A, tau)
+        state = A.copy(order="F")
+        if info != 0:
+            return None, state, tau, info
+        info = h.bsoi(A, tau)
+    return A, state, tau, info
+
+
+# ------------------------------------------------------------ device API
+def workspace_bytes(n, L, ldda):
+    return int(load().bsofi_device_workspace_bytes(n, L, ldda))
+
+
+def device_invert(n, L, dA, ldda, dtau, dwork, stream=0):
+    """bsofi_device_invert on raw device pointers (ints); asynchronous."""
+    return load().bsofi_device_invert(n, L, dA, ldda, dtau, dwork, stream)
+
+
+def device_bsoftri(n, L, dA, ldda, dtau, dwork, stream=0):
+    return load().bsofi_device_bsoftri(n, L, dA, ldda, dtau, dwork, stream)
+
+
+def device_bsoi(n, L, dA, ldda, dtau, dwork, stream=0):
+    return load().bsofi_device_bsoi(n, L, dA, ldda, dtau, dwork, stream)
+
+
+def device_info_ptr(dwork):
+    return load().bsofi_device_info(dwork)
+
+
+def last_launches():
+    return int(load().bsofi_device_last_launches())
+
+
+def selftest_gemm(M, N, K, alpha, dA, lda, upper_a, dB, ldb, upper_b, beta, dC, ldc, tile=0,
+                  stream=0):
+    return load().bsofi_selftest_gemm(M, N, K, alpha, dA, lda, int(upper_a), dB, ldb,
+                                      int(upper_b), beta, dC, ldc, tile, stream)
+
+
+def timing(on):
+    """Bracket every BSOI step GEMM launch with CUDA events (diagnostics)."""
+    load().bsofi_device_timing(1 if on else 0)
+
+
+def timing_read():
+    """(summed BSOI GEMM time in ms, number of timed launches); clears the record."""
+    ms = ctypes.c_double(0.0)
+    cnt = ctypes.c_longlong(0)
+    rc = load().bsofi_device_timing_read(ctypes.byref(ms), ctypes.byref(cnt))
+    if rc != 0:
+        raise RuntimeError("bsofi_device_timing_read failed (%d)" % rc)
+    return ms.value, cnt.value

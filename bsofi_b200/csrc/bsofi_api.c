@@ -1,0 +1,569 @@
+/*
+ * bsofi_api.c -- host C layer of libbsofi_b200.so: the reference's handle
+ * API, C names and Fortran bindings over the device pipeline.
+ *
+ * Reference interface: src/bsofi_callback.c:1-220 (handle API and timers),
+ * include/bsofi_cpu.h, include/bsofi_hybrid.h, include/bsofi_gpu.h.
+ * Unlike the reference there is no host/device switch (KAPPA split) and no
+ * LAPACK fallback: every call runs the sm_100a kernels.  Host <-> device
+ * traffic per call is what the storage contract needs:
+ *   XbsoftriH  H2D the 2L p-cyclic blocks, D2H the block upper triangle plus
+ *              the reflector blocks, D2H tau;
+ *   XbsoiH     H2D that same region and tau, D2H the dense M^{-1}.
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/time.h>
+#include <cuda_runtime_api.h>
+
+#include "../../include/bsofi_b200.h"
+#include "bsofi_device.h"
+
+#define HANDLE_MAGIC 0x49465342u /* "BSFI" */
+#define HANDLE_VERSION 1u
+#define CTX_MAGIC 0x58544342u
+
+typedef struct bsofi_ctx {
+  uint32_t magic;
+  int device;
+  int n, L, ldd;
+  cudaStream_t stream;
+  double *dA;
+  double *dtau;
+  void *dws;
+  size_t ws_bytes;
+} bsofi_ctx;
+
+/* Layout of the caller's integer handler(10) (40 bytes). */
+typedef struct bsofi_handle {
+  uint32_t magic;
+  uint32_t version;
+  uint64_t ctx;
+  int32_t n, L, lda;
+  int32_t reserved[3];
+} bsofi_handle;
+
+typedef char handle_fits_in_40_bytes[(sizeof(bsofi_handle) <= 40) ? 1 : -1];
+
+static int cuda_info(cudaError_t e) { return BSOFI_INFO_CUDA - (int)e; }
+
+static int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+static void ctx_free_buffers(bsofi_ctx *c) {
+  if (c->dA) cudaFree(c->dA);
+  if (c->dtau) cudaFree(c->dtau);
+  if (c->dws) cudaFree(c->dws);
+  c->dA = NULL;
+  c->dtau = NULL;
+  c->dws = NULL;
+  c->n = c->L = c->ldd = 0;
+}
+
+/* Make the context's buffers fit (n, L).  Returns cudaError_t. */
+static cudaError_t ctx_fit(bsofi_ctx *c, int n, int L) {
+  cudaError_t e;
+  int N = n * L, ldd;
+  if (c->dA && c->n == n && c->L == L) return cudaSuccess;
+  ctx_free_buffers(c);
+  ldd = round_up(N, 32);
+  if ((e = cudaMalloc((void **)&c->dA, sizeof(double) * (size_t)ldd * N)) != cudaSuccess) goto fail;
+  if ((e = cudaMalloc((void **)&c->dtau, sizeof(double) * (size_t)N)) != cudaSuccess) goto fail;
+  c->ws_bytes = bsofi_dev_ws_bytes(n, L, ldd);
+  if ((e = cudaMalloc(&c->dws, c->ws_bytes)) != cudaSuccess) goto fail;
+  c->n = n;
+  c->L = L;
+  c->ldd = ldd;
+  return cudaSuccess;
+fail:
+  ctx_free_buffers(c);
+  cudaGetLastError();
+  return e;
+}
+
+static bsofi_ctx *ctx_create(int n, int L, cudaError_t *err) {
+  cudaError_t e;
+  bsofi_ctx *c = (bsofi_ctx *)calloc(1, sizeof(bsofi_ctx));
+  if (!c) {
+    *err = cudaErrorMemoryAllocation;
+    return NULL;
+  }
+  c->magic = CTX_MAGIC;
+  if ((e = cudaGetDevice(&c->device)) != cudaSuccess ||
+      (e = (cudaError_t)bsofi_dev_prepare()) != cudaSuccess ||
+      (e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+    free(c);
+    *err = e;
+    return NULL;
+  }
+  if ((e = ctx_fit(c, n, L)) != cudaSuccess) {
+    cudaStreamDestroy(c->stream);
+    free(c);
+    *err = e;
+    return NULL;
+  }
+  *err = cudaSuccess;
+  return c;
+}
+
+static void ctx_destroy(bsofi_ctx *c) {
+  if (!c) return;
+  ctx_free_buffers(c);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  c->magic = 0;
+  free(c);
+}
+
+static bsofi_ctx *handle_ctx(const int *h) {
+  bsofi_handle hd;
+  bsofi_ctx *c;
+  if (!h) return NULL;
+  memcpy(&hd, h, sizeof(hd));
+  if (hd.magic != HANDLE_MAGIC || hd.version != HANDLE_VERSION) return NULL;
+  c = (bsofi_ctx *)(uintptr_t)hd.ctx;
+  if (!c || c->magic != CTX_MAGIC) return NULL;
+  return c;
+}
+
+/* ---------------------------------------------------------------- copies */
+/* H2D of the p-cyclic blocks of the host matrix (every other block zero). */
+static cudaError_t upload_pcyclic(bsofi_ctx *c, const double *A, int lda) {
+  int n = c->n, L = c->L, k;
+  size_t es = sizeof(double);
+  cudaError_t e = (cudaError_t)bsofi_dev_zero_structural(n, L, c->dA, c->ldd, c->stream);
+  if (e != cudaSuccess) return e;
+  for (k = 0; k < L - 1; k++) { /* diagonal + sub-diagonal block of column block k */
+    size_t off_h = (size_t)k * n * lda + (size_t)k * n;
+    size_t off_d = (size_t)k * n * c->ldd + (size_t)k * n;
+    e = cudaMemcpy2DAsync(c->dA + off_d, es * c->ldd, A + off_h, es * lda, es * 2 * n, n,
+                          cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return e;
+  }
+  /* last column block: corner (0, L-1) and diagonal (L-1, L-1) */
+  {
+    size_t col_h = (size_t)(L - 1) * n * lda, col_d = (size_t)(L - 1) * n * c->ldd;
+    e = cudaMemcpy2DAsync(c->dA + col_d, es * c->ldd, A + col_h, es * lda, es * n, n,
+                          cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpy2DAsync(c->dA + col_d + (size_t)(L - 1) * n, es * c->ldd,
+                          A + col_h + (size_t)(L - 1) * n, es * lda, es * n, n,
+                          cudaMemcpyHostToDevice, c->stream);
+  }
+  return e;
+}
+
+/* The BSOFTRI state: rows 0 .. min(N, (k+2)n) of every column block k. */
+static cudaError_t copy_state(bsofi_ctx *c, double *A, int lda, int to_host) {
+  int n = c->n, L = c->L, N = n * L, k;
+  size_t es = sizeof(double);
+  cudaError_t e = cudaSuccess;
+  for (k = 0; k < L; k++) {
+    int rows = (k + 2) * n < N ? (k + 2) * n : N;
+    double *h = A + (size_t)k * n * lda;
+    double *d = c->dA + (size_t)k * n * c->ldd;
+    if (to_host)
+      e = cudaMemcpy2DAsync(h, es * lda, d, es * c->ldd, es * rows, n, cudaMemcpyDeviceToHost,
+                            c->stream);
+    else
+      e = cudaMemcpy2DAsync(d, es * c->ldd, h, es * lda, es * rows, n, cudaMemcpyHostToDevice,
+                            c->stream);
+    if (e != cudaSuccess) return e;
+  }
+  return e;
+}
+
+/* ---------------------------------------------------------------- checks */
+static int check_args(const int *h_ok, int n, int L, const double *A, int lda,
+                      const double *tau, const double *work, int lwork, int first_arg) {
+  /* first_arg: position of n in the argument list (2 with a handle). */
+  if (h_ok && !*h_ok) return -1;
+  if (n < 1 || n > BSOFI_MAX_BLOCK) return -(first_arg);
+  if (L < 2 || (long long)n * L > 1000000) return -(first_arg + 1);
+  if (!A) return -(first_arg + 2);
+  if (lda < n * L) return -(first_arg + 3);
+  if (!tau) return -(first_arg + 4);
+  if ((lwork == -1 || lwork == -2) && !work) return -(first_arg + 5);
+  if (lwork < 1 && lwork != -1 && lwork != -2) return -(first_arg + 6);
+  return 0;
+}
+
+static int read_info(bsofi_ctx *c, int *info) {
+  int v = 0;
+  cudaError_t e = cudaMemcpyAsync(&v, bsofi_dev_info_ptr(c->dws), sizeof(int),
+                                  cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) {
+    *info = cuda_info(e);
+    return *info;
+  }
+  *info = (v >= 0x7f7f7f7f || v < 0) ? 0 : v;
+  return *info;
+}
+
+/* ------------------------------------------------------- phase drivers */
+/* BSOF (+ BSTRI when do_tri) on host A; returns info. */
+static int drive_bsoftri(bsofi_ctx *c, int n, int L, double *A, int lda, double *tau,
+                         int do_bsof, int do_tri) {
+  cudaError_t e;
+  int info = 0, N = n * L;
+  if ((e = ctx_fit(c, n, L)) != cudaSuccess) return cuda_info(e);
+  if (do_bsof) {
+    if ((e = upload_pcyclic(c, A, lda)) != cudaSuccess) return cuda_info(e);
+  } else {
+    if ((e = copy_state(c, A, lda, 0)) != cudaSuccess) return cuda_info(e);
+  }
+  if (do_bsof && do_tri)
+    e = (cudaError_t)bsofi_dev_bsoftri(n, L, c->dA, c->ldd, c->dtau, c->dws, c->stream);
+  else if (do_bsof)
+    e = (cudaError_t)bsofi_dev_bsof(n, L, c->dA, c->ldd, c->dtau, c->dws, c->stream);
+  else
+    e = (cudaError_t)bsofi_dev_bstri(n, L, c->dA, c->ldd, c->dws, c->stream);
+  if (e != cudaSuccess) return cuda_info(e);
+  if ((e = copy_state(c, A, lda, 1)) != cudaSuccess) return cuda_info(e);
+  if (do_bsof) {
+    e = cudaMemcpyAsync(tau, c->dtau, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream);
+    if (e != cudaSuccess) return cuda_info(e);
+  }
+  if (do_tri) return read_info(c, &info);
+  e = cudaStreamSynchronize(c->stream);
+  return e == cudaSuccess ? 0 : cuda_info(e);
+}
+
+static int drive_bsoi(bsofi_ctx *c, int n, int L, double *A, int lda, const double *tau) {
+  cudaError_t e;
+  int N = n * L;
+  if ((e = ctx_fit(c, n, L)) != cudaSuccess) return cuda_info(e);
+  if ((e = copy_state(c, A, lda, 0)) != cudaSuccess) return cuda_info(e);
+  e = cudaMemcpyAsync(c->dtau, tau, sizeof(double) * N, cudaMemcpyHostToDevice, c->stream);
+  if (e != cudaSuccess) return cuda_info(e);
+  e = (cudaError_t)bsofi_dev_bsoi(n, L, c->dA, c->ldd, c->dtau, c->dws, c->stream);
+  if (e != cudaSuccess) return cuda_info(e);
+  e = cudaMemcpy2DAsync(A, sizeof(double) * lda, c->dA, sizeof(double) * c->ldd,
+                        sizeof(double) * N, N, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  return e == cudaSuccess ? 0 : cuda_info(e);
+}
+
+/* ================================================================ handle API */
+int hybridxinith_(int *handle, int *n, int *L, int *lda) {
+  bsofi_handle hd;
+  bsofi_ctx *c;
+  cudaError_t e;
+  if (!handle || !n || !L || !lda) return -1;
+  if (*n < 1 || *n > BSOFI_MAX_BLOCK || *L < 2 || *lda < (*n) * (*L)) return -1;
+  c = ctx_create(*n, *L, &e);
+  if (!c) return -1;
+  memset(&hd, 0, sizeof(hd));
+  hd.magic = HANDLE_MAGIC;
+  hd.version = HANDLE_VERSION;
+  hd.ctx = (uint64_t)(uintptr_t)c;
+  hd.n = *n;
+  hd.L = *L;
+  hd.lda = *lda;
+  memcpy(handle, &hd, sizeof(hd));
+  return 0;
+}
+
+int hybridxbsofilworkh_(int *handle, int *n, int *L, int *lda) {
+  (void)handle;
+  (void)n;
+  (void)L;
+  (void)lda;
+  return 1;
+}
+
+int hybridxbsoftrih_(int *handle, int *n, int *L, double *A, int *lda, double *tau,
+                     double *work, int *lwork, int *info) {
+  bsofi_ctx *c = handle_ctx(handle);
+  int ok = c != NULL, r;
+  if (!info) return -9;
+  if (!n || !L || !lda || !lwork) {
+    *info = !n ? -2 : !L ? -3 : !lda ? -5 : -8;
+    return *info;
+  }
+  r = check_args(&ok, *n, *L, A, *lda, tau, work, *lwork, 2);
+  if (r) return *info = r;
+  if (*lwork == -1) {
+    work[0] = 1.0;
+    return *info = 0;
+  }
+  if (*lwork == -2) {
+    int ldd = round_up((*n) * (*L), 32), N = (*n) * (*L);
+    work[0] = (double)((size_t)ldd * N + N + bsofi_dev_ws_bytes(*n, *L, ldd) / sizeof(double));
+    return *info = 0;
+  }
+  return *info = drive_bsoftri(c, *n, *L, A, *lda, tau, 1, 1);
+}
+
+int hybridxbsoih_(int *handle, int *n, int *L, double *A, int *lda, double *tau, double *work,
+                  int *lwork, int *info) {
+  bsofi_ctx *c = handle_ctx(handle);
+  int ok = c != NULL, r;
+  if (!info) return -9;
+  if (!n || !L || !lda || !lwork) {
+    *info = !n ? -2 : !L ? -3 : !lda ? -5 : -8;
+    return *info;
+  }
+  r = check_args(&ok, *n, *L, A, *lda, tau, work, *lwork, 2);
+  if (r) return *info = r;
+  if (*lwork == -1) {
+    work[0] = 1.0;
+    return *info = 0;
+  }
+  if (*lwork == -2) {
+    int ldd = round_up((*n) * (*L), 32), N = (*n) * (*L);
+    work[0] = (double)((size_t)ldd * N + N + bsofi_dev_ws_bytes(*n, *L, ldd) / sizeof(double));
+    return *info = 0;
+  }
+  return *info = drive_bsoi(c, *n, *L, A, *lda, tau);
+}
+
+int hybridxfinalizeh_(int *handle) {
+  bsofi_ctx *c = handle_ctx(handle);
+  if (c) ctx_destroy(c);
+  if (handle) memset(handle, 0, sizeof(bsofi_handle));
+  return 0;
+}
+
+void fgetwalltime_(double tv[2]) {
+  struct timeval t;
+  gettimeofday(&t, NULL);
+  tv[0] = (double)t.tv_sec;
+  tv[1] = (double)t.tv_usec;
+}
+
+double felapsed_(double t1[2], double t0[2]) {
+  return (t1[0] - t0[0]) + (t1[1] - t0[1]) / 1000000.0;
+}
+
+/* ================================================================ C names */
+static __thread bsofi_ctx *t_ctx = NULL;
+
+static bsofi_ctx *thread_ctx(int n, int L, int *info) {
+  cudaError_t e;
+  if (t_ctx) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) == cudaSuccess && dev == t_ctx->device) return t_ctx;
+    ctx_destroy(t_ctx);
+    t_ctx = NULL;
+  }
+  t_ctx = ctx_create(n, L, &e);
+  if (!t_ctx) *info = cuda_info(e);
+  return t_ctx;
+}
+
+int lapackXbsofiLWork(int n, int L, int lda) {
+  (void)n;
+  (void)L;
+  (void)lda;
+  return 1;
+}
+
+int hybridXbsofiLWork(int n, int L, int lda, int lworkHostDevice) {
+  (void)lda;
+  if (lworkHostDevice == -2) {
+    int ldd = round_up(n * L, 32), N = n * L;
+    return (int)((size_t)ldd * N + N + bsofi_dev_ws_bytes(n, L, ldd) / sizeof(double));
+  }
+  return 1;
+}
+
+static int c_phase(int n, int L, double *A, int lda, double *tau, double *work, int lwork,
+                   int *info, int phase) {
+  int r, tmp = 0;
+  bsofi_ctx *c;
+  if (!info) info = &tmp;
+  r = check_args(NULL, n, L, A, lda, phase == 1 ? A : tau, work, lwork, 1);
+  if (r) return *info = r;
+  if (lwork == -1 || lwork == -2) {
+    work[0] = lwork == -1 ? 1.0 : (double)hybridXbsofiLWork(n, L, lda, -2);
+    return *info = 0;
+  }
+  c = thread_ctx(n, L, info);
+  if (!c) return *info;
+  if (phase == 0) return *info = drive_bsoftri(c, n, L, A, lda, tau, 1, 0);
+  if (phase == 1) return *info = drive_bsoftri(c, n, L, A, lda, tau, 0, 1);
+  if (phase == 2) return *info = drive_bsoftri(c, n, L, A, lda, tau, 1, 1);
+  return *info = drive_bsoi(c, n, L, A, lda, tau);
+}
+
+int lapackXbsof(int n, int L, double A[], int lda, double tau[], double work[], int lwork,
+                int *info) {
+  return c_phase(n, L, A, lda, tau, work, lwork, info, 0);
+}
+
+int lapackXbstri(int n, int L, double A[], int lda, int *info) {
+  double w = 0.0;
+  return c_phase(n, L, A, lda, NULL, &w, 1, info, 1);
+}
+
+int lapackXbsoi_ormqr(int n, int L, double A[], int lda, double tau[], double work[], int lwork,
+                      int *info) {
+  return c_phase(n, L, A, lda, tau, work, lwork, info, 3);
+}
+
+int lapackXbsoi_orgqr(int n, int L, double A[], int lda, double tau[], double work[], int lwork,
+                      int *info) {
+  return c_phase(n, L, A, lda, tau, work, lwork, info, 3);
+}
+
+int lapackxbsofilwork_(int *n, int *L, int *lda) { return lapackXbsofiLWork(*n, *L, *lda); }
+int lapackxbsof_(int *n, int *L, double A[], int *lda, double tau[], double work[], int *lwork,
+                 int *info) {
+  return lapackXbsof(*n, *L, A, *lda, tau, work, *lwork, info);
+}
+int lapackxbstri_(int *n, int *L, double A[], int *lda, int *info) {
+  return lapackXbstri(*n, *L, A, *lda, info);
+}
+int lapackxbsoi_ormqr_(int *n, int *L, double A[], int *lda, double tau[], double work[],
+                       int *lwork, int *info) {
+  return lapackXbsoi_ormqr(*n, *L, A, *lda, tau, work, *lwork, info);
+}
+int lapackxbsoi_orgqr_(int *n, int *L, double A[], int *lda, double tau[], double work[],
+                       int *lwork, int *info) {
+  return lapackXbsoi_orgqr(*n, *L, A, *lda, tau, work, *lwork, info);
+}
+
+int hybridXbsoftri(int handle, int n, int L, double A[], int lda, double tau[], double work[],
+                   int lwork, double dwork[], int ldwork, int *info) {
+  (void)handle;
+  (void)dwork;
+  (void)ldwork;
+  return c_phase(n, L, A, lda, tau, work, lwork, info, 2);
+}
+
+int hybridXbsoi(int handle, int n, int L, double A[], int lda, double tau[], double work[],
+                int lwork, double dwork[], int ldwork, int *info) {
+  (void)handle;
+  (void)dwork;
+  (void)ldwork;
+  return c_phase(n, L, A, lda, tau, work, lwork, info, 3);
+}
+
+/* ------------------------------------------------------ device-pointer API */
+static int gpu_phase(int n, int L, double *dA, int ldda, double *tau, int *info, int phase) {
+  int tmp = 0, N = n * L;
+  bsofi_ctx *c;
+  cudaError_t e;
+  if (!info) info = &tmp;
+  if (n < 1 || n > BSOFI_MAX_BLOCK) return *info = -1;
+  if (L < 2) return *info = -2;
+  if (!dA) return *info = -3;
+  if (ldda < N) return *info = -4;
+  if (phase != 1 && !tau) return *info = -5;
+  c = thread_ctx(n, L, info);
+  if (!c) return *info;
+  if ((e = ctx_fit(c, n, L)) != cudaSuccess) return *info = cuda_info(e);
+  if (phase == 0) {
+    e = (cudaError_t)bsofi_dev_bsof(n, L, dA, ldda, c->dtau, c->dws, c->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(tau, c->dtau, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream);
+  } else if (phase == 1) {
+    e = (cudaError_t)bsofi_dev_bstri(n, L, dA, ldda, c->dws, c->stream);
+    if (e == cudaSuccess) return read_info(c, info);
+  } else {
+    e = cudaMemcpyAsync(c->dtau, tau, sizeof(double) * N, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess)
+      e = (cudaError_t)bsofi_dev_bsoi(n, L, dA, ldda, c->dtau, c->dws, c->stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  return *info = (e == cudaSuccess ? 0 : cuda_info(e));
+}
+
+int gpuXbsof(int n, int L, double dA[], int ldda, double tau[], double work[], int lwork,
+             double *dT, int *info) {
+  (void)dT;
+  if (lwork == -1 || lwork == -2) {
+    if (!work) return info ? (*info = -6) : -6;
+    work[0] = lwork == -1 ? 1.0 : (double)bsofi_dev_ws_bytes(n, L, ldda) / sizeof(double);
+    return info ? (*info = 0) : 0;
+  }
+  return gpu_phase(n, L, dA, ldda, tau, info, 0);
+}
+
+int gpuXbstri_rseq(int n, int L, double dA[], int ldda, double dwork[], int ldwork, int *info) {
+  (void)dwork;
+  (void)ldwork;
+  return gpu_phase(n, L, dA, ldda, NULL, info, 1);
+}
+
+int gpuXbstri_rbatched(int n, int L, double dA[], int ldda, double dwork[], int ldwork,
+                       int *info) {
+  return gpuXbstri_rseq(n, L, dA, ldda, dwork, ldwork, info);
+}
+
+int gpuXbsoi_ormqr(int n, int L, double dA[], int ldda, double tau[], double work[], int lwork,
+                   double *dT, double dwork[], int ldwork, int *info) {
+  (void)dT;
+  (void)dwork;
+  (void)ldwork;
+  if (lwork == -1 || lwork == -2) {
+    if (!work) return info ? (*info = -6) : -6;
+    work[0] = lwork == -1 ? 1.0 : (double)bsofi_dev_ws_bytes(n, L, ldda) / sizeof(double);
+    return info ? (*info = 0) : 0;
+  }
+  return gpu_phase(n, L, dA, ldda, tau, info, 2);
+}
+
+int gpuXbsoi_orgqr(int n, int L, double dA[], int ldda, double tau[], double work[], int lwork,
+                   double *dT, double dwork[], int ldwork, int *info) {
+  return gpuXbsoi_ormqr(n, L, dA, ldda, tau, work, lwork, dT, dwork, ldwork, info);
+}
+
+int gpuXbsoi_batched(int n, int L, double dA[], int ldda, double tau[], double work[],
+                     int lwork, double *dT, double dwork[], int ldwork, int *info) {
+  return gpuXbsoi_ormqr(n, L, dA, ldda, tau, work, lwork, dT, dwork, ldwork, info);
+}
+
+/* ------------------------------------------------------ async device API */
+unsigned long long bsofi_device_workspace_bytes(int n, int L, int ldda) {
+  return (unsigned long long)bsofi_dev_ws_bytes(n, L, ldda);
+}
+
+int bsofi_device_bsoftri(int n, int L, double *dA, int ldda, double *dtau, void *dwork,
+                         void *stream) {
+  int e = bsofi_dev_prepare();
+  if (e) return cuda_info((cudaError_t)e);
+  e = bsofi_dev_bsoftri(n, L, dA, ldda, dtau, dwork, stream);
+  return e ? cuda_info((cudaError_t)e) : 0;
+}
+
+int bsofi_device_bsoi(int n, int L, double *dA, int ldda, const double *dtau, void *dwork,
+                      void *stream) {
+  int e = bsofi_dev_prepare();
+  if (e) return cuda_info((cudaError_t)e);
+  e = bsofi_dev_bsoi(n, L, dA, ldda, dtau, dwork, stream);
+  return e ? cuda_info((cudaError_t)e) : 0;
+}
+
+int bsofi_device_invert(int n, int L, double *dA, int ldda, double *dtau, void *dwork,
+                        void *stream) {
+  long long c;
+  int e = bsofi_device_bsoftri(n, L, dA, ldda, dtau, dwork, stream);
+  if (e) return e;
+  c = bsofi_dev_launch_count();
+  e = bsofi_device_bsoi(n, L, dA, ldda, dtau, dwork, stream);
+  bsofi_dev_add_launches(c);
+  return e;
+}
+
+int *bsofi_device_info(void *dwork) { return bsofi_dev_info_ptr(dwork); }
+
+long long bsofi_device_last_launches(void) { return bsofi_dev_launch_count(); }
+
+int bsofi_selftest_gemm(int M, int N, int K, double alpha, const double *dA, int lda,
+                        int upper_a, const double *dB, int ldb, int upper_b, double beta,
+                        double *dC, int ldc, int tile, void *stream) {
+  int e = bsofi_dev_prepare();
+  if (!e)
+    e = bsofi_dev_selftest_gemm(M, N, K, alpha, dA, lda, upper_a, dB, ldb, upper_b, beta, dC,
+                                ldc, tile, stream);
+  return e ? cuda_info((cudaError_t)e) : 0;
+}
+
+void bsofi_device_timing(int on) { bsofi_dev_timing(on); }
+
+int bsofi_device_timing_read(double *ms, long long *launches) {
+  int e = bsofi_dev_timing_read(ms, launches);
+  return e ? cuda_info((cudaError_t)e) : 0;
+}

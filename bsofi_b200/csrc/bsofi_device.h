@@ -1,0 +1,61 @@
+/*
+ * bsofi_device.h -- device-side BSOF/I pipeline, plain C interface.
+ *
+ * Used by the host C layer (bsofi_api.c).  Every function enqueues work on
+ * `stream` (a cudaStream_t passed as void*) and returns a cudaError_t value
+ * (0 = success) without synchronising.  Matrices are column-major FP64 in
+ * device memory with leading dimension ldd >= n*L.
+ */
+#ifndef BSOFI_DEVICE_H
+#define BSOFI_DEVICE_H
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Bytes of device workspace the pipeline needs for (n, L, ldd). */
+size_t bsofi_dev_ws_bytes(int n, int L, int ldd);
+
+/* One-time per-process set-up (kernel attributes).  Call before capturing
+ * the pipeline into a CUDA graph. */
+int bsofi_dev_prepare(void);
+
+/* Zero the blocks of A that the factorization reads as structural zeros
+ * (superdiagonal blocks and the last block column except its first and last
+ * blocks).  Used after copying only the p-cyclic blocks to the device. */
+int bsofi_dev_zero_structural(int n, int L, double *dA, int ldd, void *stream);
+
+/* BSOF + BSTRI: A <- reflectors + R^{-1}, tau <- reflector scalars.
+ * Resets the workspace info word first; read it with bsofi_dev_info_ptr. */
+int bsofi_dev_bsoftri(int n, int L, double *dA, int ldd, double *dtau, void *dws,
+                      void *stream);
+/* BSOF only / BSTRI only (split phases). */
+int bsofi_dev_bsof(int n, int L, double *dA, int ldd, double *dtau, void *dws, void *stream);
+int bsofi_dev_bstri(int n, int L, double *dA, int ldd, void *dws, void *stream);
+/* BSOI: A (reflectors + R^{-1}) <- M^{-1}. */
+int bsofi_dev_bsoi(int n, int L, double *dA, int ldd, const double *dtau, void *dws,
+                   void *stream);
+
+/* Device address of the int info word inside the workspace (0 = ok,
+ * i > 0: R(i,i) exactly zero, 1-based global index). */
+int *bsofi_dev_info_ptr(void *dws);
+
+/* Number of kernels the last bsofi_dev_* call on this thread launched. */
+long long bsofi_dev_launch_count(void);
+void bsofi_dev_add_launches(long long c);
+
+/* Event timing of the BSOI step GEMM launches (on/off resets the record);
+ * read returns the summed duration (ms) and the number of timed launches. */
+void bsofi_dev_timing(int on);
+int bsofi_dev_timing_read(double *ms, long long *launches);
+
+/* One call of the FP64 tile engine (diagnostics). */
+int bsofi_dev_selftest_gemm(int M, int N, int K, double alpha, const double *dA, int lda,
+                            int upper_a, const double *dB, int ldb, int upper_b, double beta,
+                            double *dC, int ldc, int tile, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

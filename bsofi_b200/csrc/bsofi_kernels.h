@@ -1,0 +1,45 @@
+// Internal C++ interface between the device pipeline and the kernel files.
+#pragma once
+#include <cuda_runtime.h>
+#include "gemm.cuh"
+
+namespace bsofi {
+
+struct WySeg {
+  double* p;
+  long long ld, bs;
+  int ncols;
+};
+
+struct WyArgs {
+  const double* V;  // leaf top-left (unit lower trapezoidal reflectors)
+  long long ldv, vbs;
+  const double* T;  // 16 x 16 compact-WY factor (ld 16)
+  long long tbs;
+  int m, nb, trans;
+  WySeg seg[3];
+};
+
+int leaf_width(int n);
+cudaError_t launch_panel_leaf(double* P, long long ldp, int m, int nc, double* tau,
+                              double* Tout, int nbw, cudaStream_t st);
+cudaError_t launch_wy_apply(const WyArgs& a, int batch, cudaStream_t st);
+
+cudaError_t launch_trtri_blocks(double* A, long long ld, int n, long long bstride,
+                                int nblk, int* info, cudaStream_t st);
+
+// cfg: 0 = choose by tile count, 1 = 128x128 tiles, 2 = 64x64 tiles.
+cudaError_t launch_gemm(const GemmDims& d, const GemmA& a, const GemmB& b,
+                        const GemmC& c, int batch, int cfg, cudaStream_t st);
+cudaError_t gemm_init_attributes();
+
+cudaError_t launch_set_identity(double* G, long long ld, int m, long long bs, int batch,
+                                cudaStream_t st);
+// dst(r,c) = src(r,c), or 0 where r - roff > c (roff = kNoMask copies all).
+cudaError_t launch_copy_masked(double* dst, long long ldd, const double* src, long long lds,
+                               int rows, int cols, int roff, cudaStream_t st);
+// Zero the n x n blocks of A that BSOF reads as structural zeros:
+// superdiagonal blocks (k,k+1) and last-column blocks (k,L-1), 1 <= k <= L-2.
+cudaError_t launch_zero_structural(double* A, long long ld, int n, int L, cudaStream_t st);
+
+}  // namespace bsofi

@@ -1,0 +1,436 @@
+// Device pipeline of BSOF/I: the order of kernels for BSOF, BSTRI and BSOI.
+//
+// Reference algorithm: src/bsofi_cpu.c:86-248 (lapackXbsof, lapackXbstri,
+// lapackXbsoi_ormqr).  All data stays in HBM; nothing runs on the host.
+//
+// Workspace (one allocation, regions 256-byte aligned):
+//   info   int                      first exactly-zero diagonal of R (1-based)
+//   T      (L-1) x leaves x 16x16   compact-WY factors of every panel leaf
+//   G      (L-1) x (2n x 2n)        explicit Q_k^T of every panel
+//   W      (L-2) x (n x n)          BSTRI row multipliers  W_i = -R_ii^{-1} R_{i,i+1}
+//   Y      (L-1) x (n x n)          BSTRI scratch  R_{i,L-1} R_{L-1,L-1}^{-1}
+//   carry  2 x (ldd x n)            BSOI ping-pong block column
+#include <climits>
+#include <vector>
+#include "bsofi_device.h"
+#include "bsofi_kernels.h"
+
+using namespace bsofi;
+
+namespace {
+
+thread_local long long g_launches = 0;
+
+// Optional CUDA-event timing of every BSOI step GEMM launch (the dominant
+// kernel), recorded on the launching stream.
+struct GemmTimer {
+  bool on = false;
+  std::vector<cudaEvent_t> ev;  // pairs (start, stop)
+  size_t used = 0;
+  cudaError_t mark(cudaStream_t st) {
+    if (used == ev.size()) {
+      cudaEvent_t e;
+      cudaError_t r = cudaEventCreate(&e);
+      if (r != cudaSuccess) return r;
+      ev.push_back(e);
+    }
+    return cudaEventRecord(ev[used++], st);
+  }
+};
+thread_local GemmTimer g_timer;
+
+struct Layout {
+  size_t info, T, G, W, Y, C0, C1, total;
+  int nbw, maxleaves;
+};
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+Layout layout(int n, int L, int ldd) {
+  Layout l;
+  l.nbw = leaf_width(n);
+  l.maxleaves = (2 * n + l.nbw - 1) / l.nbw;
+  size_t off = 0;
+  l.info = off;
+  off += 256;
+  l.T = off;
+  off += align256(sizeof(double) * (size_t)(L - 1) * l.maxleaves * 256);
+  l.G = off;
+  off += align256(sizeof(double) * (size_t)(L - 1) * 4 * n * n);
+  l.W = off;
+  off += align256(sizeof(double) * (size_t)(L > 2 ? L - 2 : 1) * n * n);
+  l.Y = off;
+  off += align256(sizeof(double) * (size_t)(L - 1) * n * n);
+  l.C0 = off;
+  off += align256(sizeof(double) * (size_t)ldd * n);
+  l.C1 = off;
+  off += align256(sizeof(double) * (size_t)ldd * n);
+  l.total = off;
+  return l;
+}
+
+template <class T>
+T* at(void* ws, size_t off) {
+  return reinterpret_cast<T*>(reinterpret_cast<char*>(ws) + off);
+}
+
+// CK: a kernel launch (counted); CKM: a memset/copy (not a kernel).
+#define CK(x)                              \
+  do {                                     \
+    cudaError_t _e = (x);                  \
+    if (_e != cudaSuccess) return (int)_e; \
+    g_launches++;                          \
+  } while (0)
+#define CKM(x)                             \
+  do {                                     \
+    cudaError_t _e = (x);                  \
+    if (_e != cudaSuccess) return (int)_e; \
+  } while (0)
+
+// Compact-WY factor of one panel leaf from its stored reflectors and tau
+// (LAPACK dlarft, forward/columnwise): T(0:i,i) = -tau_i T(0:i,0:i) V^T v_i.
+// grid (leaves, panels); rebuilt in BSOI so that the split entry points work
+// from the caller's (A, tau) alone.
+__global__ void __launch_bounds__(256) build_leaf_t_kernel(const double* __restrict__ A,
+                                                           long long ld, int n, int L,
+                                                           const double* __restrict__ tau,
+                                                           double* __restrict__ Tbase,
+                                                           int maxleaves, int nbw) {
+  __shared__ double sV[64][17];
+  __shared__ double sG[16][17];
+  __shared__ double sT[16][17];
+  const int l = blockIdx.x, k = blockIdx.y, tid = threadIdx.x;
+  const int ncp = (k < L - 2) ? n : 2 * n;
+  const int j0 = l * nbw;
+  double* Tout = Tbase + ((size_t)k * maxleaves + l) * 256;
+  if (j0 >= ncp) return;
+  const int nc = min(nbw, ncp - j0), m = 2 * n - j0;
+  const double* V = A + cm((long long)k * n + j0, (long long)k * n + j0, ld);
+  const double* tl = tau + (size_t)k * n + j0;
+  const int ga = tid % 16, gb = tid / 16;
+  double acc = 0.0;
+  for (int r0 = 0; r0 < m; r0 += 64) {
+    __syncthreads();
+    for (int e = tid; e < 64 * 16; e += 256) {
+      int rr = e % 64, aa = e / 64, r = r0 + rr;
+      double v = 0.0;
+      if (r < m && aa < nc) v = (r == aa) ? 1.0 : (r > aa ? V[cm(r, aa, ld)] : 0.0);
+      sV[rr][aa] = v;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int rr = 0; rr < 64; rr++) acc = fma(sV[rr][ga], sV[rr][gb], acc);
+  }
+  sG[ga][gb] = acc;
+  sT[ga][gb] = 0.0;
+  __syncthreads();
+  if (tid < 32) {
+    for (int i = 0; i < nc; i++) {
+      double ti = tl[i];
+      double s = 0.0;
+      if (tid < i)
+        for (int b = tid; b < i; b++) s = fma(sT[tid][b], sG[b][i], s);
+      __syncwarp();
+      if (tid < i) sT[tid][i] = -ti * s;
+      if (tid == i) sT[i][i] = ti;
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  Tout[tid] = sT[tid % 16][tid / 16];
+}
+
+int run_bsof(int n, int L, double* dA, int ldd, double* dtau, void* ws, cudaStream_t st) {
+  Layout ly = layout(n, L, ldd);
+  double* Tb = at<double>(ws, ly.T);
+  for (int k = 0; k <= L - 2; k++) {
+    const int ncp = (k < L - 2) ? n : 2 * n;
+    double* P0 = dA + cm((long long)k * n, (long long)k * n, ldd);
+    for (int l = 0, j0 = 0; j0 < ncp; l++, j0 += ly.nbw) {
+      const int nc = min(ly.nbw, ncp - j0), m = 2 * n - j0;
+      double* P = P0 + cm(j0, j0, ldd);
+      double* T = Tb + ((size_t)k * ly.maxleaves + l) * 256;
+      CK(launch_panel_leaf(P, ldd, m, nc, dtau + (size_t)k * n + j0, T, ly.nbw, st));
+      WyArgs a = {};
+      a.V = P;
+      a.ldv = ldd;
+      a.T = T;
+      a.m = m;
+      a.nb = nc;
+      a.trans = 1;
+      a.seg[0] = {P0 + cm(j0, j0 + nc, ldd), ldd, 0, ncp - j0 - nc};
+      if (k < L - 2) {
+        a.seg[1] = {dA + cm((long long)k * n + j0, (long long)(k + 1) * n, ldd), ldd, 0, n};
+        a.seg[2] = {dA + cm((long long)k * n + j0, (long long)(L - 1) * n, ldd), ldd, 0, n};
+      }
+      CK(launch_wy_apply(a, 1, st));
+    }
+  }
+  return 0;
+}
+
+int run_bstri(int n, int L, double* dA, int ldd, void* ws, cudaStream_t st) {
+  Layout ly = layout(n, L, ldd);
+  int* info = at<int>(ws, ly.info);
+  double* W = at<double>(ws, ly.W);
+  double* Y = at<double>(ws, ly.Y);
+  const long long nn = (long long)n * n, diag = (long long)n * (ldd + 1);
+  CKM(cudaMemsetAsync(info, 0x7f, sizeof(int), st));
+  // X_ii = R_ii^{-1} for every diagonal block.
+  CK(launch_trtri_blocks(dA, ldd, n, diag, L, info, st));
+  GemmDims d = {n, n, n};
+  // Y_i = R_{i,L-1} X_{L-1,L-1},  i = 0..L-2.
+  {
+    GemmA a = {};
+    a.p0 = dA + cm(0, (long long)(L - 1) * n, ldd);
+    a.ld0 = ldd;
+    a.bs0 = n;
+    a.ld1 = 2;
+    a.ksplit = n;
+    a.rlim0 = INT_MAX;
+    a.roff0 = kNoMask;
+    a.rlim1 = INT_MAX;
+    a.roff1 = kNoMask;
+    GemmB b = {dA + cm((long long)(L - 1) * n, (long long)(L - 1) * n, ldd), ldd, 0, 0};
+    GemmC c = {};
+    c.p0 = Y;
+    c.ld0 = n;
+    c.bs0 = nn;
+    c.ld1 = 1;
+    c.nsplit = n;
+    c.alpha = 1.0;
+    CK(launch_gemm(d, a, b, c, L - 1, 0, st));
+  }
+  // Z_i = -X_ii Y_i  -> A(i, L-1).
+  {
+    GemmA a = {};
+    a.p0 = dA;
+    a.ld0 = ldd;
+    a.bs0 = diag;
+    a.ld1 = 2;
+    a.ksplit = n;
+    a.rlim0 = INT_MAX;
+    a.roff0 = 0;
+    a.rlim1 = INT_MAX;
+    a.roff1 = kNoMask;
+    GemmB b = {Y, n, nn, kNoMask};
+    GemmC c = {};
+    c.p0 = dA + cm(0, (long long)(L - 1) * n, ldd);
+    c.ld0 = ldd;
+    c.bs0 = n;
+    c.ld1 = 1;
+    c.nsplit = n;
+    c.alpha = -1.0;
+    CK(launch_gemm(d, a, b, c, L - 1, 0, st));
+  }
+  if (L >= 3) {
+    // W_i = -X_ii R_{i,i+1},  i = 0..L-3.
+    GemmA a = {};
+    a.p0 = dA;
+    a.ld0 = ldd;
+    a.bs0 = diag;
+    a.ld1 = 2;
+    a.ksplit = n;
+    a.rlim0 = INT_MAX;
+    a.roff0 = 0;
+    a.rlim1 = INT_MAX;
+    a.roff1 = kNoMask;
+    GemmB b = {dA + cm(0, n, ldd), ldd, diag, kNoMask};
+    GemmC c = {};
+    c.p0 = W;
+    c.ld0 = n;
+    c.bs0 = nn;
+    c.ld1 = 1;
+    c.nsplit = n;
+    c.alpha = -1.0;
+    CK(launch_gemm(d, a, b, c, L - 2, 0, st));
+  }
+  // Row recurrence: X_{i, i+1:L} = W_i X_{i+1, i+1:L} (+ Z_i on the last block).
+  for (int i = L - 3; i >= 0; i--) {
+    const int ncol = (L - 1 - i) * n;
+    GemmDims dr = {n, ncol, n};
+    GemmA a = {};
+    a.p0 = W + (size_t)i * nn;
+    a.ld0 = n;
+    a.ld1 = 2;
+    a.ksplit = n;
+    a.rlim0 = INT_MAX;
+    a.roff0 = kNoMask;
+    a.rlim1 = INT_MAX;
+    a.roff1 = kNoMask;
+    GemmB b = {dA + cm((long long)(i + 1) * n, (long long)(i + 1) * n, ldd), ldd, 0, 0};
+    GemmC c = {};
+    c.p0 = dA + cm((long long)i * n, (long long)(i + 1) * n, ldd);
+    c.ld0 = ldd;
+    c.p1 = dA + cm((long long)i * n, (long long)(L - 1) * n, ldd);
+    c.ld1 = ldd;
+    c.nsplit = ncol - n;
+    c.alpha = 1.0;
+    c.beta0 = 0.0;
+    c.beta1 = 1.0;
+    CK(launch_gemm(dr, a, b, c, 1, 2, st));
+  }
+  return 0;
+}
+
+int run_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* ws, cudaStream_t st) {
+  Layout ly = layout(n, L, ldd);
+  double* Tb = at<double>(ws, ly.T);
+  double* G = at<double>(ws, ly.G);
+  double* C[2] = {at<double>(ws, ly.C0), at<double>(ws, ly.C1)};
+  const int N = n * L, n2 = 2 * n;
+  const long long g2 = (long long)n2 * n2;
+
+  // Compact-WY factors from the stored reflectors, then G_k = Q_k^T.
+  build_leaf_t_kernel<<<dim3(ly.maxleaves, L - 1), 256, 0, st>>>(dA, ldd, n, L, dtau, Tb,
+                                                                  ly.maxleaves, ly.nbw);
+  CK(cudaGetLastError());
+  CK(launch_set_identity(G, n2, n2, g2, L - 1, st));
+  for (int l = 0, j0 = 0; j0 < n2; l++, j0 += ly.nbw) {
+    // Regular panels k = 0..L-3 have n reflectors, the last one 2n.
+    for (int part = 0; part < 2; part++) {
+      const int k0 = (part == 0) ? 0 : L - 2;
+      const int batch = (part == 0) ? L - 2 : 1;
+      const int ncp = (part == 0) ? n : n2;
+      if (batch <= 0 || j0 >= ncp) continue;
+      WyArgs a = {};
+      a.V = dA + cm((long long)k0 * n + j0, (long long)k0 * n + j0, ldd);
+      a.ldv = ldd;
+      a.vbs = (long long)n * (ldd + 1);
+      a.T = Tb + ((size_t)k0 * ly.maxleaves + l) * 256;
+      a.tbs = (long long)ly.maxleaves * 256;
+      a.m = n2 - j0;
+      a.nb = min(ly.nbw, ncp - j0);
+      a.trans = 1;
+      a.seg[0] = {G + (size_t)k0 * g2 + j0, n2, g2, n2};
+      CK(launch_wy_apply(a, batch, st));
+    }
+  }
+
+  // Carry for the first step: X(:, L-1) with the triangular diagonal block.
+  CK(launch_copy_masked(C[0], ldd, dA + cm(0, (long long)(L - 1) * n, ldd), ldd, N, n,
+                        (L - 1) * n, st));
+  int cur = 0;
+  for (int k = L - 2; k >= 0; k--) {
+    GemmDims d = {N, n2, n2};
+    GemmA a = {};
+    a.p0 = dA + cm(0, (long long)k * n, ldd);
+    a.ld0 = ldd;
+    a.p1 = C[cur];
+    a.ld1 = ldd;
+    a.ksplit = n;
+    a.rlim0 = (k + 1) * n;
+    a.roff0 = k * n;
+    a.rlim1 = INT_MAX;
+    a.roff1 = kNoMask;
+    GemmB b = {G + (size_t)k * g2, n2, 0, kNoMask};
+    GemmC c = {};
+    c.p0 = C[cur ^ 1];
+    c.ld0 = ldd;
+    c.p1 = dA + cm(0, (long long)(k + 1) * n, ldd);
+    c.ld1 = ldd;
+    c.nsplit = n;
+    c.alpha = 1.0;
+    if (g_timer.on) CKM(g_timer.mark(st));
+    CK(launch_gemm(d, a, b, c, 1, 0, st));
+    if (g_timer.on) CKM(g_timer.mark(st));
+    cur ^= 1;
+  }
+  CK(launch_copy_masked(dA, ldd, C[cur], ldd, N, n, kNoMask, st));
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t bsofi_dev_ws_bytes(int n, int L, int ldd) { return layout(n, L, ldd).total; }
+
+int bsofi_dev_prepare(void) { return (int)gemm_init_attributes(); }
+
+int bsofi_dev_zero_structural(int n, int L, double* dA, int ldd, void* stream) {
+  g_launches = 0;
+  CK(launch_zero_structural(dA, ldd, n, L, (cudaStream_t)stream));
+  return 0;
+}
+
+int bsofi_dev_bsof(int n, int L, double* dA, int ldd, double* dtau, void* dws, void* stream) {
+  g_launches = 0;
+  return run_bsof(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream);
+}
+
+int bsofi_dev_bstri(int n, int L, double* dA, int ldd, void* dws, void* stream) {
+  g_launches = 0;
+  return run_bstri(n, L, dA, ldd, dws, (cudaStream_t)stream);
+}
+
+int bsofi_dev_bsoftri(int n, int L, double* dA, int ldd, double* dtau, void* dws,
+                      void* stream) {
+  g_launches = 0;
+  int e = run_bsof(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream);
+  if (e) return e;
+  long long c = g_launches;
+  e = run_bstri(n, L, dA, ldd, dws, (cudaStream_t)stream);
+  g_launches += c;
+  return e;
+}
+
+int bsofi_dev_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* dws,
+                   void* stream) {
+  g_launches = 0;
+  return run_bsoi(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream);
+}
+
+int* bsofi_dev_info_ptr(void* dws) { return at<int>(dws, 0); }
+
+int bsofi_dev_selftest_gemm(int M, int N, int K, double alpha, const double* dA, int lda,
+                            int upper_a, const double* dB, int ldb, int upper_b, double beta,
+                            double* dC, int ldc, int tile, void* stream) {
+  GemmDims d = {M, N, K};
+  GemmA a = {};
+  a.p0 = dA;
+  a.ld0 = lda;
+  a.ld1 = 2;
+  a.ksplit = K;
+  a.rlim0 = INT_MAX;
+  a.roff0 = upper_a ? 0 : kNoMask;
+  a.rlim1 = INT_MAX;
+  a.roff1 = kNoMask;
+  GemmB b = {dB, ldb, 0, upper_b ? 0 : kNoMask};
+  GemmC c = {};
+  c.p0 = dC;
+  c.ld0 = ldc;
+  c.ld1 = 1;
+  c.nsplit = N;
+  c.alpha = alpha;
+  c.beta0 = beta;
+  g_launches = 0;
+  CK(launch_gemm(d, a, b, c, 1, tile, (cudaStream_t)stream));
+  return 0;
+}
+
+long long bsofi_dev_launch_count(void) { return g_launches; }
+
+void bsofi_dev_add_launches(long long c) { g_launches += c; }
+
+void bsofi_dev_timing(int on) {
+  g_timer.on = on != 0;
+  g_timer.used = 0;
+}
+
+int bsofi_dev_timing_read(double* ms, long long* launches) {
+  double tot = 0.0;
+  for (size_t i = 0; i + 1 < g_timer.used; i += 2) {
+    float t = 0.f;
+    cudaError_t e = cudaEventSynchronize(g_timer.ev[i + 1]);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, g_timer.ev[i], g_timer.ev[i + 1]);
+    if (e != cudaSuccess) return (int)e;
+    tot += t;
+  }
+  *ms = tot;
+  *launches = (long long)(g_timer.used / 2);
+  g_timer.used = 0;
+  return 0;
+}
+
+}  // extern "C"

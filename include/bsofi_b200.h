@@ -1,0 +1,183 @@
+/*
+ * bsofi_b200.h -- C ABI of the B200-native BSOF/I library (libbsofi_b200.so).
+ *
+ * BSOF/I: structured orthogonal factorization and explicit inversion of an
+ * N x N block p-cyclic matrix (N = n*L): identity-like diagonal blocks A_k,
+ * sub-diagonal blocks at (k+1, k) and a corner block at (0, L-1).  All
+ * arithmetic is FP64 on the GPU; there is no CPU fallback.
+ *
+ * The entry points keep the reference's names, argument lists and meaning
+ * (scalar_t = double, Fortran symbols lowercase with a trailing underscore,
+ * every Fortran argument by pointer).  Each declaration cites the reference
+ * interface it replaces.
+ *
+ * Storage contract (reference src/bsofi_cpu.c:58-85):
+ *   A      column-major, leading dimension lda >= n*L, overwritten in place.
+ *          Only the p-cyclic blocks (diagonal, sub-diagonal, corner) of the
+ *          input are read; every other block is taken as zero (the
+ *          reference reads them and assumes they are zero).
+ *   after XbsoftriH: the Householder vectors of panel k are stored below the
+ *          diagonal of A(kn:(k+2)n, kn:(k+1)n) (unit entry implicit), tau(kn+i)
+ *          their scalars (the last panel has 2n of them), and the block upper
+ *          triangle of A holds R^{-1}.
+ *   after XbsoiH: A holds M^{-1} (dense).
+ *
+ * Errors: info = 0 success; info = -i the i-th argument is illegal (LAPACK
+ * convention; i counts the handle as argument 1 in the handle API);
+ * info = i > 0 after BSTRI: R(i,i) is exactly zero (1-based global index,
+ * the inverse was not formed); info <= BSOFI_INFO_CUDA: a CUDA runtime error
+ * (BSOFI_INFO_CUDA - cudaError_t).  No entry point exits the process.
+ *
+ * Threading: every handle owns its own stream and device buffers, so calls
+ * on different handles may run from different threads.  The C names without
+ * a handle (lapackX*, hybridX*, gpuX*) share one context per thread.
+ */
+#ifndef BSOFI_B200_H
+#define BSOFI_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BSOFI_INFO_CUDA (-1000)
+#define BSOFI_MAX_BLOCK 1024 /* largest supported block size n */
+
+/* ------------------------------------------------------------------------
+ * Fortran handle API (primary drop-in).  `handle` is the caller's
+ * integer handler(10) array (40 bytes); it stores a context pointer.
+ * ---------------------------------------------------------------------- */
+
+/* Replaces cb_hybridXinitH, src/bsofi_callback.c:101-128 (bsofi.h:282).
+ * Allocates the device context for (n, L, lda).  Returns 0, or -1 on an
+ * illegal argument or a device failure (as the reference). */
+int hybridxinith_(int *handle, int *n, int *L, int *lda);
+
+/* Replaces cb_hybridXbsofiLWorkH, src/bsofi_callback.c:170-180
+ * (bsofi.h:290).  Returns the host workspace length in doubles for `work`
+ * of XbsoftriH / XbsoiH.  The GPU path keeps its workspace on the device,
+ * so this is 1. */
+int hybridxbsofilworkh_(int *handle, int *n, int *L, int *lda);
+
+/* Replaces cb_hybridXbsoftriH, src/bsofi_callback.c:130-144 (bsofi.h:283).
+ * BSOF + BSTRI.  lwork = -1: work[0] <- host workspace length;
+ * lwork = -2: work[0] <- device workspace length (doubles).  Returns *info. */
+int hybridxbsoftrih_(int *handle, int *n, int *L, double *A, int *lda, double *tau,
+                     double *work, int *lwork, int *info);
+
+/* Replaces cb_hybridXbsoiH, src/bsofi_callback.c:146-157 (bsofi.h:286).
+ * BSOI: A (reflectors + R^{-1}, tau) <- M^{-1}.  Returns *info. */
+int hybridxbsoih_(int *handle, int *n, int *L, double *A, int *lda, double *tau,
+                  double *work, int *lwork, int *info);
+
+/* Replaces cb_hybridXfinalizeH, src/bsofi_callback.c:159-168 (bsofi.h:289).
+ * Frees the context and clears the handle.  Returns 0. */
+int hybridxfinalizeh_(int *handle);
+
+/* Replace the timer callbacks fgetwalltime/felapsed,
+ * src/bsofi_callback.c:189-218. */
+void fgetwalltime_(double tv[2]);
+double felapsed_(double t1[2], double t0[2]);
+
+/* ------------------------------------------------------------------------
+ * C names of the reference (thin wrappers over the same device pipeline).
+ * ---------------------------------------------------------------------- */
+
+/* Replaces lapackXbsofiLWork, src/bsofi_cpu.c:31-42 (include/bsofi_cpu.h:24). */
+int lapackXbsofiLWork(int n, int L, int lda);
+/* Replaces lapackXbsof, src/bsofi_cpu.c:86-118 (include/bsofi_cpu.h:26). */
+int lapackXbsof(int n, int L, double A[], int lda, double tau[], double work[], int lwork,
+                int *info);
+/* Replaces lapackXbstri, src/bsofi_cpu.c:146-177 (include/bsofi_cpu.h:38). */
+int lapackXbstri(int n, int L, double A[], int lda, int *info);
+/* Replace lapackXbsoi_ormqr / lapackXbsoi_orgqr, src/bsofi_cpu.c:211-248 and
+ * 283-333 (include/bsofi_cpu.h:30-36).  Both compute M^{-1} = R^{-1} Q^T. */
+int lapackXbsoi_ormqr(int n, int L, double A[], int lda, double tau[], double work[],
+                      int lwork, int *info);
+int lapackXbsoi_orgqr(int n, int L, double A[], int lda, double tau[], double work[],
+                      int lwork, int *info);
+
+/* Fortran twins, include/bsofi_cpu.h:48-72 (src/bsofi_callback.c:24-56). */
+int lapackxbsofilwork_(int *n, int *L, int *lda);
+int lapackxbsof_(int *n, int *L, double A[], int *lda, double tau[], double work[],
+                 int *lwork, int *info);
+int lapackxbstri_(int *n, int *L, double A[], int *lda, int *info);
+int lapackxbsoi_ormqr_(int *n, int *L, double A[], int *lda, double tau[], double work[],
+                       int *lwork, int *info);
+int lapackxbsoi_orgqr_(int *n, int *L, double A[], int *lda, double tau[], double work[],
+                       int *lwork, int *info);
+
+/* Replaces hybridXbsofiLWork, src/bsofi_hybrid_adaptive.c:43-57
+ * (include/bsofi_hybrid.h:110).  lworkHostDevice = -1: host length,
+ * -2: device length (doubles). */
+int hybridXbsofiLWork(int n, int L, int lda, int lworkHostDevice);
+/* Replace hybridXbsoftri / hybridXbsoi, src/bsofi_hybrid_adaptive.c:108-213,
+ * 255-403 (include/bsofi_hybrid.h:120-130).  `handle` is the reference's
+ * cublasHandle_t slot (an int when cuBLAS is absent) and is ignored; dwork
+ * and ldwork are accepted for ABI compatibility and not used. */
+int hybridXbsoftri(int handle, int n, int L, double A[], int lda, double tau[], double work[],
+                   int lwork, double dwork[], int ldwork, int *info);
+int hybridXbsoi(int handle, int n, int L, double A[], int lda, double tau[], double work[],
+                int lwork, double dwork[], int ldwork, int *info);
+
+/* Device-pointer API, include/bsofi_gpu.h:34-62 (src/bsofi_gpu.c:74-414).
+ * dA is device memory (ldda >= n*L), tau is HOST memory as in the reference
+ * (MAGMA returns tau on the host).  dT / dwork are accepted and not used.
+ * Synchronous. */
+int gpuXbsof(int n, int L, double dA[], int ldda, double tau[], double work[], int lwork,
+             double *dT, int *info);
+int gpuXbstri_rseq(int n, int L, double dA[], int ldda, double dwork[], int ldwork, int *info);
+int gpuXbstri_rbatched(int n, int L, double dA[], int ldda, double dwork[], int ldwork,
+                       int *info);
+int gpuXbsoi_ormqr(int n, int L, double dA[], int ldda, double tau[], double work[], int lwork,
+                   double *dT, double dwork[], int ldwork, int *info);
+int gpuXbsoi_orgqr(int n, int L, double dA[], int ldda, double tau[], double work[], int lwork,
+                   double *dT, double dwork[], int ldwork, int *info);
+int gpuXbsoi_batched(int n, int L, double dA[], int ldda, double tau[], double work[],
+                     int lwork, double *dT, double dwork[], int ldwork, int *info);
+
+/* ------------------------------------------------------------------------
+ * Asynchronous device-resident API.  No reference counterpart: the
+ * reference's GPU routines are synchronous and keep tau on the host.  Used
+ * by callers that hold M in HBM (batched walkers, the benchmark).
+ * ---------------------------------------------------------------------- */
+
+/* Device workspace bytes for (n, L, ldda). */
+unsigned long long bsofi_device_workspace_bytes(int n, int L, int ldda);
+
+/* BSOF + BSTRI + BSOI on device memory, enqueued on `stream`
+ * (cudaStream_t, 0 = legacy default stream); dtau is device memory (N
+ * doubles), dwork device memory of bsofi_device_workspace_bytes.  dA must
+ * hold the p-cyclic input with every other block zero.  Returns 0 or
+ * BSOFI_INFO_CUDA - cudaError_t; the BSTRI info word is at
+ * bsofi_device_info(dwork) (device int, values >= 0x7f7f7f7f mean 0). */
+int bsofi_device_invert(int n, int L, double *dA, int ldda, double *dtau, void *dwork,
+                        void *stream);
+int bsofi_device_bsoftri(int n, int L, double *dA, int ldda, double *dtau, void *dwork,
+                         void *stream);
+int bsofi_device_bsoi(int n, int L, double *dA, int ldda, const double *dtau, void *dwork,
+                      void *stream);
+int *bsofi_device_info(void *dwork);
+/* Kernels launched by the last bsofi_device_* call on this thread. */
+long long bsofi_device_last_launches(void);
+
+/* Diagnostics (no reference counterpart): when on, every BSOI step GEMM
+ * launch (the dominant kernel) made by this thread is bracketed by CUDA
+ * events on its stream; bsofi_device_timing_read waits for them and returns
+ * the summed kernel time in ms and the number of timed launches, then clears
+ * the record. */
+void bsofi_device_timing(int on);
+int bsofi_device_timing_read(double *ms, long long *launches);
+
+/* Diagnostic entry point (no reference counterpart): one call of the FP64
+ * DMMA tile engine, C = alpha*A*B + beta*C on device memory (column-major),
+ * with the optional upper-triangular masks the pipeline uses (upper_a: A(i,k)
+ * = 0 for i > k; upper_b: B(k,j) = 0 for k > j).  tile: 0 auto, 1 128x128,
+ * 2 64x64.  Enqueued on `stream`; returns 0 or BSOFI_INFO_CUDA - error. */
+int bsofi_selftest_gemm(int M, int N, int K, double alpha, const double *dA, int lda,
+                        int upper_a, const double *dB, int ldb, int upper_b, double beta,
+                        double *dC, int ldc, int tile, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
