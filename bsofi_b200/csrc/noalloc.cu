@@ -1,0 +1,79 @@
+// Allocation-free variant of the device-resident inversion.
+//
+// Some callers cannot allocate device memory when they invert: a DQMC code
+// whose memory pool has already reserved nearly all of HBM (a fresh
+// cudaMalloc fails), or a caller that must not let cudaMalloc/cudaFree
+// synchronize the device in the middle of a Monte Carlo sweep while other
+// streams are busy.  bsofi_device_invert_noalloc serves them: it runs the same
+// BSOF + BSTRI + BSOI kernels as bsofi_device_invert, but its workspace is the
+// file-scope array below instead of a caller buffer, and it calls no
+// cudaMalloc, cudaFree or allocating library routine.
+//
+// The array is BSOFI_NOALLOC_SCRATCH_BYTES (32 MiB) and every GPU that loads
+// this library holds it until the process exits.  All calls share it and it
+// keeps the previous call's contents: the pipeline writes every scratch
+// region before reading it (the BSTRI info word is reset at the start of each
+// call), so nothing needs clearing between calls, but calls that overlap on
+// the GPU (different streams or threads on the same device) race on it.
+#include <cuda_runtime.h>
+#include <pthread.h>
+
+#include "bsofi_device.h"
+
+#define BSOFI_NOALLOC_SCRATCH_BYTES (32ull << 20)
+#define BSOFI_NOALLOC_MAX_DEVICES 64
+#define BSOFI_INFO_CUDA (-1000)
+#define BSOFI_NOALLOC_TOO_LARGE (-2000)
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[BSOFI_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+pthread_mutex_t g_mu = PTHREAD_MUTEX_INITIALIZER;
+void* g_scratch_addr[BSOFI_NOALLOC_MAX_DEVICES];
+
+// Device address of the scratch array on the current device.  In host code
+// the array's name is only a host-side stand-in, so the address is looked up
+// once per device (with that device current) and cached.
+cudaError_t scratch_address(void** out) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= BSOFI_NOALLOC_MAX_DEVICES) return cudaErrorInvalidDevice;
+  pthread_mutex_lock(&g_mu);
+  if (g_scratch_addr[dev] == nullptr) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e == cudaSuccess) g_scratch_addr[dev] = p;
+  }
+  *out = g_scratch_addr[dev];
+  pthread_mutex_unlock(&g_mu);
+  return e;
+}
+
+}  // namespace
+
+extern "C" __attribute__((visibility("default"))) unsigned long long
+bsofi_noalloc_scratch_bytes(void) {
+  return BSOFI_NOALLOC_SCRATCH_BYTES;
+}
+
+extern "C" __attribute__((visibility("default"))) int bsofi_device_invert_noalloc(
+    int n, int L, double* dA, int ldda, double* dtau, int* dinfo, void* stream) {
+  if (n < 1 || n > 1024 || L < 2 || ldda < n * L || dA == nullptr || dtau == nullptr) return -1;
+  if (bsofi_dev_ws_bytes(n, L, ldda) > BSOFI_NOALLOC_SCRATCH_BYTES) return BSOFI_NOALLOC_TOO_LARGE;
+  void* ws = nullptr;
+  cudaError_t e = scratch_address(&ws);
+  if (e != cudaSuccess) return BSOFI_INFO_CUDA - (int)e;
+  int r = bsofi_dev_prepare();
+  if (r == 0) r = bsofi_dev_bsoftri(n, L, dA, ldda, dtau, ws, stream);
+  if (r == 0 && dinfo != nullptr)
+    r = (int)cudaMemcpyAsync(dinfo, bsofi_dev_info_ptr(ws), sizeof(int), cudaMemcpyDeviceToDevice,
+                             (cudaStream_t)stream);
+  if (r == 0) {
+    long long c = bsofi_dev_launch_count();
+    r = bsofi_dev_bsoi(n, L, dA, ldda, dtau, ws, stream);
+    bsofi_dev_add_launches(c);
+  }
+  return r ? BSOFI_INFO_CUDA - r : 0;
+}

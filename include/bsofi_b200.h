@@ -160,6 +160,27 @@ int *bsofi_device_info(void *dwork);
 /* Kernels launched by the last bsofi_device_* call on this thread. */
 long long bsofi_device_last_launches(void);
 
+/* Allocation-free inversion.  No counterpart in the reference.  For callers
+ * that cannot allocate device memory at inversion time: a code whose memory
+ * pool already holds nearly all of HBM (cudaMalloc would fail), or one that
+ * cannot let cudaMalloc/cudaFree synchronize the device mid-sweep.  Same
+ * kernels and result as bsofi_device_invert, but the workspace is a static
+ * device array of bsofi_noalloc_scratch_bytes() (32 MiB) that every GPU
+ * loading this library keeps until exit; the call makes no cudaMalloc,
+ * cudaFree or other allocating call.  Problems whose workspace
+ * (bsofi_device_workspace_bytes) exceeds it are rejected with
+ * BSOFI_NOALLOC_TOO_LARGE (for example n=64 up to L=64, n=128 up to L=16).
+ * The first call on a device looks up the array's device address (with that
+ * device current) and should come before any stream capture.  All calls share
+ * the array: calls that overlap on the GPU race.  dinfo (device int, may be
+ * NULL) receives the BSTRI info word (values >= 0x7f7f7f7f mean 0).
+ * Returns 0, -1 for an illegal argument, BSOFI_NOALLOC_TOO_LARGE, or
+ * BSOFI_INFO_CUDA - cudaError_t. */
+#define BSOFI_NOALLOC_TOO_LARGE (-2000)
+unsigned long long bsofi_noalloc_scratch_bytes(void);
+int bsofi_device_invert_noalloc(int n, int L, double *dA, int ldda, double *dtau, int *dinfo,
+                                void *stream);
+
 /* Diagnostics (no reference counterpart): when on, every BSOI step GEMM
  * launch (the dominant kernel) made by this thread is bracketed by CUDA
  * events on its stream; bsofi_device_timing_read waits for them and returns
