@@ -187,16 +187,22 @@ static int check_args(const int *h_ok, int n, int L, const double *A, int lda,
   return 0;
 }
 
+/* Reads the BSTRI info word and the BSOF error word (a bounded wait inside
+ * the persistent BSOF kernel that gave up) after synchronising the stream. */
 static int read_info(bsofi_ctx *c, int *info) {
-  int v = 0;
-  cudaError_t e = cudaMemcpyAsync(&v, bsofi_dev_info_ptr(c->dws), sizeof(int),
+  int v[2] = {0, 0};
+  cudaError_t e = cudaMemcpyAsync(v, bsofi_dev_info_ptr(c->dws), sizeof(v),
                                   cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) {
     *info = cuda_info(e);
     return *info;
   }
-  *info = (v >= 0x7f7f7f7f || v < 0) ? 0 : v;
+  if (v[1] != 0) {
+    *info = cuda_info(cudaErrorLaunchTimeout);
+    return *info;
+  }
+  *info = (v[0] >= 0x7f7f7f7f || v[0] < 0) ? 0 : v[0];
   return *info;
 }
 
@@ -225,6 +231,10 @@ static int drive_bsoftri(bsofi_ctx *c, int n, int L, double *A, int lda, double 
     if (e != cudaSuccess) return cuda_info(e);
   }
   if (do_tri) return read_info(c, &info);
+  if (do_bsof) {
+    read_info(c, &info);
+    return info < 0 ? info : 0;
+  }
   e = cudaStreamSynchronize(c->stream);
   return e == cudaSuccess ? 0 : cuda_info(e);
 }
@@ -567,3 +577,15 @@ int bsofi_device_timing_read(double *ms, long long *launches) {
   int e = bsofi_dev_timing_read(ms, launches);
   return e ? cuda_info((cudaError_t)e) : 0;
 }
+
+int bsofi_device_bsof_timeline(int n, int L, int ldda, void *dwork, unsigned long long *host,
+                               int max_leaves) {
+  unsigned long long *d = NULL;
+  int leaves = bsofi_dev_bsof_timeline(n, L, ldda, dwork, &d);
+  int cnt = leaves < max_leaves ? leaves : max_leaves;
+  cudaError_t e = cudaMemcpy(host, d, sizeof(unsigned long long) * 4 * (size_t)cnt,
+                             cudaMemcpyDeviceToHost);
+  return e == cudaSuccess ? cnt : cuda_info(e);
+}
+
+void bsofi_device_set_bsof_workers(int workers) { bsofi_dev_set_bsof_workers(workers); }

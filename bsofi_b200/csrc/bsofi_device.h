@@ -50,6 +50,12 @@ void bsofi_dev_add_launches(long long c);
 void bsofi_dev_timing(int on);
 int bsofi_dev_timing_read(double *ms, long long *launches);
 
+/* Device address of the BSOF timeline (4 globaltimer stamps per leaf: loop
+ * start, tile ready, leaf published, next-tile update start); returns the
+ * number of leaves. */
+int bsofi_dev_bsof_timeline(int n, int L, int ldd, void *dws, unsigned long long **ptr);
+void bsofi_dev_set_bsof_workers(int w);
+
 /* One call of the FP64 tile engine (diagnostics). */
 int bsofi_dev_selftest_gemm(int M, int N, int K, double alpha, const double *dA, int lda,
                             int upper_a, const double *dB, int ldb, int upper_b, double beta,

@@ -1,0 +1,744 @@
+// BSOF as one persistent kernel.
+//
+// Reference: lapackXbsof, src/bsofi_cpu.c:86-118: for k = 0..L-3, dgeqrf of
+// the stacked 2n x n panel [R~_k; B_k] at A_BLK(k,k), dormqr('L','T') of
+// A_BLK(k,k+1) and A_BLK(k,L-1); then dgeqrf of the final 2n x 2n block.
+//
+// Work decomposition.  Every block column is cut into tiles of NB columns
+// (the last one may be narrower).  A "leaf" is the Householder QR of one tile
+// inside its panel; leaves are numbered s = 0..S-1 in the reference's order
+// (panel k, left to right; the final panel has the tiles of block columns L-2
+// and L-1).  Leaf s updates a set of target tiles with its block reflector
+// (I - V T V^T)^T: the rest of its panel, the next diagonal block column
+// (A_BLK(k,k+1)) and the last block column (A_BLK(k,L-1)).
+//
+// For a physical tile x the leaves that update it form one contiguous range
+// [lo(x), hi(x)) of leaf numbers, and hi(x) is the leaf that factors it.  A
+// counter cnt[x] holds how many of those updates are done, so leaf s may
+// update x once cnt[x] == s - lo(x), and may factor x once cnt[x] == hi - lo.
+//
+// CTA 0 runs the critical chain: factor leaf s, then immediately apply it to
+// the tile of leaf s+1 (target 0).  The other CTAs claim the remaining
+// (leaf, target) updates from an ordered task counter.  Every wait depends
+// only on tasks earlier in that order and all CTAs are co-resident
+// (cooperative launch), so the schedule cannot deadlock; every spin is
+// bounded and sets an error word instead of hanging.
+#include <climits>
+#include "bsofi_common.cuh"
+#include "bsofi_kernels.h"
+
+namespace bsofi {
+
+constexpr int BT = 256;  // threads per CTA
+constexpr int BW = BT / 32;
+
+struct BsofGeom {
+  int n, L, NB, nl, S;
+};
+
+// Leaf s -> panel k, leaf index l in the panel, tile (m, t), panel column j0.
+struct Leaf {
+  int k, l, m, t, j0, w;
+};
+
+BSOFI_DEVINL Leaf leaf_of(const BsofGeom& g, int s) {
+  Leaf f;
+  const int reg = (g.L - 2) * g.nl;
+  if (s < reg) {
+    f.k = s / g.nl;
+    f.l = s % g.nl;
+    f.m = f.k;
+    f.t = f.l;
+    f.j0 = f.t * g.NB;
+  } else {
+    f.k = g.L - 2;
+    f.l = s - reg;
+    if (f.l < g.nl) {
+      f.m = g.L - 2;
+      f.t = f.l;
+      f.j0 = f.t * g.NB;
+    } else {
+      f.m = g.L - 1;
+      f.t = f.l - g.nl;
+      f.j0 = g.n + f.t * g.NB;
+    }
+  }
+  f.w = min(g.NB, g.n - f.t * g.NB);
+  return f;
+}
+
+BSOFI_DEVINL int tile_id(const BsofGeom& g, int m, int t) { return m * g.nl + t; }
+
+BSOFI_DEVINL void tile_range(const BsofGeom& g, int m, int t, int& lo, int& hi) {
+  if (m <= g.L - 2) {
+    lo = max(0, (m - 1) * g.nl);
+    hi = m * g.nl + t;
+  } else {
+    lo = 0;
+    hi = (g.L - 1) * g.nl + t;
+  }
+}
+
+// Number of targets of leaf s; target q (0 = tile of leaf s+1).
+BSOFI_DEVINL int ntargets(const BsofGeom& g, const Leaf& f) {
+  if (f.k <= g.L - 3) return (g.nl - 1 - f.l) + 2 * g.nl;
+  return 2 * g.nl - 1 - f.l;
+}
+
+BSOFI_DEVINL void target_of(const BsofGeom& g, const Leaf& f, int q, int& m, int& t) {
+  if (f.k <= g.L - 3) {
+    const int np = g.nl - 1 - f.l;
+    if (q < np) {
+      m = f.k;
+      t = f.l + 1 + q;
+    } else if (q < np + g.nl) {
+      m = f.k + 1;
+      t = q - np;
+    } else {
+      m = g.L - 1;
+      t = q - np - g.nl;
+    }
+  } else {
+    int u = f.l + 1 + q;
+    if (u < g.nl) {
+      m = g.L - 2;
+      t = u;
+    } else {
+      m = g.L - 1;
+      t = u - g.nl;
+    }
+  }
+}
+
+// Worker tasks before leaf s (each leaf contributes ntargets - 1 tasks).
+BSOFI_DEVINL long long tasks_before(const BsofGeom& g, int s) {
+  const int reg = (g.L - 2) * g.nl;
+  const long long nl = g.nl;
+  const long long per_reg_leaf0 = 3 * nl - 2;  // tasks of regular leaf l: 3nl - 2 - l
+  const long long per_panel = nl * per_reg_leaf0 - nl * (nl - 1) / 2;
+  if (s <= reg) {
+    long long k = s / g.nl, l = s % g.nl;
+    return k * per_panel + l * per_reg_leaf0 - l * (l - 1) / 2;
+  }
+  long long base = (long long)(g.L - 2) * per_panel;
+  long long l = s - reg;  // final leaf l has max(2nl - 2 - l, 0) tasks
+  long long full = min(l, 2 * nl - 1);
+  return base + full * (2 * nl - 2) - full * (full - 1) / 2;
+}
+
+struct BsofState {
+  double* A;
+  long long ld;
+  double* tau;
+  double* T;  // 256 doubles per leaf: (k * maxleaves + l) * 256
+  int maxleaves;
+  int* cnt;       // per tile
+  int* factored;  // per leaf
+  int* next_task;
+  int* err;       // 0 ok; 1 timeout
+  long long spin_limit;
+  unsigned long long* timeline;  // 4 stamps per leaf from the panel CTA (diagnostics)
+};
+
+BSOFI_DEVINL unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+BSOFI_DEVINL int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+BSOFI_DEVINL void red_release_add(int* p, int v) {
+  asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Thread 0 waits until *p >= target (bounded); the result is broadcast.
+// Returns false when the wait timed out or another CTA reported an error.
+BSOFI_DEVINL bool block_wait_geq(const BsofState& st, const int* p, int target, int* sflag) {
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    long long it = 0;
+    while (ld_acquire(p) < target) {
+      if (ld_acquire(st.err) != 0) {
+        ok = 0;
+        break;
+      }
+      if (++it > st.spin_limit) {
+        atomicExch(st.err, 1);
+        ok = 0;
+        break;
+      }
+      __nanosleep(64);
+    }
+    *sflag = ok;
+  }
+  __syncthreads();
+  bool ok = *sflag != 0;
+  __syncthreads();
+  return ok;
+}
+
+// Sum NB values per lane over a warp (transpose reduction): lane l ends with
+// the warp sum of value (l >> (5 - log2 NB)) & (NB - 1).
+template <int NB>
+BSOFI_DEVINL double wsum_t(double (&v)[NB], int lane) {
+  constexpr int LOG = (NB == 16) ? 4 : 3;
+#pragma unroll
+  for (int lev = 0; lev < LOG; lev++) {
+    const int off = 16 >> lev, half = NB >> (lev + 1);
+    const bool up = (lane & off) != 0;
+#pragma unroll
+    for (int j = 0; j < half; j++) {
+      double send = up ? v[j] : v[j + half];
+      double keep = up ? v[j + half] : v[j];
+      v[j] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+    }
+  }
+  double s = v[0];
+#pragma unroll
+  for (int off = 16 >> LOG; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+  return s;
+}
+
+template <int NB>
+struct Smem {
+  double red[2][BW][NB];
+  double coef[2][NB + 4];   // tau*w_c (c < NB), tau, scale, beta
+  double prow[2][NB];
+  double gsh[2][NB];
+  double T[NB][NB + 1];
+  double redW[BW][NB][NB + 1];
+  double W[NB][NB + 1];
+  int flag;
+  int task;
+};
+
+// Load rows [row0 + r] (thread-owned rows r = tid + BT*i) of NB columns.
+template <int R, int NB>
+BSOFI_DEVINL void load_rows(double (&a)[R][NB], const double* P, long long ld, int m, int w) {
+#pragma unroll
+  for (int i = 0; i < R; i++) {
+    const int r = threadIdx.x + BT * i;
+#pragma unroll
+    for (int c = 0; c < NB; c++) a[i][c] = (r < m && c < w) ? __ldcg(P + cm(r, c, ld)) : 0.0;
+  }
+}
+
+template <int R, int NB>
+BSOFI_DEVINL void store_rows(const double (&a)[R][NB], double* P, long long ld, int m, int w) {
+#pragma unroll
+  for (int i = 0; i < R; i++) {
+    const int r = threadIdx.x + BT * i;
+    if (r < m) {
+#pragma unroll
+      for (int c = 0; c < NB; c++)
+        if (c < w) __stcg(P + cm(r, c, ld), a[i][c]);
+    }
+  }
+}
+
+// T(0:I, I) = -tau_I T(0:I,0:I) g_I (LAPACK dlarft), run by one warp one
+// column behind the factorization; T and g are zero outside their ranges.
+template <int NB>
+BSOFI_DEVINL void t_column(Smem<NB>& sm, int I, int lane) {
+  const int buf = I & 1;
+  const double taui = sm.coef[buf][NB];
+  if (lane < I) {
+    double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+    for (int b = 0; b < NB; b += 2) {
+      s0 = fma(sm.T[lane][b], sm.gsh[buf][b], s0);
+      s1 = fma(sm.T[lane][b + 1], sm.gsh[buf][b + 1], s1);
+    }
+    sm.T[lane][I] = -taui * (s0 + s1);
+  }
+  if (lane == I) sm.T[I][I] = taui;
+  __syncwarp();
+}
+
+// Householder QR of one leaf held in registers (thread t owns rows t + BT*i).
+// The column loop is a runtime loop over a rotating layout: at step I
+// position 0 holds column I, positions 1..NB-1-I the columns not yet
+// factored, and positions NB-I..NB-1 the finished reflectors 0..I-1; the
+// array rotates left by one position after each step, so every register index
+// is a compile-time constant while the loop body exists once (a fully
+// unrolled column loop overflows the instruction cache).
+//
+// One block reduction per column carries, per position, either the dot
+// product d_c = sum_{r>I} a_rI a_rc with a pending column (position 0 gives
+// ||x||^2) or e_j = sum_{r>I} v_j[r] a_rI with a finished reflector, which
+// builds the dlarft factor T(0:I,I) = -tau_I T(0:I,0:I) V^T v_I.
+template <int R, int NB>
+BSOFI_DEVINL void factor_leaf(double (&a)[R][NB], Smem<NB>& sm, int m, int w, double* tau_out) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int SH = (NB == 16) ? 1 : 2;
+#pragma unroll 1
+  for (int I = 0; I < w; I++) {
+    const int buf = I & 1;
+    const int ndone0 = NB - I;  // first position holding a finished reflector
+    if (tid == I) {
+#pragma unroll
+      for (int p = 0; p < NB; p++) sm.prow[buf][p] = a[0][p];
+    }
+    double part[NB];
+#pragma unroll
+    for (int p = 0; p < NB; p++) part[p] = 0.0;
+#pragma unroll
+    for (int i = 0; i < R; i++) {
+      const int r = tid + BT * i;
+      const double x = (r > I) ? a[i][0] : 0.0;  // rows >= m hold zeros
+#pragma unroll
+      for (int p = 0; p < NB; p++) part[p] = fma(x, a[i][p], part[p]);
+    }
+    {
+      double sum = wsum_t<NB>(part, lane);
+      if ((lane & ((1 << SH) - 1)) == 0) sm.red[buf][warp][(lane >> SH) & (NB - 1)] = sum;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      const int slot = lane % NB;
+      double tot = 0.0;
+#pragma unroll
+      for (int k = lane / NB; k < BW; k += 32 / NB) tot += sm.red[buf][k][slot];
+#pragma unroll
+      for (int off = NB; off < 32; off <<= 1) tot += __shfl_xor_sync(0xffffffffu, tot, off);
+      const double xnorm2 = __shfl_sync(0xffffffffu, tot, 0);
+      const double alpha = sm.prow[buf][0];
+      double beta, taui, scale;
+      if (xnorm2 == 0.0) {
+        taui = 0.0;
+        beta = alpha;
+        scale = 1.0;
+      } else {
+        // beta = -sign(alpha) ||(alpha, x)||, tau = (beta - alpha)/beta = 1 + |alpha|/||.||,
+        // scale = 1/(alpha - beta): one reciprocal square root and one division.
+        const double s2 = fma(alpha, alpha, xnorm2);
+        const double rn = rsqrt(s2);
+        beta = -copysign(s2 * rn, alpha);
+        taui = fma(fabs(alpha), rn, 1.0);
+        scale = 1.0 / (alpha - beta);
+      }
+      const double val = fma(scale, tot, sm.prow[buf][slot]);
+      if (lane < NB) {
+        // tau*w_c at pending positions 1..NB-1-I, zero elsewhere, so the row
+        // update below needs no predicates.
+        sm.coef[buf][slot] = (slot >= 1 && slot < ndone0) ? taui * val : 0.0;
+        // g_j = v_j^T v_I for j < I, zero for j >= I.
+        // lane slot writes g at index (slot - ndone0) mod NB: indices < I get
+        // the reflector dot products, the others zero.
+        const int j = (slot + I) & (NB - 1);
+        sm.gsh[buf][j] = (slot >= ndone0) ? val : 0.0;
+      }
+      if (lane == 0) {
+        sm.coef[buf][NB] = taui;
+        sm.coef[buf][NB + 1] = scale;
+        sm.coef[buf][NB + 2] = beta;
+        tau_out[I] = taui;
+      }
+    }
+    if (warp == 1 && I > 0) t_column<NB>(sm, I - 1, lane);
+    __syncthreads();
+    const double taui = sm.coef[buf][NB], scale = sm.coef[buf][NB + 1],
+                 beta = sm.coef[buf][NB + 2];
+    double cf[NB];
+#pragma unroll
+    for (int p = 1; p < NB; p++) cf[p] = sm.coef[buf][p];
+#pragma unroll
+    for (int i = 0; i < R; i++) {
+      const int r = tid + BT * i;
+      const double sv = a[i][0] * scale;
+      const double v = (r > I) ? sv : ((r == I) ? 1.0 : 0.0);
+      a[i][0] = (r > I) ? sv : ((r == I) ? beta : a[i][0]);
+#pragma unroll
+      for (int p = 1; p < NB; p++) a[i][p] = fma(-v, cf[p], a[i][p]);
+    }
+    // Rotate left: the finished column moves to the last position.
+#pragma unroll
+    for (int i = 0; i < R; i++) {
+      const double t0 = a[i][0];
+#pragma unroll
+      for (int p = 0; p < NB - 1; p++) a[i][p] = a[i][p + 1];
+      a[i][NB - 1] = t0;
+    }
+  }
+  __syncthreads();
+  if (warp == 1) t_column<NB>(sm, w - 1, lane);
+  __syncthreads();
+  // A leaf narrower than NB needs NB - w more rotations to restore column order.
+#pragma unroll 1
+  for (int k = w; k < NB; k++) {
+#pragma unroll
+    for (int i = 0; i < R; i++) {
+      const double t0 = a[i][0];
+#pragma unroll
+      for (int p = 0; p < NB - 1; p++) a[i][p] = a[i][p + 1];
+      a[i][NB - 1] = t0;
+    }
+  }
+}
+
+// C <- (I - V T V^T)^T C on the tile at C (m rows, w columns, thread-owned
+// rows); v holds the reflectors with the unit diagonal and the zeros above it
+// materialised, T is in sm.T.  C columns are streamed from L2 twice (for
+// W = V^T C and for C -= V (T^T W)) so that only V stays in registers.
+template <int R, int NB>
+BSOFI_DEVINL void apply_qt(const double (&v)[R][NB], double* C, long long ld, int m, int w,
+                           Smem<NB>& sm, double* sC) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int SH = (NB == 16) ? 1 : 2;
+  constexpr int MP = R * BT;  // row stride of the staged tile
+  // Stage the thread's own rows of C (all loads in flight at once).
+#pragma unroll
+  for (int i = 0; i < R; i++) {
+    const int r = tid + BT * i;
+#pragma unroll
+    for (int cc = 0; cc < NB; cc++)
+      sC[cc * MP + r] = (r < m && cc < w) ? __ldcg(C + cm(r, cc, ld)) : 0.0;
+  }
+#pragma unroll 1
+  for (int cc = 0; cc < NB; cc++) {
+    double part[NB];
+#pragma unroll
+    for (int a = 0; a < NB; a++) {
+      double t = 0.0;
+#pragma unroll
+      for (int i = 0; i < R; i++) t = fma(v[i][a], sC[cc * MP + tid + BT * i], t);
+      part[a] = t;
+    }
+    double sum = wsum_t<NB>(part, lane);
+    if ((lane & ((1 << SH) - 1)) == 0) sm.redW[warp][cc][(lane >> SH) & (NB - 1)] = sum;
+  }
+  __syncthreads();
+  for (int e = tid; e < NB * NB; e += BT) {
+    const int a = e % NB, cc = e / NB;
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < BW; k++) acc += sm.redW[k][cc][a];
+    sm.W[a][cc] = acc;
+  }
+  __syncthreads();
+  for (int e = tid; e < NB * NB; e += BT) {
+    const int a = e % NB, cc = e / NB;
+    double acc = 0.0;
+    for (int b = 0; b <= a; b++) acc = fma(sm.T[b][a], sm.W[b][cc], acc);
+    sm.redW[0][cc][a] = acc;
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (int cc = 0; cc < w; cc++) {
+    {
+#pragma unroll
+      for (int i = 0; i < R; i++) {
+        const int r = tid + BT * i;
+        if (r < m) {
+          double acc = 0.0;
+#pragma unroll
+          for (int a = 0; a < NB; a++) acc = fma(v[i][a], sm.redW[0][cc][a], acc);
+          __stcg(C + cm(r, cc, ld), sC[cc * MP + r] - acc);
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// 16-wide block reflector applied with DMMA (mma.sync m16n8k4 f64):
+//   W = V^T C (16 x 16, K = rows split over the 8 warps), W <- -T^T W,
+//   C <- C + V W (rows split over the warps).
+// sV, sC: MP x 20 row-major tiles in shared memory (rows >= m are zero); the
+// caller fills sV, this function stages C.  A stride of 20 doubles makes the
+// fragment loads of both products bank-conflict free.
+constexpr int MS = 20;
+
+template <int R>
+BSOFI_DEVINL void apply_qt_mma(double* sV, double* sC, double* C, long long ld, int m, int w,
+                               Smem<16>& sm) {
+  constexpr int MP = R * BT;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int i = 0; i < R; i++) {
+    const int r = tid + BT * i;
+#pragma unroll
+    for (int cc = 0; cc < 16; cc++)
+      sC[r * MS + cc] = (r < m && cc < w) ? __ldcg(C + cm(r, cc, ld)) : 0.0;
+  }
+  __syncthreads();
+  {  // W partial over this warp's rows
+    double acc[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
+    constexpr int KW = MP / BW;
+    const int r0 = warp * KW;
+#pragma unroll 4
+    for (int k0 = r0; k0 < r0 + KW; k0 += 4) {
+      const double a0 = sV[(k0 + t) * MS + g], a1 = sV[(k0 + t) * MS + g + 8];
+      dmma_16x8x4(acc[0], a0, a1, sC[(k0 + t) * MS + g]);
+      dmma_16x8x4(acc[1], a0, a1, sC[(k0 + t) * MS + 8 + g]);
+    }
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+      sm.redW[warp][g][8 * j + 2 * t] = acc[j][0];
+      sm.redW[warp][g][8 * j + 2 * t + 1] = acc[j][1];
+      sm.redW[warp][g + 8][8 * j + 2 * t] = acc[j][2];
+      sm.redW[warp][g + 8][8 * j + 2 * t + 1] = acc[j][3];
+    }
+  }
+  __syncthreads();
+  {
+    const int a = tid & 15, cc = tid >> 4;
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < BW; k++) acc += sm.redW[k][a][cc];
+    sm.W[a][cc] = acc;
+  }
+  __syncthreads();
+  {  // -(T^T W)
+    const int a = tid & 15, cc = tid >> 4;
+    double acc = 0.0;
+#pragma unroll
+    for (int b = 0; b < 16; b++) acc = fma(sm.T[b][a], sm.W[b][cc], acc);  // T zero below diag
+    sm.redW[0][a][cc] = -acc;
+  }
+  __syncthreads();
+  {  // C += V W over this warp's rows
+    constexpr int RW = MP / BW;
+#pragma unroll 1
+    for (int m0 = warp * RW; m0 < (warp + 1) * RW; m0 += 16) {
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        double acc[4];
+        acc[0] = sC[(m0 + g) * MS + 8 * j + 2 * t];
+        acc[1] = sC[(m0 + g) * MS + 8 * j + 2 * t + 1];
+        acc[2] = sC[(m0 + g + 8) * MS + 8 * j + 2 * t];
+        acc[3] = sC[(m0 + g + 8) * MS + 8 * j + 2 * t + 1];
+#pragma unroll
+        for (int k4 = 0; k4 < 16; k4 += 4)
+          dmma_16x8x4(acc, sV[(m0 + g) * MS + k4 + t], sV[(m0 + g + 8) * MS + k4 + t],
+                      sm.redW[0][k4 + t][8 * j + g]);
+        const int c0 = 8 * j + 2 * t;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int r = m0 + g + 8 * h;
+          if (r < m) {
+            if (c0 < w) __stcg(C + cm(r, c0, ld), acc[2 * h]);
+            if (c0 + 1 < w) __stcg(C + cm(r, c0 + 1, ld), acc[2 * h + 1]);
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Materialise the unit lower trapezoidal V of a factored leaf held in a.
+template <int R, int NB>
+BSOFI_DEVINL void leaf_to_v(const double (&a)[R][NB], double (&v)[R][NB], int m, int w) {
+#pragma unroll
+  for (int i = 0; i < R; i++) {
+    const int r = threadIdx.x + BT * i;
+#pragma unroll
+    for (int c = 0; c < NB; c++)
+      v[i][c] = (c >= w || r >= m) ? 0.0 : (r == c ? 1.0 : (r > c ? a[i][c] : 0.0));
+  }
+}
+
+template <int R, int NB>
+__global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, BsofState st) {
+  __shared__ Smem<NB> sm;
+  extern __shared__ __align__(16) double sC[];  // NB x (R*BT) staged tile
+  const int tid = threadIdx.x;
+  const long long total_tasks = tasks_before(g, g.S);
+
+  if (blockIdx.x == 0) {
+    // ---------------------------------------------------------- panel chain
+    for (int s = 0; s < g.S; s++) {
+      const Leaf f = leaf_of(g, s);
+      int lo, hi;
+      tile_range(g, f.m, f.t, lo, hi);
+      if (tid == 0) st.timeline[4 * s + 0] = gtimer();
+      if (!block_wait_geq(st, st.cnt + tile_id(g, f.m, f.t), hi - lo, &sm.flag)) return;
+      if (tid == 0) st.timeline[4 * s + 1] = gtimer();
+      const int mrows = 2 * g.n - f.j0;
+      double* P = st.A + cm((long long)f.k * g.n + f.j0, (long long)f.m * g.n + f.t * g.NB, st.ld);
+      double a[R][NB];
+      load_rows<R, NB>(a, P, st.ld, mrows, f.w);
+      for (int e = tid; e < NB * (NB + 1); e += BT) (&sm.T[0][0])[e] = 0.0;
+      if (tid < 2 * NB) (&sm.gsh[0][0])[tid] = 0.0;
+      __syncthreads();
+      factor_leaf<R, NB>(a, sm, mrows, f.w, st.tau + (long long)f.k * g.n + f.j0);
+      store_rows<R, NB>(a, P, st.ld, mrows, f.w);
+      __syncthreads();
+      double* Tout = st.T + ((long long)f.k * st.maxleaves + f.l) * 256;
+      for (int e = tid; e < 256; e += BT) {
+        const int rr = e % 16, cc = e / 16;
+        Tout[e] = (rr < NB && cc < NB && rr < f.w && cc < f.w) ? sm.T[rr][cc] : 0.0;
+      }
+      __syncthreads();
+      if (tid == 0) {
+        __threadfence();
+        red_release_add(st.factored + s, 1);
+        st.timeline[4 * s + 2] = gtimer();
+      }
+      // Apply leaf s to the tile of leaf s+1 (target 0).
+      if (ntargets(g, f) > 0) {
+        int m2, t2;
+        target_of(g, f, 0, m2, t2);
+        int lo2, hi2;
+        tile_range(g, m2, t2, lo2, hi2);
+        const int x2 = tile_id(g, m2, t2);
+        if (!block_wait_geq(st, st.cnt + x2, s - lo2, &sm.flag)) return;
+        double v[R][NB];
+        leaf_to_v<R, NB>(a, v, mrows, f.w);
+        double* C = st.A + cm((long long)f.k * g.n + f.j0, (long long)m2 * g.n + t2 * g.NB, st.ld);
+        const int w2 = min(g.NB, g.n - t2 * g.NB);
+        if (tid == 0) st.timeline[4 * s + 3] = gtimer();
+        if constexpr (NB == 16) {
+#pragma unroll
+          for (int i = 0; i < R; i++)
+#pragma unroll
+            for (int c = 0; c < 16; c++) sC[(tid + BT * i) * MS + c] = v[i][c];
+          apply_qt_mma<R>(sC, sC + R * BT * MS, C, st.ld, mrows, w2, sm);
+        } else {
+          apply_qt<R, NB>(v, C, st.ld, mrows, w2, sm, sC);
+        }
+        if (tid == 0) {
+          __threadfence();
+          red_release_add(st.cnt + x2, 1);
+        }
+      }
+    }
+    return;
+  }
+
+  // ------------------------------------------------------------ workers
+  for (;;) {
+    if (tid == 0) sm.task = atomicAdd(st.next_task, 1);
+    __syncthreads();
+    const long long task = sm.task;
+    __syncthreads();
+    if (task >= total_tasks) return;
+    // Leaf of this task: largest s with tasks_before(s) <= task.
+    int lo_s = 0, hi_s = g.S - 1;
+    while (lo_s < hi_s) {
+      const int mid = (lo_s + hi_s + 1) / 2;
+      if (tasks_before(g, mid) <= task) lo_s = mid;
+      else hi_s = mid - 1;
+    }
+    const int s = lo_s;
+    const int q = 1 + (int)(task - tasks_before(g, s));
+    const Leaf f = leaf_of(g, s);
+    int m2, t2;
+    target_of(g, f, q, m2, t2);
+    int lo2, hi2;
+    tile_range(g, m2, t2, lo2, hi2);
+    const int x2 = tile_id(g, m2, t2);
+    if (!block_wait_geq(st, st.factored + s, 1, &sm.flag)) return;
+    const int mrows = 2 * g.n - f.j0;
+    const double* T = st.T + ((long long)f.k * st.maxleaves + f.l) * 256;
+    for (int e = tid; e < NB * NB; e += BT) sm.T[e % NB][e / NB] = __ldcg(T + (e % NB) + 16 * (e / NB));
+    const double* P = st.A + cm((long long)f.k * g.n + f.j0, (long long)f.m * g.n + f.t * g.NB, st.ld);
+    double* C = st.A + cm((long long)f.k * g.n + f.j0, (long long)m2 * g.n + t2 * g.NB, st.ld);
+    const int w2 = min(g.NB, g.n - t2 * g.NB);
+    if constexpr (NB == 16) {
+#pragma unroll
+      for (int i = 0; i < R; i++) {
+        const int r = tid + BT * i;
+#pragma unroll
+        for (int c = 0; c < 16; c++)
+          sC[r * MS + c] = (r >= mrows || c >= f.w) ? 0.0
+                           : (r == c ? 1.0 : (r > c ? __ldcg(P + cm(r, c, st.ld)) : 0.0));
+      }
+      if (!block_wait_geq(st, st.cnt + x2, s - lo2, &sm.flag)) return;
+      apply_qt_mma<R>(sC, sC + R * BT * MS, C, st.ld, mrows, w2, sm);
+    } else {
+      double v[R][NB];
+      {
+        double a[R][NB];
+        load_rows<R, NB>(a, P, st.ld, mrows, f.w);
+        leaf_to_v<R, NB>(a, v, mrows, f.w);
+      }
+      if (!block_wait_geq(st, st.cnt + x2, s - lo2, &sm.flag)) return;
+      apply_qt<R, NB>(v, C, st.ld, mrows, w2, sm, sC);
+    }
+    if (tid == 0) {
+      __threadfence();
+      red_release_add(st.cnt + x2, 1);
+    }
+  }
+}
+
+// ------------------------------------------------------------------ launcher
+// 16-wide leaves keep V and C rows in registers up to 2n = 512 rows; wider
+// panels use 8-wide leaves (up to 2n = 1536 rows, six rows per thread).
+int bsof_leaf_width(int n) { return n <= 256 ? 16 : 8; }
+
+int bsof_tiles(int n) { return (n + bsof_leaf_width(n) - 1) / bsof_leaf_width(n); }
+
+template <int R, int NB>
+static size_t dyn_smem() {
+  return NB == 16 ? sizeof(double) * 2 * (size_t)R * BT * MS : sizeof(double) * (size_t)NB * R * BT;
+}
+
+template <int R, int NB>
+static cudaError_t launch_R(const BsofGeom& g, const BsofState& st, int grid, cudaStream_t s) {
+  void* args[] = {(void*)&g, (void*)&st};
+  return cudaLaunchCooperativeKernel((const void*)bsof_persistent_kernel<R, NB>, dim3(grid),
+                                     dim3(BT), args, dyn_smem<R, NB>(), s);
+}
+
+template <int R, int NB>
+static int max_grid() {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaFuncSetAttribute(bsof_persistent_kernel<R, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)dyn_smem<R, NB>());
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bsof_persistent_kernel<R, NB>, BT,
+                                                dyn_smem<R, NB>());
+  return sms * (per > 0 ? per : 1);
+}
+
+cudaError_t launch_bsof_persistent(double* A, long long ld, int n, int L, double* tau, double* T,
+                                   int maxleaves, int* cnt, int* factored, int* next_task,
+                                   int* err, unsigned long long* timeline, int workers,
+                                   cudaStream_t st) {
+  BsofGeom g;
+  g.n = n;
+  g.L = L;
+  g.NB = bsof_leaf_width(n);
+  g.nl = bsof_tiles(n);
+  g.S = (L - 2) * g.nl + 2 * g.nl;
+  BsofState s;
+  s.A = A;
+  s.ld = ld;
+  s.tau = tau;
+  s.T = T;
+  s.maxleaves = maxleaves;
+  s.cnt = cnt;
+  s.factored = factored;
+  s.next_task = next_task;
+  s.err = err;
+  s.timeline = timeline;
+  s.spin_limit = 1ll << 22;  // polls of ~0.5 us each: a few seconds at most
+  const int R = (2 * n + BT - 1) / BT;
+  int grid = 1 + workers;
+  if (g.NB == 16) {
+    switch (R) {
+      case 1: grid = min(grid, max_grid<1, 16>()); return launch_R<1, 16>(g, s, grid, st);
+      case 2: grid = min(grid, max_grid<2, 16>()); return launch_R<2, 16>(g, s, grid, st);
+      default: return cudaErrorInvalidValue;
+    }
+  }
+  switch (R) {
+    case 3: grid = min(grid, max_grid<3, 8>()); return launch_R<3, 8>(g, s, grid, st);
+    case 4: grid = min(grid, max_grid<4, 8>()); return launch_R<4, 8>(g, s, grid, st);
+    case 5: grid = min(grid, max_grid<5, 8>()); return launch_R<5, 8>(g, s, grid, st);
+    case 6: grid = min(grid, max_grid<6, 8>()); return launch_R<6, 8>(g, s, grid, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace bsofi

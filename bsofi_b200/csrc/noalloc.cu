@@ -60,7 +60,7 @@ bsofi_noalloc_scratch_bytes(void) {
 
 extern "C" __attribute__((visibility("default"))) int bsofi_device_invert_noalloc(
     int n, int L, double* dA, int ldda, double* dtau, int* dinfo, void* stream) {
-  if (n < 1 || n > 1024 || L < 2 || ldda < n * L || dA == nullptr || dtau == nullptr) return -1;
+  if (n < 1 || n > 768 || L < 2 || ldda < n * L || dA == nullptr || dtau == nullptr) return -1;
   if (bsofi_dev_ws_bytes(n, L, ldda) > BSOFI_NOALLOC_SCRATCH_BYTES) return BSOFI_NOALLOC_TOO_LARGE;
   void* ws = nullptr;
   cudaError_t e = scratch_address(&ws);

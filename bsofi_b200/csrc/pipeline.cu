@@ -40,8 +40,8 @@ struct GemmTimer {
 thread_local GemmTimer g_timer;
 
 struct Layout {
-  size_t info, T, G, W, Y, C0, C1, total;
-  int nbw, maxleaves;
+  size_t info, sync, tl, T, G, W, Y, C0, C1, total;
+  int nbw, maxleaves, tiles, leaves, sync_ints;
 };
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
@@ -49,10 +49,17 @@ size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 Layout layout(int n, int L, int ldd) {
   Layout l;
   l.nbw = leaf_width(n);
-  l.maxleaves = (2 * n + l.nbw - 1) / l.nbw;
+  l.tiles = bsof_tiles(n);
+  l.leaves = (L - 2) * l.tiles + 2 * l.tiles;
+  l.maxleaves = max((2 * n + l.nbw - 1) / l.nbw, 2 * l.tiles);
+  l.sync_ints = L * l.tiles + l.leaves + 2;
   size_t off = 0;
-  l.info = off;
+  l.info = off;  // int info, int bsof error word
   off += 256;
+  l.sync = off;  // tile counters, leaf flags, task counter, spare
+  off += align256(sizeof(int) * (size_t)l.sync_ints);
+  l.tl = off;    // BSOF timeline: 4 globaltimer stamps per leaf
+  off += align256(sizeof(unsigned long long) * 4 * (size_t)l.leaves);
   l.T = off;
   off += align256(sizeof(double) * (size_t)(L - 1) * l.maxleaves * 256);
   l.G = off;
@@ -140,32 +147,20 @@ __global__ void __launch_bounds__(256) build_leaf_t_kernel(const double* __restr
   Tout[tid] = sT[tid % 16][tid / 16];
 }
 
+int g_bsof_workers = 32;
+
 int run_bsof(int n, int L, double* dA, int ldd, double* dtau, void* ws, cudaStream_t st) {
   Layout ly = layout(n, L, ldd);
   double* Tb = at<double>(ws, ly.T);
-  for (int k = 0; k <= L - 2; k++) {
-    const int ncp = (k < L - 2) ? n : 2 * n;
-    double* P0 = dA + cm((long long)k * n, (long long)k * n, ldd);
-    for (int l = 0, j0 = 0; j0 < ncp; l++, j0 += ly.nbw) {
-      const int nc = min(ly.nbw, ncp - j0), m = 2 * n - j0;
-      double* P = P0 + cm(j0, j0, ldd);
-      double* T = Tb + ((size_t)k * ly.maxleaves + l) * 256;
-      CK(launch_panel_leaf(P, ldd, m, nc, dtau + (size_t)k * n + j0, T, ly.nbw, st));
-      WyArgs a = {};
-      a.V = P;
-      a.ldv = ldd;
-      a.T = T;
-      a.m = m;
-      a.nb = nc;
-      a.trans = 1;
-      a.seg[0] = {P0 + cm(j0, j0 + nc, ldd), ldd, 0, ncp - j0 - nc};
-      if (k < L - 2) {
-        a.seg[1] = {dA + cm((long long)k * n + j0, (long long)(k + 1) * n, ldd), ldd, 0, n};
-        a.seg[2] = {dA + cm((long long)k * n + j0, (long long)(L - 1) * n, ldd), ldd, 0, n};
-      }
-      CK(launch_wy_apply(a, 1, st));
-    }
-  }
+  int* sync = at<int>(ws, ly.sync);
+  CKM(cudaMemsetAsync(sync, 0, sizeof(int) * ly.sync_ints, st));
+  CKM(cudaMemsetAsync(at<int>(ws, ly.info) + 1, 0, sizeof(int), st));
+  // 16-wide leaves apply with DMMA and need few workers; 8-wide leaves
+  // (n > 256) have three times the tasks per leaf and use every SM.
+  const int workers = bsof_leaf_width(n) == 16 ? g_bsof_workers : 4 * g_bsof_workers;
+  CK(launch_bsof_persistent(dA, ldd, n, L, dtau, Tb, ly.maxleaves, sync, sync + L * ly.tiles,
+                            sync + L * ly.tiles + ly.leaves, at<int>(ws, ly.info) + 1,
+                            at<unsigned long long>(ws, ly.tl), workers, st));
   return 0;
 }
 
@@ -382,6 +377,14 @@ int bsofi_dev_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* 
 }
 
 int* bsofi_dev_info_ptr(void* dws) { return at<int>(dws, 0); }
+
+int bsofi_dev_bsof_timeline(int n, int L, int ldd, void* dws, unsigned long long** ptr) {
+  Layout ly = layout(n, L, ldd);
+  *ptr = at<unsigned long long>(dws, ly.tl);
+  return ly.leaves;
+}
+
+void bsofi_dev_set_bsof_workers(int w) { g_bsof_workers = w > 0 ? w : 32; }
 
 int bsofi_dev_selftest_gemm(int M, int N, int K, double alpha, const double* dA, int lda,
                             int upper_a, const double* dB, int ldb, int upper_b, double beta,

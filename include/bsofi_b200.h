@@ -40,7 +40,7 @@ extern "C" {
 #endif
 
 #define BSOFI_INFO_CUDA (-1000)
-#define BSOFI_MAX_BLOCK 1024 /* largest supported block size n */
+#define BSOFI_MAX_BLOCK 768 /* largest supported block size n */
 
 /* ------------------------------------------------------------------------
  * Fortran handle API (primary drop-in).  `handle` is the caller's
@@ -188,6 +188,16 @@ int bsofi_device_invert_noalloc(int n, int L, double *dA, int ldda, double *dtau
  * the record. */
 void bsofi_device_timing(int on);
 int bsofi_device_timing_read(double *ms, long long *launches);
+
+/* Diagnostics (no reference counterpart): the BSOF timeline of the last
+ * factorization that used `dwork` -- four globaltimer stamps (ns) per leaf
+ * from the CTA that runs the critical chain: loop start, tile ready, leaf
+ * published, next-tile update start.  Copies up to max_leaves leaves to host
+ * and returns the number copied.  set_bsof_workers sets the number of worker
+ * CTAs of the persistent BSOF kernel (default 32) for this process. */
+int bsofi_device_bsof_timeline(int n, int L, int ldda, void *dwork, unsigned long long *host,
+                               int max_leaves);
+void bsofi_device_set_bsof_workers(int workers);
 
 /* Diagnostic entry point (no reference counterpart): one call of the FP64
  * DMMA tile engine, C = alpha*A*B + beta*C on device memory (column-major),

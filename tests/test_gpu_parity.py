@@ -41,8 +41,8 @@ def test_handle_api_matches_golden(cuda_device, case):
 
 
 @pytest.mark.parametrize("n,L", [(1, 2), (1, 7), (2, 2), (3, 3), (5, 4), (8, 16), (17, 5),
-                                 (33, 3), (31, 9), (64, 4), (100, 3), (129, 2), (300, 3),
-                                 (520, 2)])
+                                 (33, 3), (31, 9), (64, 4), (100, 3), (129, 2), (255, 4),
+                                 (257, 3), (300, 3), (400, 3), (520, 2), (700, 2)])
 def test_random_pcyclic_vs_oracle(cuda_device, n, L):
     M = random_pcyclic(n, L, seed=n * 100 + L)
     Ar, taur, infor = oracle.port_bsoftri(M, n, L)
