@@ -548,13 +548,9 @@ int bsofi_device_bsoi(int n, int L, double *dA, int ldda, const double *dtau, vo
 
 int bsofi_device_invert(int n, int L, double *dA, int ldda, double *dtau, void *dwork,
                         void *stream) {
-  long long c;
-  int e = bsofi_device_bsoftri(n, L, dA, ldda, dtau, dwork, stream);
-  if (e) return e;
-  c = bsofi_dev_launch_count();
-  e = bsofi_device_bsoi(n, L, dA, ldda, dtau, dwork, stream);
-  bsofi_dev_add_launches(c);
-  return e;
+  int e = bsofi_dev_prepare();
+  if (!e) e = bsofi_dev_invert(n, L, dA, ldda, dtau, dwork, stream);
+  return e ? cuda_info((cudaError_t)e) : 0;
 }
 
 int *bsofi_device_info(void *dwork) { return bsofi_dev_info_ptr(dwork); }

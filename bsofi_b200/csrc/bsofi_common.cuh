@@ -43,6 +43,17 @@ BSOFI_DEVINL void dmma_16x8x4(double (&d)[4], double a0, double a1, double b0) {
       : "d"(a0), "d"(a1), "d"(b0));
 }
 
+// D = A(16x8, row) * B(8x8, col) + D.  a0 = A[g][t], a1 = A[g+8][t],
+// a2 = A[g][t+4], a3 = A[g+8][t+4]; b0 = B[t][g], b1 = B[t+4][g]; D as above.
+BSOFI_DEVINL void dmma_16x8x8(double (&d)[4], double a0, double a1, double a2, double a3,
+                              double b0, double b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 "
+      "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
+}
+
 // ---------------------------------------------------------------- warp sums
 BSOFI_DEVINL double warp_sum(double v) {
 #pragma unroll

@@ -23,14 +23,16 @@ struct WyArgs {
 int leaf_width(int n);
 cudaError_t launch_wy_apply(const WyArgs& a, int batch, cudaStream_t st);
 
-// Persistent BSOF (kernels_bsof.cu).  cnt: L*tiles ints, factored: leaves
-// ints, next_task and err: one int each, all zeroed before the launch.
+// Persistent BSOF (kernels_bsof.cu).  cnt: (L + 2(L-1))*tiles ints,
+// factored: leaves ints, next_task and err: one int each, all zeroed before
+// the launch.  G (optional): (L-1) x (2n)^2 identity matrices that become
+// Q_k^T.
 int bsof_leaf_width(int n);
 int bsof_tiles(int n);
 cudaError_t launch_bsof_persistent(double* A, long long ld, int n, int L, double* tau, double* T,
-                                   int maxleaves, int* cnt, int* factored, int* next_task,
-                                   int* err, unsigned long long* timeline, int workers,
-                                   cudaStream_t st);
+                                   double* G, int maxleaves, int* cnt, int* factored,
+                                   int* next_task, int* err, unsigned long long* timeline,
+                                   int workers, cudaStream_t st);
 
 cudaError_t launch_trtri_blocks(double* A, long long ld, int n, long long bstride,
                                 int nblk, int* info, cudaStream_t st);

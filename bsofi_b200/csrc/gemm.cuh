@@ -1,7 +1,7 @@
 // FP64 tensor-core tile engine for the BSOF/I contractions (sm_100a).
 //
 // C = alpha * A * B + beta * C, column-major, strided batch, computed with
-// DMMA (mma.sync m16n8k4 f64; tcgen05 has no FP64 kind).  Operands are staged
+// DMMA (mma.sync m16n8k8 f64; tcgen05 has no FP64 kind).  Operands are staged
 // in shared memory by cp.async with hardware zero-fill, which also applies the
 // structural masks of the block p-cyclic algorithm for free:
 //   * A is split along K into two segments with their own base pointers
@@ -218,19 +218,25 @@ BSOFI_DEVINL void gemm_tile(const GemmDims& d, const GemmA& a, const GemmB& b,
     const double* tA = sA + (it % Cfg::STAGES) * Cfg::A_STAGE + wm * Cfg::WTM + g;
     const double* tB = sB + (it % Cfg::STAGES) * Cfg::B_STAGE + (wn * Cfg::WTN + g) * Cfg::SB + t;
 #pragma unroll
-    for (int k4 = 0; k4 < Cfg::BK / 4; k4++) {
-      double af[Cfg::MT][2], bf[Cfg::NT];
+    for (int k8 = 0; k8 < Cfg::BK / 8; k8++) {
+      double af[Cfg::MT][4], bf[Cfg::NT][2];
 #pragma unroll
       for (int i = 0; i < Cfg::MT; i++) {
-        af[i][0] = tA[(k4 * 4 + t) * Cfg::SA + i * 16];
-        af[i][1] = tA[(k4 * 4 + t) * Cfg::SA + i * 16 + 8];
+        af[i][0] = tA[(k8 * 8 + t) * Cfg::SA + i * 16];
+        af[i][1] = tA[(k8 * 8 + t) * Cfg::SA + i * 16 + 8];
+        af[i][2] = tA[(k8 * 8 + t + 4) * Cfg::SA + i * 16];
+        af[i][3] = tA[(k8 * 8 + t + 4) * Cfg::SA + i * 16 + 8];
       }
 #pragma unroll
-      for (int j = 0; j < Cfg::NT; j++) bf[j] = tB[j * 8 * Cfg::SB + k4 * 4];
+      for (int j = 0; j < Cfg::NT; j++) {
+        bf[j][0] = tB[j * 8 * Cfg::SB + k8 * 8];
+        bf[j][1] = tB[j * 8 * Cfg::SB + k8 * 8 + 4];
+      }
 #pragma unroll
       for (int i = 0; i < Cfg::MT; i++)
 #pragma unroll
-        for (int j = 0; j < Cfg::NT; j++) dmma_16x8x4(acc[i][j], af[i][0], af[i][1], bf[j]);
+        for (int j = 0; j < Cfg::NT; j++)
+          dmma_16x8x8(acc[i][j], af[i][0], af[i][1], af[i][2], af[i][3], bf[j][0], bf[j][1]);
     }
   }
   cp_async_wait<0>();

@@ -34,6 +34,7 @@ constexpr int BW = BT / 32;
 
 struct BsofGeom {
   int n, L, NB, nl, S;
+  int form_g;  // 1: leaves also update G_k = Q_k^T (identity-initialised by the caller)
 };
 
 // Leaf s -> panel k, leaf index l in the panel, tile (m, t), panel column j0.
@@ -70,6 +71,12 @@ BSOFI_DEVINL Leaf leaf_of(const BsofGeom& g, int s) {
 BSOFI_DEVINL int tile_id(const BsofGeom& g, int m, int t) { return m * g.nl + t; }
 
 BSOFI_DEVINL void tile_range(const BsofGeom& g, int m, int t, int& lo, int& hi) {
+  if (m >= g.L) {  // G_k tile: every leaf of panel k, in order
+    const int k = (m - g.L) / 2;
+    lo = k * g.nl;
+    hi = lo + (k <= g.L - 3 ? g.nl : 2 * g.nl);
+    return;
+  }
   if (m <= g.L - 2) {
     lo = max(0, (m - 1) * g.nl);
     hi = m * g.nl + t;
@@ -79,13 +86,23 @@ BSOFI_DEVINL void tile_range(const BsofGeom& g, int m, int t, int& lo, int& hi) 
   }
 }
 
-// Number of targets of leaf s; target q (0 = tile of leaf s+1).
+// Number of targets of leaf s; target q (0 = tile of leaf s+1).  With
+// form_g the 2*nl column tiles of G_k follow the matrix targets; they are
+// reported as block columns m = L + 2k + h (h = 0, 1) of a virtual matrix.
 BSOFI_DEVINL int ntargets(const BsofGeom& g, const Leaf& f) {
-  if (f.k <= g.L - 3) return (g.nl - 1 - f.l) + 2 * g.nl;
-  return 2 * g.nl - 1 - f.l;
+  const int gt = g.form_g ? 2 * g.nl : 0;
+  if (f.k <= g.L - 3) return (g.nl - 1 - f.l) + 2 * g.nl + gt;
+  return 2 * g.nl - 1 - f.l + gt;
 }
 
 BSOFI_DEVINL void target_of(const BsofGeom& g, const Leaf& f, int q, int& m, int& t) {
+  const int nmat = (f.k <= g.L - 3) ? (g.nl - 1 - f.l) + 2 * g.nl : 2 * g.nl - 1 - f.l;
+  if (q >= nmat) {
+    const int u = q - nmat;
+    m = g.L + 2 * f.k + u / g.nl;
+    t = u % g.nl;
+    return;
+  }
   if (f.k <= g.L - 3) {
     const int np = g.nl - 1 - f.l;
     if (q < np) {
@@ -113,22 +130,38 @@ BSOFI_DEVINL void target_of(const BsofGeom& g, const Leaf& f, int q, int& m, int
 // Worker tasks before leaf s (each leaf contributes ntargets - 1 tasks).
 BSOFI_DEVINL long long tasks_before(const BsofGeom& g, int s) {
   const int reg = (g.L - 2) * g.nl;
-  const long long nl = g.nl;
-  const long long per_reg_leaf0 = 3 * nl - 2;  // tasks of regular leaf l: 3nl - 2 - l
+  const long long nl = g.nl, gt = g.form_g ? 2 * nl : 0;
+  const long long per_reg_leaf0 = 3 * nl - 2 + gt;  // tasks of regular leaf l: 3nl - 2 - l + gt
   const long long per_panel = nl * per_reg_leaf0 - nl * (nl - 1) / 2;
   if (s <= reg) {
     long long k = s / g.nl, l = s % g.nl;
     return k * per_panel + l * per_reg_leaf0 - l * (l - 1) / 2;
   }
   long long base = (long long)(g.L - 2) * per_panel;
-  long long l = s - reg;  // final leaf l has max(2nl - 2 - l, 0) tasks
+  long long l = s - reg;  // final leaf l has max(2nl - 2 - l + gt, 0) tasks
+  if (gt > 0) return base + l * (2 * nl - 2 + gt) - l * (l - 1) / 2;
   long long full = min(l, 2 * nl - 1);
   return base + full * (2 * nl - 2) - full * (full - 1) / 2;
+}
+
+// Column tile (m, t) of the matrix, or of G_k for m >= L: base pointer at the
+// leaf's first row j0 of its panel, and leading dimension.
+BSOFI_DEVINL double* tile_ptr(const BsofGeom& g, double* A, long long ld, double* G, int k, int j0,
+                              int m, int t, long long& ldt) {
+  if (m >= g.L) {
+    const int kk = (m - g.L) / 2, h = (m - g.L) % 2;
+    const long long n2 = 2ll * g.n;
+    ldt = n2;
+    return G + (long long)kk * n2 * n2 + cm(j0, (long long)h * g.n + t * g.NB, n2);
+  }
+  ldt = ld;
+  return A + cm((long long)k * g.n + j0, (long long)m * g.n + t * g.NB, ld);
 }
 
 struct BsofState {
   double* A;
   long long ld;
+  double* G;  // (L-1) x (2n)^2, used when form_g
   double* tau;
   double* T;  // 256 doubles per leaf: (k * maxleaves + l) * 256
   int maxleaves;
@@ -592,7 +625,8 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
         if (!block_wait_geq(st, st.cnt + x2, s - lo2, &sm.flag)) return;
         double v[R][NB];
         leaf_to_v<R, NB>(a, v, mrows, f.w);
-        double* C = st.A + cm((long long)f.k * g.n + f.j0, (long long)m2 * g.n + t2 * g.NB, st.ld);
+        long long ldc;
+        double* C = tile_ptr(g, st.A, st.ld, st.G, f.k, f.j0, m2, t2, ldc);
         const int w2 = min(g.NB, g.n - t2 * g.NB);
         if (tid == 0) st.timeline[4 * s + 3] = gtimer();
         if constexpr (NB == 16) {
@@ -600,9 +634,9 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
           for (int i = 0; i < R; i++)
 #pragma unroll
             for (int c = 0; c < 16; c++) sC[(tid + BT * i) * MS + c] = v[i][c];
-          apply_qt_mma<R>(sC, sC + R * BT * MS, C, st.ld, mrows, w2, sm);
+          apply_qt_mma<R>(sC, sC + R * BT * MS, C, ldc, mrows, w2, sm);
         } else {
-          apply_qt<R, NB>(v, C, st.ld, mrows, w2, sm, sC);
+          apply_qt<R, NB>(v, C, ldc, mrows, w2, sm, sC);
         }
         if (tid == 0) {
           __threadfence();
@@ -640,7 +674,8 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
     const double* T = st.T + ((long long)f.k * st.maxleaves + f.l) * 256;
     for (int e = tid; e < NB * NB; e += BT) sm.T[e % NB][e / NB] = __ldcg(T + (e % NB) + 16 * (e / NB));
     const double* P = st.A + cm((long long)f.k * g.n + f.j0, (long long)f.m * g.n + f.t * g.NB, st.ld);
-    double* C = st.A + cm((long long)f.k * g.n + f.j0, (long long)m2 * g.n + t2 * g.NB, st.ld);
+    long long ldc;
+    double* C = tile_ptr(g, st.A, st.ld, st.G, f.k, f.j0, m2, t2, ldc);
     const int w2 = min(g.NB, g.n - t2 * g.NB);
     if constexpr (NB == 16) {
 #pragma unroll
@@ -652,7 +687,7 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
                            : (r == c ? 1.0 : (r > c ? __ldcg(P + cm(r, c, st.ld)) : 0.0));
       }
       if (!block_wait_geq(st, st.cnt + x2, s - lo2, &sm.flag)) return;
-      apply_qt_mma<R>(sC, sC + R * BT * MS, C, st.ld, mrows, w2, sm);
+      apply_qt_mma<R>(sC, sC + R * BT * MS, C, ldc, mrows, w2, sm);
     } else {
       double v[R][NB];
       {
@@ -661,7 +696,7 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
         leaf_to_v<R, NB>(a, v, mrows, f.w);
       }
       if (!block_wait_geq(st, st.cnt + x2, s - lo2, &sm.flag)) return;
-      apply_qt<R, NB>(v, C, st.ld, mrows, w2, sm, sC);
+      apply_qt<R, NB>(v, C, ldc, mrows, w2, sm, sC);
     }
     if (tid == 0) {
       __threadfence();
@@ -702,10 +737,11 @@ static int max_grid() {
 }
 
 cudaError_t launch_bsof_persistent(double* A, long long ld, int n, int L, double* tau, double* T,
-                                   int maxleaves, int* cnt, int* factored, int* next_task,
-                                   int* err, unsigned long long* timeline, int workers,
-                                   cudaStream_t st) {
+                                   double* G, int maxleaves, int* cnt, int* factored,
+                                   int* next_task, int* err, unsigned long long* timeline,
+                                   int workers, cudaStream_t st) {
   BsofGeom g;
+  g.form_g = G != nullptr;
   g.n = n;
   g.L = L;
   g.NB = bsof_leaf_width(n);
@@ -714,6 +750,7 @@ cudaError_t launch_bsof_persistent(double* A, long long ld, int n, int L, double
   BsofState s;
   s.A = A;
   s.ld = ld;
+  s.G = G;
   s.tau = tau;
   s.T = T;
   s.maxleaves = maxleaves;

@@ -52,7 +52,7 @@ Layout layout(int n, int L, int ldd) {
   l.tiles = bsof_tiles(n);
   l.leaves = (L - 2) * l.tiles + 2 * l.tiles;
   l.maxleaves = max((2 * n + l.nbw - 1) / l.nbw, 2 * l.tiles);
-  l.sync_ints = L * l.tiles + l.leaves + 2;
+  l.sync_ints = (L + 2 * (L - 1)) * l.tiles + l.leaves + 2;
   size_t off = 0;
   l.info = off;  // int info, int bsof error word
   off += 256;
@@ -149,17 +149,23 @@ __global__ void __launch_bounds__(256) build_leaf_t_kernel(const double* __restr
 
 int g_bsof_workers = 32;
 
-int run_bsof(int n, int L, double* dA, int ldd, double* dtau, void* ws, cudaStream_t st) {
+// BSOF.  form_q: the persistent kernel also forms G_k = Q_k^T for BSOI.
+int run_bsof(int n, int L, double* dA, int ldd, double* dtau, void* ws, cudaStream_t st,
+             bool form_q) {
   Layout ly = layout(n, L, ldd);
   double* Tb = at<double>(ws, ly.T);
+  double* G = at<double>(ws, ly.G);
   int* sync = at<int>(ws, ly.sync);
+  const int ntiles = (L + 2 * (L - 1)) * ly.tiles;
   CKM(cudaMemsetAsync(sync, 0, sizeof(int) * ly.sync_ints, st));
   CKM(cudaMemsetAsync(at<int>(ws, ly.info) + 1, 0, sizeof(int), st));
+  if (form_q) CK(launch_set_identity(G, 2 * n, 2 * n, 4ll * n * n, L - 1, st));
   // 16-wide leaves apply with DMMA and need few workers; 8-wide leaves
   // (n > 256) have three times the tasks per leaf and use every SM.
-  const int workers = bsof_leaf_width(n) == 16 ? g_bsof_workers : 4 * g_bsof_workers;
-  CK(launch_bsof_persistent(dA, ldd, n, L, dtau, Tb, ly.maxleaves, sync, sync + L * ly.tiles,
-                            sync + L * ly.tiles + ly.leaves, at<int>(ws, ly.info) + 1,
+  int workers = bsof_leaf_width(n) == 16 ? g_bsof_workers : 4 * g_bsof_workers;
+  if (form_q) workers *= 2;
+  CK(launch_bsof_persistent(dA, ldd, n, L, dtau, Tb, form_q ? G : nullptr, ly.maxleaves, sync,
+                            sync + ntiles, sync + ntiles + ly.leaves, at<int>(ws, ly.info) + 1,
                             at<unsigned long long>(ws, ly.tl), workers, st));
   return 0;
 }
@@ -268,7 +274,8 @@ int run_bstri(int n, int L, double* dA, int ldd, void* ws, cudaStream_t st) {
   return 0;
 }
 
-int run_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* ws, cudaStream_t st) {
+int run_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* ws, cudaStream_t st,
+             bool q_ready) {
   Layout ly = layout(n, L, ldd);
   double* Tb = at<double>(ws, ly.T);
   double* G = at<double>(ws, ly.G);
@@ -276,7 +283,9 @@ int run_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* ws, cu
   const int N = n * L, n2 = 2 * n;
   const long long g2 = (long long)n2 * n2;
 
-  // Compact-WY factors from the stored reflectors, then G_k = Q_k^T.
+  // Compact-WY factors from the stored reflectors, then G_k = Q_k^T (unless
+  // the factorization already formed G_k).
+  if (!q_ready) {
   build_leaf_t_kernel<<<dim3(ly.maxleaves, L - 1), 256, 0, st>>>(dA, ldd, n, L, dtau, Tb,
                                                                   ly.maxleaves, ly.nbw);
   CK(cudaGetLastError());
@@ -300,6 +309,7 @@ int run_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* ws, cu
       a.seg[0] = {G + (size_t)k0 * g2 + j0, n2, g2, n2};
       CK(launch_wy_apply(a, batch, st));
     }
+  }
   }
 
   // Carry for the first step: X(:, L-1) with the triangular diagonal block.
@@ -351,7 +361,7 @@ int bsofi_dev_zero_structural(int n, int L, double* dA, int ldd, void* stream) {
 
 int bsofi_dev_bsof(int n, int L, double* dA, int ldd, double* dtau, void* dws, void* stream) {
   g_launches = 0;
-  return run_bsof(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream);
+  return run_bsof(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, false);
 }
 
 int bsofi_dev_bstri(int n, int L, double* dA, int ldd, void* dws, void* stream) {
@@ -362,18 +372,23 @@ int bsofi_dev_bstri(int n, int L, double* dA, int ldd, void* dws, void* stream) 
 int bsofi_dev_bsoftri(int n, int L, double* dA, int ldd, double* dtau, void* dws,
                       void* stream) {
   g_launches = 0;
-  int e = run_bsof(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream);
+  int e = run_bsof(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, false);
   if (e) return e;
-  long long c = g_launches;
-  e = run_bstri(n, L, dA, ldd, dws, (cudaStream_t)stream);
-  g_launches += c;
-  return e;
+  return run_bstri(n, L, dA, ldd, dws, (cudaStream_t)stream);
 }
 
 int bsofi_dev_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* dws,
                    void* stream) {
   g_launches = 0;
-  return run_bsoi(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream);
+  return run_bsoi(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, false);
+}
+
+int bsofi_dev_invert(int n, int L, double* dA, int ldd, double* dtau, void* dws, void* stream) {
+  g_launches = 0;
+  int e = run_bsof(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, true);
+  if (!e) e = run_bstri(n, L, dA, ldd, dws, (cudaStream_t)stream);
+  if (!e) e = run_bsoi(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, true);
+  return e;
 }
 
 int* bsofi_dev_info_ptr(void* dws) { return at<int>(dws, 0); }
