@@ -215,6 +215,9 @@ BSOFI_DEVINL bool block_wait_geq(const BsofState& st, const int* p, int target, 
   return ok;
 }
 
+// Barrier among the first `count` threads of the CTA (id 1; id 0 is __syncthreads).
+BSOFI_DEVINL void named_bar(int count) { asm volatile("bar.sync 1, %0;" ::"r"(count) : "memory"); }
+
 // Sum NB values per lane over a warp (transpose reduction): lane l ends with
 // the warp sum of value (l >> (5 - log2 NB)) & (NB - 1).
 template <int NB>
@@ -305,10 +308,15 @@ BSOFI_DEVINL void t_column(Smem<NB>& sm, int I, int lane) {
 // product d_c = sum_{r>I} a_rI a_rc with a pending column (position 0 gives
 // ||x||^2) or e_j = sum_{r>I} v_j[r] a_rI with a finished reflector, which
 // builds the dlarft factor T(0:I,I) = -tau_I T(0:I,0:I) V^T v_I.
-template <int R, int NB>
+template <int R, int NB, int FW>
 BSOFI_DEVINL void factor_leaf(double (&a)[R][NB], Smem<NB>& sm, int m, int w, double* tau_out) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int SH = (NB == 16) ? 1 : 2;
+  constexpr int FT = FW * 32;  // threads taking part; thread t owns rows t + FT*i
+  auto bar = [&]() {
+    if constexpr (FW == BW) __syncthreads();
+    else named_bar(FT);
+  };
 #pragma unroll 1
   for (int I = 0; I < w; I++) {
     const int buf = I & 1;
@@ -322,7 +330,7 @@ BSOFI_DEVINL void factor_leaf(double (&a)[R][NB], Smem<NB>& sm, int m, int w, do
     for (int p = 0; p < NB; p++) part[p] = 0.0;
 #pragma unroll
     for (int i = 0; i < R; i++) {
-      const int r = tid + BT * i;
+      const int r = tid + FT * i;
       const double x = (r > I) ? a[i][0] : 0.0;  // rows >= m hold zeros
 #pragma unroll
       for (int p = 0; p < NB; p++) part[p] = fma(x, a[i][p], part[p]);
@@ -331,12 +339,12 @@ BSOFI_DEVINL void factor_leaf(double (&a)[R][NB], Smem<NB>& sm, int m, int w, do
       double sum = wsum_t<NB>(part, lane);
       if ((lane & ((1 << SH) - 1)) == 0) sm.red[buf][warp][(lane >> SH) & (NB - 1)] = sum;
     }
-    __syncthreads();
+    bar();
     if (warp == 0) {
       const int slot = lane % NB;
       double tot = 0.0;
 #pragma unroll
-      for (int k = lane / NB; k < BW; k += 32 / NB) tot += sm.red[buf][k][slot];
+      for (int k = lane / NB; k < FW; k += 32 / NB) tot += sm.red[buf][k][slot];
 #pragma unroll
       for (int off = NB; off < 32; off <<= 1) tot += __shfl_xor_sync(0xffffffffu, tot, off);
       const double xnorm2 = __shfl_sync(0xffffffffu, tot, 0);
@@ -374,7 +382,7 @@ BSOFI_DEVINL void factor_leaf(double (&a)[R][NB], Smem<NB>& sm, int m, int w, do
       }
     }
     if (warp == 1 && I > 0) t_column<NB>(sm, I - 1, lane);
-    __syncthreads();
+    bar();
     const double taui = sm.coef[buf][NB], scale = sm.coef[buf][NB + 1],
                  beta = sm.coef[buf][NB + 2];
     double cf[NB];
@@ -382,7 +390,7 @@ BSOFI_DEVINL void factor_leaf(double (&a)[R][NB], Smem<NB>& sm, int m, int w, do
     for (int p = 1; p < NB; p++) cf[p] = sm.coef[buf][p];
 #pragma unroll
     for (int i = 0; i < R; i++) {
-      const int r = tid + BT * i;
+      const int r = tid + FT * i;
       const double sv = a[i][0] * scale;
       const double v = (r > I) ? sv : ((r == I) ? 1.0 : 0.0);
       a[i][0] = (r > I) ? sv : ((r == I) ? beta : a[i][0]);
@@ -398,9 +406,9 @@ BSOFI_DEVINL void factor_leaf(double (&a)[R][NB], Smem<NB>& sm, int m, int w, do
       a[i][NB - 1] = t0;
     }
   }
-  __syncthreads();
+  bar();
   if (warp == 1) t_column<NB>(sm, w - 1, lane);
-  __syncthreads();
+  bar();
   // A leaf narrower than NB needs NB - w more rotations to restore column order.
 #pragma unroll 1
   for (int k = w; k < NB; k++) {
@@ -596,13 +604,43 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
       if (tid == 0) st.timeline[4 * s + 1] = gtimer();
       const int mrows = 2 * g.n - f.j0;
       double* P = st.A + cm((long long)f.k * g.n + f.j0, (long long)f.m * g.n + f.t * g.NB, st.ld);
-      double a[R][NB];
-      load_rows<R, NB>(a, P, st.ld, mrows, f.w);
       for (int e = tid; e < NB * (NB + 1); e += BT) (&sm.T[0][0])[e] = 0.0;
       if (tid < 2 * NB) (&sm.gsh[0][0])[tid] = 0.0;
       __syncthreads();
-      factor_leaf<R, NB>(a, sm, mrows, f.w, st.tau + (long long)f.k * g.n + f.j0);
-      store_rows<R, NB>(a, P, st.ld, mrows, f.w);
+      // 16-wide leaves are factored by 4 warps with 2R rows per thread (the
+      // per-column shuffle reduction costs per warp); the other warps wait.
+      constexpr int FW = (NB == 16) ? 4 : BW;
+      constexpr int FR = R * BW / FW;
+      double a[FR][NB];
+      if (tid < FW * 32) {
+#pragma unroll
+        for (int i = 0; i < FR; i++) {
+          const int r = tid + FW * 32 * i;
+#pragma unroll
+          for (int c = 0; c < NB; c++)
+            a[i][c] = (r < mrows && c < f.w) ? __ldcg(P + cm(r, c, st.ld)) : 0.0;
+        }
+        factor_leaf<FR, NB, FW>(a, sm, mrows, f.w, st.tau + (long long)f.k * g.n + f.j0);
+#pragma unroll
+        for (int i = 0; i < FR; i++) {
+          const int r = tid + FW * 32 * i;
+          if (r < mrows) {
+#pragma unroll
+            for (int c = 0; c < NB; c++)
+              if (c < f.w) __stcg(P + cm(r, c, st.ld), a[i][c]);
+            if constexpr (NB == 16) {  // reflectors for the next-tile update
+#pragma unroll
+              for (int c = 0; c < 16; c++)
+                sC[r * MS + c] = (c >= f.w) ? 0.0 : (r == c ? 1.0 : (r > c ? a[i][c] : 0.0));
+            }
+          } else if constexpr (NB == 16) {
+            if (r < R * BT) {
+#pragma unroll
+              for (int c = 0; c < 16; c++) sC[r * MS + c] = 0.0;
+            }
+          }
+        }
+      }
       __syncthreads();
       double* Tout = st.T + ((long long)f.k * st.maxleaves + f.l) * 256;
       for (int e = tid; e < 256; e += BT) {
@@ -623,19 +661,15 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
         tile_range(g, m2, t2, lo2, hi2);
         const int x2 = tile_id(g, m2, t2);
         if (!block_wait_geq(st, st.cnt + x2, s - lo2, &sm.flag)) return;
-        double v[R][NB];
-        leaf_to_v<R, NB>(a, v, mrows, f.w);
         long long ldc;
         double* C = tile_ptr(g, st.A, st.ld, st.G, f.k, f.j0, m2, t2, ldc);
         const int w2 = min(g.NB, g.n - t2 * g.NB);
         if (tid == 0) st.timeline[4 * s + 3] = gtimer();
         if constexpr (NB == 16) {
-#pragma unroll
-          for (int i = 0; i < R; i++)
-#pragma unroll
-            for (int c = 0; c < 16; c++) sC[(tid + BT * i) * MS + c] = v[i][c];
           apply_qt_mma<R>(sC, sC + R * BT * MS, C, ldc, mrows, w2, sm);
         } else {
+          double v[R][NB];
+          leaf_to_v<R, NB>(a, v, mrows, f.w);
           apply_qt<R, NB>(v, C, ldc, mrows, w2, sm, sC);
         }
         if (tid == 0) {
