@@ -57,6 +57,9 @@ _SIGS = {
                                          _vp, _vp]),
     "bsofi_device_info": (_vp, [_vp]),
     "bsofi_device_last_launches": (ctypes.c_longlong, []),
+    "bsofi_batch_workspace_bytes": (ctypes.c_ulonglong, [ctypes.c_int, _vp, _vp, _vp]),
+    "bsofi_device_invert_batched": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp,
+                                                   ctypes.c_int, _vp]),
     "bsofi_noalloc_scratch_bytes": (ctypes.c_ulonglong, []),
     "bsofi_device_invert_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int,
                                                    _vp, _vp, _vp]),

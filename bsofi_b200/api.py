@@ -147,3 +147,25 @@ def timing_read():
     if rc != 0:
         raise RuntimeError("bsofi_device_timing_read failed (%d)" % rc)
     return ms.value, cnt.value
+
+
+def batch_workspace_bytes(ns, Ls, lddas):
+    import numpy as _np
+    n = _np.ascontiguousarray(ns, dtype=_np.int32)
+    L = _np.ascontiguousarray(Ls, dtype=_np.int32)
+    ld = _np.ascontiguousarray(lddas, dtype=_np.int32)
+    return int(load().bsofi_batch_workspace_bytes(len(n), n.ctypes.data, L.ctypes.data,
+                                                  ld.ctypes.data))
+
+
+def device_invert_batched(ns, Ls, dAs, lddas, dtaus, dwork, streams=8, stream=0):
+    """bsofi_device_invert_batched on raw device pointers; asynchronous."""
+    import numpy as _np
+    n = _np.ascontiguousarray(ns, dtype=_np.int32)
+    L = _np.ascontiguousarray(Ls, dtype=_np.int32)
+    ld = _np.ascontiguousarray(lddas, dtype=_np.int32)
+    pa = _np.ascontiguousarray(dAs, dtype=_np.uint64)
+    pt = _np.ascontiguousarray(dtaus, dtype=_np.uint64)
+    return load().bsofi_device_invert_batched(len(n), n.ctypes.data, L.ctypes.data, pa.ctypes.data,
+                                              ld.ctypes.data, pt.ctypes.data, dwork, streams,
+                                              stream)

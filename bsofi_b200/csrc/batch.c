@@ -1,0 +1,145 @@
+/*
+ * batch.c -- batched inversion of independent block p-cyclic matrices.
+ *
+ * DQMC runs many Monte Carlo walkers, each with its own Green's-function
+ * matrix M (n, L differ between walkers only through the lattice and the
+ * number of time slices).  The reference inverts them one call at a time
+ * (src/bsofi_callback.c:130-157).  Here a batch is one call: instances are
+ * ordered by their flop count (largest first) and dealt over a pool of
+ * streams owned by the calling thread; each instance runs the fused device
+ * pipeline with a small BSOF worker pool, so the latency-bound panel chains
+ * of several instances overlap each other and the GEMM phases of the rest.
+ * The caller's stream waits for the whole batch (event fork/join), so the
+ * call is asynchronous like the single-instance device API.
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <cuda_runtime_api.h>
+
+#include "../../include/bsofi_b200.h"
+#include "bsofi_device.h"
+
+#define MAX_STREAMS 32
+
+typedef struct {
+  int ready, count, device;
+  cudaStream_t s[MAX_STREAMS];
+  cudaEvent_t ev[MAX_STREAMS + 1];
+} stream_pool;
+
+static __thread stream_pool t_pool;
+
+static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+static cudaError_t pool_get(int want, stream_pool **out) {
+  stream_pool *p = &t_pool;
+  int dev = -1, i;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (p->ready && p->device != dev) {
+    for (i = 0; i < p->count; i++) cudaStreamDestroy(p->s[i]);
+    for (i = 0; i <= p->count; i++) cudaEventDestroy(p->ev[i]);
+    p->ready = 0;
+    p->count = 0;
+  }
+  if (!p->ready) {
+    if ((e = cudaEventCreateWithFlags(&p->ev[0], cudaEventDisableTiming)) != cudaSuccess) return e;
+    p->ready = 1;
+    p->device = dev;
+  }
+  while (p->count < want && p->count < MAX_STREAMS) {
+    if ((e = cudaStreamCreateWithFlags(&p->s[p->count], cudaStreamNonBlocking)) != cudaSuccess)
+      return e;
+    if ((e = cudaEventCreateWithFlags(&p->ev[p->count + 1], cudaEventDisableTiming)) != cudaSuccess)
+      return e;
+    p->count++;
+  }
+  *out = p;
+  return cudaSuccess;
+}
+
+static double cost(int n, int L) { return 7.0 * (double)n * (double)n * (double)n * L * L; }
+
+unsigned long long bsofi_batch_workspace_bytes(int count, const int *n, const int *L,
+                                               const int *ldda) {
+  unsigned long long tot = 0;
+  int i;
+  for (i = 0; i < count; i++) tot += align256(bsofi_dev_ws_bytes(n[i], L[i], ldda[i]));
+  return tot;
+}
+
+typedef struct {
+  double c;
+  int i;
+} order_t;
+
+static int by_cost_desc(const void *a, const void *b) {
+  double x = ((const order_t *)a)->c, y = ((const order_t *)b)->c;
+  return x < y ? 1 : (x > y ? -1 : 0);
+}
+
+int bsofi_device_invert_batched(int count, const int *n, const int *L, double *const *dA,
+                                const int *ldda, double *const *dtau, void *dwork, int streams,
+                                void *stream) {
+  stream_pool *p;
+  order_t *ord;
+  size_t *off;
+  cudaError_t e;
+  int i, used, r = 0;
+  long long launches = 0;
+  if (count < 0 || (count > 0 && (!n || !L || !dA || !ldda || !dtau || !dwork))) return -1;
+  for (i = 0; i < count; i++)
+    if (n[i] < 1 || n[i] > BSOFI_MAX_BLOCK || L[i] < 2 || ldda[i] < n[i] * L[i] || !dA[i] ||
+        !dtau[i])
+      return -1;
+  if (count == 0) return 0;
+  if ((e = (cudaError_t)bsofi_dev_prepare()) != cudaSuccess) return BSOFI_INFO_CUDA - (int)e;
+  if (streams < 1) streams = 8;
+  if (streams > MAX_STREAMS) streams = MAX_STREAMS;
+  if ((e = pool_get(streams, &p)) != cudaSuccess) return BSOFI_INFO_CUDA - (int)e;
+  used = streams < count ? streams : count;
+  ord = (order_t *)malloc(sizeof(order_t) * count);
+  off = (size_t *)malloc(sizeof(size_t) * count);
+  if (!ord || !off) {
+    free(ord);
+    free(off);
+    return BSOFI_INFO_CUDA - (int)cudaErrorMemoryAllocation;
+  }
+  {
+    size_t o = 0;
+    for (i = 0; i < count; i++) {
+      ord[i].c = cost(n[i], L[i]);
+      ord[i].i = i;
+      off[i] = o;
+      o += align256(bsofi_dev_ws_bytes(n[i], L[i], ldda[i]));
+    }
+  }
+  qsort(ord, count, sizeof(order_t), by_cost_desc);
+  if ((e = cudaEventRecord(p->ev[0], (cudaStream_t)stream)) != cudaSuccess) goto fail;
+  for (i = 0; i < used; i++)
+    if ((e = cudaStreamWaitEvent(p->s[i], p->ev[0], 0)) != cudaSuccess) goto fail;
+  for (i = 0; i < count; i++) {
+    const int k = ord[i].i;
+    /* Few BSOF workers per instance: the batch supplies the parallelism. */
+    const int workers = n[k] <= 256 ? 6 : 24;
+    r = bsofi_dev_invert_ex(n[k], L[k], dA[k], ldda[k], dtau[k], (char *)dwork + off[k],
+                            p->s[i % used], workers);
+    if (r) {
+      e = (cudaError_t)r;
+      goto fail;
+    }
+    launches += bsofi_dev_launch_count();
+  }
+  for (i = 0; i < used; i++) {
+    if ((e = cudaEventRecord(p->ev[i + 1], p->s[i])) != cudaSuccess) goto fail;
+    if ((e = cudaStreamWaitEvent((cudaStream_t)stream, p->ev[i + 1], 0)) != cudaSuccess) goto fail;
+  }
+  free(ord);
+  free(off);
+  bsofi_dev_add_launches(launches - bsofi_dev_launch_count());
+  return 0;
+fail:
+  free(ord);
+  free(off);
+  return BSOFI_INFO_CUDA - (int)e;
+}

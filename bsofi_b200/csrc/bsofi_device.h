@@ -36,6 +36,9 @@ int bsofi_dev_bstri(int n, int L, double *dA, int ldd, void *dws, void *stream);
 /* BSOF + BSTRI + BSOI in one sequence; the factorization also forms the
  * explicit Q_k^T that BSOI consumes, off its critical chain. */
 int bsofi_dev_invert(int n, int L, double *dA, int ldd, double *dtau, void *dws, void *stream);
+/* Same with an explicit number of BSOF worker CTAs (0 = default). */
+int bsofi_dev_invert_ex(int n, int L, double *dA, int ldd, double *dtau, void *dws, void *stream,
+                        int workers);
 
 /* BSOI: A (reflectors + R^{-1}) <- M^{-1}. */
 int bsofi_dev_bsoi(int n, int L, double *dA, int ldd, const double *dtau, void *dws,

@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(256) build_leaf_t_kernel(const double* __restr
   Tout[tid] = sT[tid % 16][tid / 16];
 }
 
-int g_bsof_workers = 32;
+thread_local int g_bsof_workers = 32;
 
 // BSOF.  form_q: the persistent kernel also forms G_k = Q_k^T for BSOI.
 int run_bsof(int n, int L, double* dA, int ldd, double* dtau, void* ws, cudaStream_t st,
@@ -384,8 +384,16 @@ int bsofi_dev_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* 
 }
 
 int bsofi_dev_invert(int n, int L, double* dA, int ldd, double* dtau, void* dws, void* stream) {
+  return bsofi_dev_invert_ex(n, L, dA, ldd, dtau, dws, stream, 0);
+}
+
+int bsofi_dev_invert_ex(int n, int L, double* dA, int ldd, double* dtau, void* dws, void* stream,
+                        int workers) {
   g_launches = 0;
+  const int saved = g_bsof_workers;
+  if (workers > 0) g_bsof_workers = workers;
   int e = run_bsof(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, true);
+  g_bsof_workers = saved;
   if (!e) e = run_bstri(n, L, dA, ldd, dws, (cudaStream_t)stream);
   if (!e) e = run_bsoi(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, true);
   return e;

@@ -160,6 +160,20 @@ int *bsofi_device_info(void *dwork);
 /* Kernels launched by the last bsofi_device_* call on this thread. */
 long long bsofi_device_last_launches(void);
 
+/* Batched inversion of `count` independent matrices (no reference
+ * counterpart: the reference inverts one walker per call).  Instance i has
+ * block size n[i], L[i] blocks, device matrix dA[i] (ldda[i]) and device tau
+ * dtau[i]; dwork is one device workspace of bsofi_batch_workspace_bytes
+ * bytes.  Instances run largest first over `streams` internal streams
+ * (0 = 8, at most 32) owned by the calling thread; `stream` waits for the
+ * whole batch.  Returns 0, -1 for an illegal argument, or
+ * BSOFI_INFO_CUDA - cudaError_t. */
+unsigned long long bsofi_batch_workspace_bytes(int count, const int *n, const int *L,
+                                               const int *ldda);
+int bsofi_device_invert_batched(int count, const int *n, const int *L, double *const *dA,
+                                const int *ldda, double *const *dtau, void *dwork, int streams,
+                                void *stream);
+
 /* Allocation-free inversion.  No counterpart in the reference.  For callers
  * that cannot allocate device memory at inversion time: a code whose memory
  * pool already holds nearly all of HBM (cudaMalloc would fail), or one that
