@@ -35,7 +35,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-from bsofi_b200.flops import bsofi_flops, flops_bsoi  # noqa: E402
+from bsofi_b200.flops import bsofi_flops, flops_bsof, flops_bsoi  # noqa: E402
 from bsofi_b200.hubbard import hubbard_blocks  # noqa: E402
 
 METRIC = "inversions/s (FP64 BSOF/I, n=256, p=32)"
@@ -54,6 +54,11 @@ def parse():
     p.add_argument("--cpu-sample", type=int, default=2, help="reference inversions in cpu_baseline")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--batch", type=int, default=16,
+                   help="instances of the headline size per batched step (0 = skip)")
+    p.add_argument("--batch-mixed", type=int, default=64,
+                   help="instances in the mixed-size batched sample (0 = skip)")
+    p.add_argument("--batch-steps", type=int, default=3)
     return p.parse_args()
 
 
@@ -162,6 +167,29 @@ def measure_dgemm_peak(torch, dev, size=8192, reps=6):
         best = max(best, 2.0 * size ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
     del a, b, c
     return best
+
+
+def hbm_peak():
+    """Measured HBM copy bandwidth of this pool (GB/s), else the fallback."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(path))["hbm_gbs"])
+    except (OSError, ValueError, KeyError):
+        return 6650.0
+
+
+def bsof_chain_ms(api, n, L, ldd, ws):
+    """Duration of the BSOF chain of the last inversion that used `ws`
+    (globaltimer stamps written by the kernel's critical CTA)."""
+    from bsofi_b200 import _lib
+    nl = (n + 15) // 16 if n <= 256 else (n + 7) // 8
+    S = (L - 2) * nl + 2 * nl
+    buf = np.zeros(4 * S, dtype=np.uint64)
+    cnt = _lib.load().bsofi_device_bsof_timeline(n, L, ldd, ws.data_ptr(), buf.ctypes.data, S)
+    if cnt != S:
+        return None
+    t = buf.reshape(S, 4).astype(np.int64)
+    return float(t[-1, 2] - t[0, 0]) / 1e6
 
 
 def traffic_per_launch():
@@ -305,7 +333,8 @@ def main():
 
     peak = measure_dgemm_peak(torch, dev)
     achieved = flops_bsoi(n, L) * args.steps / (gemm_ms * 1e-3) / 1e12 if gemm_ms > 0 else None
-    roofline = {"kernel": "BSOI step GEMM (gemm_kernel, FP64 DMMA m16n8k4)",
+    roofline = {"kernel": "BSOI step GEMM (gemm_kernel, FP64 DMMA m16n8k8); dominant by "
+                          "algorithmic work (79% of the flop model)",
                 "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if achieved else None,
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor)",
@@ -313,6 +342,37 @@ def main():
                 "avg_launch_ms": gemm_ms / max(gemm_launches, 1),
                 "algorithmic_flops_per_launch": flops_bsoi(n, L) / (L - 1),
                 "traffic": traffic_per_launch()}
+    # The persistent BSOF kernel is the largest share of device time: a serial
+    # Householder chain, latency bound.  Reported against HBM as the panels'
+    # roofline, with its algorithmic flops beside it.
+    bsof_ms = bsof_chain_ms(api, n, L, ldd, ws)
+    bsof_bytes = 8.0 * ((L - 1) * 2 * n * 3 * n * 2 + 2 * L * n * n)
+    roofline_bsof = {"kernel": "bsof_persistent_kernel (Householder panel chain + trailing "
+                               "updates + Q_k^T formation)",
+                     "bound": "latency (serial chain of N Householder columns)",
+                     "chain_ms": bsof_ms,
+                     "achieved_gbs": bsof_bytes / (bsof_ms * 1e-3) / 1e9 if bsof_ms else None,
+                     "peak_gbs": hbm_peak(),
+                     "algorithmic_bytes": bsof_bytes,
+                     "achieved_tflops": flops_bsof(n, L) / (bsof_ms * 1e-3) / 1e12 if bsof_ms else None}
+
+    batched = None
+    if args.batch > 0:
+        specs = [(side, L, U, 5000 + 100 * rank + i) for i in range(args.batch)]
+        batched = run_batched(api, torch, dev, specs, args.batch_steps, stream)
+        batched["workload"] = ("%d independent FP64 inversions per step, %dx%d lattice, n=%d, "
+                               "p=%d (one walker each)" % (args.batch, side, side, n, L))
+    batched_mixed = None
+    if args.batch_mixed > 0:
+        rng = np.random.default_rng(77 + rank)
+        specs = [(int(rng.choice([8, 10, 12, 14, 16])), int(rng.integers(8, 65)),
+                  float(rng.uniform(2.0, 6.0)), 9000 + 1000 * rank + i)
+                 for i in range(args.batch_mixed)]
+        batched_mixed = run_batched(api, torch, dev, specs, args.batch_steps, stream)
+        batched_mixed["workload"] = ("%d independent FP64 inversions per step, lattice side in "
+                                     "{8,10,12,14,16}, p uniform in [8,64], U uniform in [2,6] "
+                                     "(a sample of the 256-walker batched configuration)"
+                                     % args.batch_mixed)
 
     e2e = None
     if not args.no_e2e and args.e2e_steps > 0:
@@ -337,12 +397,71 @@ def main():
                 "config": config(args, n, N),
                 "tflops": bsofi_flops(n, L) * value / world / 1e12,
                 "residual": resid,
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "roofline": roofline, "roofline_bsof": roofline_bsof,
+                "cpu_baseline": cpu, "e2e": e2e,
+                "batched": batched, "batched_mixed_sizes": batched_mixed,
                 "gpu_launches": launches_per_step * args.steps,
                 "clocks": clk}
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
+
+
+def run_batched(api, torch, dev, specs, steps, stream):
+    """Time bsofi_device_invert_batched over `steps` batches.  Every batch
+    starts from fresh inputs copied from pristine device buffers outside the
+    timed window; the reported rate is instances / summed batch time, max
+    over ranks."""
+    from bsofi_b200 import replicas
+    ns, Ls, lds, pristine = [], [], [], []
+    flops = 0.0
+    for side, L, U, seed in specs:
+        n = side * side
+        N = n * L
+        ld = (N + 31) // 32 * 32
+        pristine.append(pcyclic_device(torch, *hubbard_pcyclic(side, L, U, seed), ld, dev))
+        ns.append(n)
+        Ls.append(L)
+        lds.append(ld)
+        flops += bsofi_flops(n, L)
+    work = [torch.empty_like(t) for t in pristine]
+    taus = [torch.zeros(n * L, dtype=torch.float64, device=dev) for n, L in zip(ns, Ls)]
+    ws = torch.zeros(api.batch_workspace_bytes(ns, Ls, lds) // 8 + 1, dtype=torch.float64,
+                     device=dev)
+    sp = stream.cuda_stream
+    total_ms = 0.0
+    for it in range(steps + 1):  # the first batch is a warm-up
+        for w, p0 in zip(work, pristine):
+            w.copy_(p0)
+        torch.cuda.synchronize()
+        replicas.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            rc = api.device_invert_batched(ns, Ls, [w.data_ptr() for w in work], lds,
+                                           [t.data_ptr() for t in taus], ws.data_ptr(), 8, sp)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        if rc != 0:
+            raise RuntimeError("bsofi_device_invert_batched failed: %d" % rc)
+        if it > 0:
+            total_ms += e0.elapsed_time(e1)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from gpu_util import block_residual_gpu
+    side, L, U, seed = specs[0]
+    resid = block_residual_gpu(torch, *hubbard_pcyclic(side, L, U, seed),
+                               work[0][:, :ns[0] * Ls[0]].T.contiguous())
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    ms_max = replicas.max_over_ranks(total_ms, dev)
+    rate = world * len(specs) * steps / (ms_max * 1e-3)
+    out = {"value": rate, "unit": "inversions/s", "steps": steps,
+           "ms_per_step": ms_max / steps, "tflops": flops * steps * world / (ms_max * 1e-3) / 1e12,
+           "instances_per_step": len(specs), "residual_first_instance": resid,
+           "gpu_launches_per_step": api.last_launches()}
+    del work, pristine, ws
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_e2e(api, torch, dist, world, side, L, U, rank, steps):
