@@ -59,6 +59,9 @@ def parse():
     p.add_argument("--batch-mixed", type=int, default=64,
                    help="instances in the mixed-size batched sample (0 = skip)")
     p.add_argument("--batch-steps", type=int, default=3)
+    p.add_argument("--serve", type=int, default=60,
+                   help="requests in the served Poisson stream (0 = skip)")
+    p.add_argument("--serve-rate", type=float, default=12.0, help="mean arrivals per second")
     return p.parse_args()
 
 
@@ -374,6 +377,10 @@ def main():
                                      "(a sample of the 256-walker batched configuration)"
                                      % args.batch_mixed)
 
+    served = None
+    if args.serve > 0:
+        served = run_serving(api, torch, dev, args.serve, args.serve_rate, 31 + rank)
+
     e2e = None
     if not args.no_e2e and args.e2e_steps > 0:
         e2e = run_e2e(api, torch, dist, world, side, L, U, rank, args.e2e_steps)
@@ -399,7 +406,7 @@ def main():
                 "residual": resid,
                 "roofline": roofline, "roofline_bsof": roofline_bsof,
                 "cpu_baseline": cpu, "e2e": e2e,
-                "batched": batched, "batched_mixed_sizes": batched_mixed,
+                "batched": batched, "batched_mixed_sizes": batched_mixed, "served": served,
                 "gpu_launches": launches_per_step * args.steps,
                 "clocks": clk}
         print(json.dumps(line))
@@ -462,6 +469,61 @@ def run_batched(api, torch, dev, specs, steps, stream):
     del work, pristine, ws
     torch.cuda.empty_cache()
     return out
+
+
+def run_serving(api, torch, dev, nreq, rate, seed):
+    """A Poisson stream of inversion requests through the continuous-batching
+    server (bsofi_server_*).  Sizes follow the serving configuration (lattice
+    side uniform in 8..24, so n = 64..576; p uniform in 10..80; U in 2..6);
+    every request's matrix is built in HBM at its arrival and stays there.
+    Latency is wall clock from submission to the poll that sees it finish."""
+    from bsofi_b200 import replicas
+    rng = np.random.default_rng(seed)
+    specs = [(int(rng.integers(8, 25)), int(rng.integers(10, 81)), float(rng.uniform(2, 6)),
+              70000 + 97 * seed + i) for i in range(nreq)]
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
+    blocks = [hubbard_pcyclic(sd, L, U, sdd) for sd, L, U, sdd in specs]
+    flops = sum(bsofi_flops(sd * sd, L) for sd, L, _, _ in specs)
+    srv = api.Server(slots=8, pool_bytes=24 << 30)
+    submit_t, lat, bufs = {}, [], {}
+    nxt, done = 0, 0
+    replicas.barrier()
+    t0 = time.perf_counter()
+    while done < nreq:
+        now = time.perf_counter() - t0
+        while nxt < nreq and arrivals[nxt] <= now:
+            sd, L, U, _ = specs[nxt]
+            n = sd * sd
+            N = n * L
+            ld = (N + 31) // 32 * 32
+            A = pcyclic_device(torch, *blocks[nxt], ld, dev)
+            tau = torch.zeros(N, dtype=torch.float64, device=dev)
+            torch.cuda.current_stream().synchronize()  # the matrix is in HBM before submission
+            rid = srv.submit(n, L, A.data_ptr(), ld, tau.data_ptr())
+            submit_t[rid] = time.perf_counter() - t0
+            bufs[rid] = (A, tau)
+            nxt += 1
+        for rid, st in srv.poll():
+            if st != 0:
+                raise RuntimeError("served request %d failed: %d" % (rid, st))
+            lat.append(time.perf_counter() - t0 - submit_t[rid])
+            del bufs[rid]
+            done += 1
+        time.sleep(0.0002)
+    t_end = time.perf_counter() - t0
+    srv.close()
+    torch.cuda.empty_cache()
+    lat = np.array(lat) * 1e3
+    span = t_end - arrivals[0]
+    return {"requests": nreq, "arrival_rate_per_s": rate,
+            "value": nreq / span, "unit": "inversions/s",
+            "tflops": flops / span / 1e12,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "max_ms": float(lat.max()), "precision_mix": "all FP64",
+            "workload": "Poisson stream, lattice side uniform in 8..24 (n = 64..576), p uniform "
+                        "in 10..80, U uniform in 2..6; %d requests (a bounded sample of the "
+                        "10,000-request serving configuration), 8 slots, 24 GiB workspace pool"
+                        % nreq}
 
 
 def run_e2e(api, torch, dist, world, side, L, U, rank, steps):

@@ -169,3 +169,48 @@ def device_invert_batched(ns, Ls, dAs, lddas, dtaus, dwork, streams=8, stream=0)
     return load().bsofi_device_invert_batched(len(n), n.ctypes.data, L.ctypes.data, pa.ctypes.data,
                                               ld.ctypes.data, pt.ctypes.data, dwork, streams,
                                               stream)
+
+
+class Server:
+    """Continuous-batching inversion server (bsofi_server_*): submit
+    device-resident matrices, poll for finished requests."""
+
+    def __init__(self, slots=8, pool_bytes=8 << 30):
+        self.ptr = load().bsofi_server_create(int(slots), int(pool_bytes))
+        if not self.ptr:
+            raise RuntimeError("bsofi_server_create failed")
+        import numpy as _np
+        self._ids = _np.zeros(256, dtype=_np.int64)
+        self._st = _np.zeros(256, dtype=_np.int32)
+
+    def submit(self, n, L, dA, ldda, dtau, precision=0):
+        rid = load().bsofi_server_submit(self.ptr, n, L, dA, ldda, dtau, precision)
+        if rid < 0:
+            raise RuntimeError("bsofi_server_submit failed: %d" % rid)
+        return rid
+
+    def poll(self):
+        """List of (request id, status) that finished since the last poll."""
+        k = load().bsofi_server_poll(self.ptr, self._ids.ctypes.data, self._st.ctypes.data,
+                                     len(self._ids))
+        if k < 0:
+            raise RuntimeError("bsofi_server_poll failed")
+        return [(int(self._ids[i]), int(self._st[i])) for i in range(k)]
+
+    def pending(self):
+        return int(load().bsofi_server_pending(self.ptr))
+
+    def close(self):
+        if self.ptr:
+            load().bsofi_server_destroy(self.ptr)
+            self.ptr = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def server_request_bytes(n, L, ldda):
+    return int(load().bsofi_server_request_bytes(n, L, ldda))

@@ -1,0 +1,286 @@
+/*
+ * server.c -- continuous-batching inversion server.
+ *
+ * DQMC production runs and parameter sweeps produce a stream of inversion
+ * requests of different sizes (n = lattice sites, L = time slices).  The
+ * reference has no serving layer: each call is synchronous
+ * (src/bsofi_callback.c:130-157).  This server keeps every request's matrix
+ * and result resident in HBM (the caller owns them), runs up to `slots`
+ * requests at once (one stream each, so their kernels overlap on the
+ * device), and admits queued requests as slots and workspace memory free up:
+ *   * workspace comes from one device pool allocated at creation, handed out
+ *     first-fit; a request is admitted only when its workspace fits
+ *     (admission by memory footprint);
+ *   * admission is FIFO, but a request that does not fit may be passed by
+ *     smaller ones behind it at most BYPASS_LIMIT times, after which nothing
+ *     is admitted until it fits (no starvation);
+ *   * a request whose workspace exceeds the whole pool fails at submission.
+ * Progress is driven by bsofi_server_poll (no background thread): it retires
+ * finished requests (event query, no device synchronisation) and admits new
+ * ones.  One server is used by one host thread at a time.
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <cuda_runtime_api.h>
+
+#include "../../include/bsofi_b200.h"
+#include "bsofi_device.h"
+
+#define MAX_SLOTS 64
+#define BYPASS_LIMIT 16
+
+typedef struct {
+  long long id;
+  int n, L, ldda, precision;
+  double *dA, *dtau;
+  size_t ws;
+} request;
+
+typedef struct {
+  int busy;
+  long long id;
+  size_t off, len;
+  cudaStream_t stream;
+  cudaEvent_t done;
+  int *hinfo; /* pinned: BSTRI info word, BSOF error word */
+} slot;
+
+typedef struct {
+  size_t off, len;
+} span;
+
+struct bsofi_server {
+  int device, nslots;
+  slot s[MAX_SLOTS];
+  char *pool;
+  size_t pool_bytes;
+  span *free_list;
+  int nfree, cap_free;
+  request *queue;
+  int qhead, qlen, qcap;
+  int bypassed;
+  long long next_id;
+};
+
+typedef struct bsofi_server bsofi_server;
+
+static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+/* ------------------------------------------------------------ pool */
+static int pool_alloc(bsofi_server *sv, size_t len, size_t *off) {
+  int i;
+  for (i = 0; i < sv->nfree; i++) {
+    if (sv->free_list[i].len >= len) {
+      *off = sv->free_list[i].off;
+      sv->free_list[i].off += len;
+      sv->free_list[i].len -= len;
+      if (sv->free_list[i].len == 0) {
+        memmove(&sv->free_list[i], &sv->free_list[i + 1], sizeof(span) * (sv->nfree - i - 1));
+        sv->nfree--;
+      }
+      return 1;
+    }
+  }
+  return 0;
+}
+
+static int pool_free(bsofi_server *sv, size_t off, size_t len) {
+  int i = 0, j;
+  while (i < sv->nfree && sv->free_list[i].off < off) i++;
+  if (sv->nfree == sv->cap_free) {
+    span *nl = (span *)realloc(sv->free_list, sizeof(span) * 2 * sv->cap_free);
+    if (!nl) return 0;
+    sv->free_list = nl;
+    sv->cap_free *= 2;
+  }
+  memmove(&sv->free_list[i + 1], &sv->free_list[i], sizeof(span) * (sv->nfree - i));
+  sv->free_list[i].off = off;
+  sv->free_list[i].len = len;
+  sv->nfree++;
+  /* merge with neighbours */
+  for (j = (i > 0 ? i - 1 : 0); j + 1 < sv->nfree && j <= i;) {
+    if (sv->free_list[j].off + sv->free_list[j].len == sv->free_list[j + 1].off) {
+      sv->free_list[j].len += sv->free_list[j + 1].len;
+      memmove(&sv->free_list[j + 1], &sv->free_list[j + 2], sizeof(span) * (sv->nfree - j - 2));
+      sv->nfree--;
+    } else {
+      j++;
+    }
+  }
+  return 1;
+}
+
+/* ------------------------------------------------------------ queue */
+static int queue_push(bsofi_server *sv, const request *r) {
+  if (sv->qlen == sv->qcap) {
+    int ncap = sv->qcap ? 2 * sv->qcap : 64, i;
+    request *nq = (request *)malloc(sizeof(request) * ncap);
+    if (!nq) return 0;
+    for (i = 0; i < sv->qlen; i++) nq[i] = sv->queue[(sv->qhead + i) % sv->qcap];
+    free(sv->queue);
+    sv->queue = nq;
+    sv->qcap = ncap;
+    sv->qhead = 0;
+  }
+  sv->queue[(sv->qhead + sv->qlen) % sv->qcap] = *r;
+  sv->qlen++;
+  return 1;
+}
+
+static void queue_remove(bsofi_server *sv, int pos) {
+  int i;
+  for (i = pos; i > 0; i--)
+    sv->queue[(sv->qhead + i) % sv->qcap] = sv->queue[(sv->qhead + i - 1) % sv->qcap];
+  sv->qhead = (sv->qhead + 1) % sv->qcap;
+  sv->qlen--;
+}
+
+/* ------------------------------------------------------------ API */
+bsofi_server *bsofi_server_create(int slots, unsigned long long pool_bytes) {
+  bsofi_server *sv;
+  int i;
+  if (slots < 1 || slots > MAX_SLOTS || pool_bytes < 4096) return NULL;
+  if (bsofi_dev_prepare() != 0) return NULL;
+  sv = (bsofi_server *)calloc(1, sizeof(bsofi_server));
+  if (!sv) return NULL;
+  if (cudaGetDevice(&sv->device) != cudaSuccess) goto fail;
+  sv->nslots = slots;
+  sv->pool_bytes = (size_t)pool_bytes & ~(size_t)255;
+  if (cudaMalloc((void **)&sv->pool, sv->pool_bytes) != cudaSuccess) goto fail;
+  sv->cap_free = 64;
+  sv->free_list = (span *)malloc(sizeof(span) * sv->cap_free);
+  if (!sv->free_list) goto fail;
+  sv->free_list[0].off = 0;
+  sv->free_list[0].len = sv->pool_bytes;
+  sv->nfree = 1;
+  for (i = 0; i < slots; i++) {
+    if (cudaStreamCreateWithFlags(&sv->s[i].stream, cudaStreamNonBlocking) != cudaSuccess) goto fail;
+    if (cudaEventCreateWithFlags(&sv->s[i].done, cudaEventDisableTiming) != cudaSuccess) goto fail;
+    if (cudaMallocHost((void **)&sv->s[i].hinfo, 2 * sizeof(int)) != cudaSuccess) goto fail;
+  }
+  return sv;
+fail:
+  bsofi_server_destroy(sv);
+  return NULL;
+}
+
+void bsofi_server_destroy(bsofi_server *sv) {
+  int i;
+  if (!sv) return;
+  for (i = 0; i < MAX_SLOTS; i++) {
+    if (sv->s[i].stream) {
+      cudaStreamSynchronize(sv->s[i].stream);
+      cudaStreamDestroy(sv->s[i].stream);
+    }
+    if (sv->s[i].done) cudaEventDestroy(sv->s[i].done);
+    if (sv->s[i].hinfo) cudaFreeHost(sv->s[i].hinfo);
+  }
+  if (sv->pool) cudaFree(sv->pool);
+  free(sv->free_list);
+  free(sv->queue);
+  free(sv);
+}
+
+unsigned long long bsofi_server_request_bytes(int n, int L, int ldda) {
+  return align256(bsofi_dev_ws_bytes(n, L, ldda));
+}
+
+long long bsofi_server_submit(bsofi_server *sv, int n, int L, double *dA, int ldda,
+                              double *dtau, int precision) {
+  request r;
+  if (!sv) return -1;
+  if (n < 1 || n > BSOFI_MAX_BLOCK || L < 2 || ldda < n * L || !dA || !dtau) return -2;
+  if (precision != 0) return -3; /* only the FP64 path is served */
+  r.ws = align256(bsofi_dev_ws_bytes(n, L, ldda));
+  if (r.ws > sv->pool_bytes) return -4; /* can never be admitted */
+  r.id = sv->next_id++;
+  r.n = n;
+  r.L = L;
+  r.ldda = ldda;
+  r.precision = precision;
+  r.dA = dA;
+  r.dtau = dtau;
+  if (!queue_push(sv, &r)) return -5;
+  return r.id;
+}
+
+static int launch(bsofi_server *sv, slot *sl, const request *r) {
+  int e, workers = r->n <= 256 ? 6 : 24;
+  void *ws = sv->pool + sl->off;
+  e = bsofi_dev_invert_ex(r->n, r->L, r->dA, r->ldda, r->dtau, ws, sl->stream, workers);
+  if (!e)
+    e = (int)cudaMemcpyAsync(sl->hinfo, bsofi_dev_info_ptr(ws), 2 * sizeof(int),
+                             cudaMemcpyDeviceToHost, sl->stream);
+  if (!e) e = (int)cudaEventRecord(sl->done, sl->stream);
+  return e;
+}
+
+/* Admit queued requests into free slots while their workspace fits. */
+static int admit(bsofi_server *sv, long long *done_ids, int *done_status, int max, int *ndone) {
+  int pos = 0, i;
+  while (pos < sv->qlen) {
+    slot *sl = NULL;
+    request *r = &sv->queue[(sv->qhead + pos) % sv->qcap];
+    size_t off;
+    for (i = 0; i < sv->nslots; i++)
+      if (!sv->s[i].busy) {
+        sl = &sv->s[i];
+        break;
+      }
+    if (!sl) break;
+    if (!pool_alloc(sv, r->ws, &off)) {
+      if (pos == 0 && sv->bypassed >= BYPASS_LIMIT) break; /* hold for the head */
+      pos++;
+      continue;
+    }
+    if (pos > 0) sv->bypassed++;
+    else sv->bypassed = 0;
+    sl->busy = 1;
+    sl->id = r->id;
+    sl->off = off;
+    sl->len = r->ws;
+    {
+      const int e = launch(sv, sl, r);
+      if (e != 0) { /* a launch error retires the request at once */
+        sl->busy = 0;
+        pool_free(sv, off, r->ws);
+        if (*ndone < max) {
+          done_ids[*ndone] = r->id;
+          done_status[*ndone] = BSOFI_INFO_CUDA - e;
+          (*ndone)++;
+        }
+      }
+    }
+    queue_remove(sv, pos);
+  }
+  return 0;
+}
+
+int bsofi_server_poll(bsofi_server *sv, long long *done_ids, int *done_status, int max) {
+  int i, ndone = 0;
+  if (!sv || max < 0) return -1;
+  for (i = 0; i < sv->nslots && ndone < max; i++) {
+    slot *sl = &sv->s[i];
+    cudaError_t q;
+    if (!sl->busy) continue;
+    q = cudaEventQuery(sl->done);
+    if (q == cudaErrorNotReady) continue;
+    done_ids[ndone] = sl->id;
+    if (q != cudaSuccess) done_status[ndone] = BSOFI_INFO_CUDA - (int)q;
+    else if (sl->hinfo[1] != 0) done_status[ndone] = BSOFI_INFO_CUDA - (int)cudaErrorLaunchTimeout;
+    else done_status[ndone] = (sl->hinfo[0] >= 0x7f7f7f7f || sl->hinfo[0] < 0) ? 0 : sl->hinfo[0];
+    ndone++;
+    sl->busy = 0;
+    pool_free(sv, sl->off, sl->len);
+  }
+  admit(sv, done_ids, done_status, max, &ndone);
+  return ndone;
+}
+
+int bsofi_server_pending(bsofi_server *sv) {
+  int i, busy = 0;
+  if (!sv) return -1;
+  for (i = 0; i < sv->nslots; i++) busy += sv->s[i].busy;
+  return busy + sv->qlen;
+}

@@ -174,6 +174,27 @@ int bsofi_device_invert_batched(int count, const int *n, const int *L, double *c
                                 const int *ldda, double *const *dtau, void *dwork, int streams,
                                 void *stream);
 
+/* Continuous-batching inversion server (no reference counterpart: the
+ * reference's calls are synchronous, one matrix at a time).  Requests invert
+ * caller-owned device-resident matrices; up to `slots` run at once, each on
+ * its own stream, with workspace taken first-fit from a device pool of
+ * `pool_bytes` allocated at creation (admission by memory footprint, FIFO
+ * with bounded bypass so large requests are not starved).  Progress is made
+ * in bsofi_server_poll, which retires finished requests (writing up to `max`
+ * ids and statuses: 0, info > 0 for an exactly singular R, or
+ * BSOFI_INFO_CUDA - cudaError_t) and admits queued ones; it never blocks.
+ * submit returns the request id (>= 0) or -1 bad server, -2 illegal size,
+ * -3 unsupported precision (only 0 = FP64), -4 workspace larger than the
+ * pool, -5 out of host memory.  One host thread per server. */
+typedef struct bsofi_server bsofi_server;
+bsofi_server *bsofi_server_create(int slots, unsigned long long pool_bytes);
+unsigned long long bsofi_server_request_bytes(int n, int L, int ldda);
+long long bsofi_server_submit(bsofi_server *server, int n, int L, double *dA, int ldda,
+                              double *dtau, int precision);
+int bsofi_server_poll(bsofi_server *server, long long *done_ids, int *done_status, int max);
+int bsofi_server_pending(bsofi_server *server);
+void bsofi_server_destroy(bsofi_server *server);
+
 /* Allocation-free inversion.  No counterpart in the reference.  For callers
  * that cannot allocate device memory at inversion time: a code whose memory
  * pool already holds nearly all of HBM (cudaMalloc would fail), or one that
