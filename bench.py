@@ -550,6 +550,14 @@ def run_e2e(api, torch, dist, world, side, L, U, rank, steps):
         if i > 0:
             times.append(dt)
     h.close()
+    # The e2e result must be the inverse: residual of the last step on the GPU.
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from gpu_util import block_residual_gpu
+    from bsofi_b200.hubbard import pcyclic_blocks
+    resid = block_residual_gpu(torch, *pcyclic_blocks(M, n, L),
+                               torch.from_numpy(np.ascontiguousarray(A)).to("cuda"))
+    if not resid < 1e-12:
+        raise RuntimeError("e2e result check failed: residual %g" % resid)
     tot = sum(times)
     t = torch.tensor([tot], dtype=torch.float64, device="cuda")
     if world > 1:
@@ -561,7 +569,7 @@ def run_e2e(api, torch, dist, world, side, L, U, rank, steps):
     return {"value": world * len(times) / tot, "unit": "inversions/s",
             "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
             "api": "hybridxbsoftrih_ + hybridxbsoih_ (host pageable buffers)",
-            "steps": len(times)}
+            "steps": len(times), "residual": resid}
 
 
 if __name__ == "__main__":

@@ -11,10 +11,12 @@
  *              the reflector blocks, D2H tau;
  *   XbsoiH     H2D that same region and tau, D2H the dense M^{-1}.
  */
+#include <pthread.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 #include <sys/time.h>
+#include <unistd.h>
 #include <cuda_runtime_api.h>
 
 #include "../../include/bsofi_b200.h"
@@ -23,6 +25,128 @@
 #define HANDLE_MAGIC 0x49465342u /* "BSFI" */
 #define HANDLE_VERSION 1u
 #define CTX_MAGIC 0x58544342u
+
+/* ------------------------------------------------------------------------
+ * Host staging.  The caller's arrays are pageable; copies go through two
+ * pinned buffers (double buffering against the DMA engine), packed and
+ * unpacked column by column by a small pool of host threads so that host
+ * memory bandwidth, not one core, bounds the transfer.
+ * ---------------------------------------------------------------------- */
+#define STAGE_BYTES ((size_t)64 << 20)
+#define MAX_COPY_THREADS 16
+#define PAR_MIN_BYTES ((size_t)1 << 20)
+
+typedef struct copy_pool {
+  int nthreads;
+  pthread_t th[MAX_COPY_THREADS];
+  pthread_mutex_t mu;
+  pthread_cond_t cv_work, cv_done;
+  unsigned long generation;
+  int remaining, stop;
+  char *dst;
+  const char *src;
+  size_t dpitch, spitch, width, height;
+} copy_pool;
+
+typedef struct {
+  copy_pool *p;
+  int index;
+} copy_arg;
+
+static void copy_rows(char *dst, size_t dpitch, const char *src, size_t spitch, size_t width,
+                      size_t h0, size_t h1) {
+  size_t i;
+  for (i = h0; i < h1; i++) memcpy(dst + i * dpitch, src + i * spitch, width);
+}
+
+static void *copy_worker(void *arg) {
+  copy_arg *a = (copy_arg *)arg;
+  copy_pool *p = a->p;
+  unsigned long seen = 0;
+  for (;;) {
+    size_t h0, h1;
+    pthread_mutex_lock(&p->mu);
+    while (p->generation == seen && !p->stop) pthread_cond_wait(&p->cv_work, &p->mu);
+    if (p->stop) {
+      pthread_mutex_unlock(&p->mu);
+      break;
+    }
+    seen = p->generation;
+    h0 = p->height * (size_t)a->index / (size_t)(p->nthreads + 1);
+    h1 = p->height * (size_t)(a->index + 1) / (size_t)(p->nthreads + 1);
+    pthread_mutex_unlock(&p->mu);
+    copy_rows(p->dst, p->dpitch, p->src, p->spitch, p->width, h0, h1);
+    pthread_mutex_lock(&p->mu);
+    if (--p->remaining == 0) pthread_cond_signal(&p->cv_done);
+    pthread_mutex_unlock(&p->mu);
+  }
+  free(a);
+  return NULL;
+}
+
+static copy_pool *copy_pool_create(void) {
+  copy_pool *p = (copy_pool *)calloc(1, sizeof(copy_pool));
+  long nproc = sysconf(_SC_NPROCESSORS_ONLN);
+  int i, want;
+  if (!p) return NULL;
+  want = (int)(nproc > 1 ? nproc - 1 : 0);
+  if (want > MAX_COPY_THREADS - 1) want = MAX_COPY_THREADS - 1;
+  pthread_mutex_init(&p->mu, NULL);
+  pthread_cond_init(&p->cv_work, NULL);
+  pthread_cond_init(&p->cv_done, NULL);
+  for (i = 0; i < want; i++) {
+    copy_arg *a = (copy_arg *)malloc(sizeof(copy_arg));
+    if (!a) break;
+    a->p = p;
+    a->index = i;
+    if (pthread_create(&p->th[i], NULL, copy_worker, a) != 0) {
+      free(a);
+      break;
+    }
+    p->nthreads++;
+  }
+  return p;
+}
+
+static void copy_pool_destroy(copy_pool *p) {
+  int i;
+  if (!p) return;
+  pthread_mutex_lock(&p->mu);
+  p->stop = 1;
+  pthread_cond_broadcast(&p->cv_work);
+  pthread_mutex_unlock(&p->mu);
+  for (i = 0; i < p->nthreads; i++) pthread_join(p->th[i], NULL);
+  pthread_mutex_destroy(&p->mu);
+  pthread_cond_destroy(&p->cv_work);
+  pthread_cond_destroy(&p->cv_done);
+  free(p);
+}
+
+/* height rows of `width` bytes, split over the pool and the calling thread. */
+static void par_copy2d(copy_pool *p, char *dst, size_t dpitch, const char *src, size_t spitch,
+                       size_t width, size_t height) {
+  size_t h0;
+  if (!p || p->nthreads == 0 || width * height < PAR_MIN_BYTES) {
+    copy_rows(dst, dpitch, src, spitch, width, 0, height);
+    return;
+  }
+  pthread_mutex_lock(&p->mu);
+  p->dst = dst;
+  p->src = src;
+  p->dpitch = dpitch;
+  p->spitch = spitch;
+  p->width = width;
+  p->height = height;
+  p->remaining = p->nthreads;
+  p->generation++;
+  pthread_cond_broadcast(&p->cv_work);
+  pthread_mutex_unlock(&p->mu);
+  h0 = height * (size_t)p->nthreads / (size_t)(p->nthreads + 1);
+  copy_rows(dst, dpitch, src, spitch, width, h0, height);
+  pthread_mutex_lock(&p->mu);
+  while (p->remaining > 0) pthread_cond_wait(&p->cv_done, &p->mu);
+  pthread_mutex_unlock(&p->mu);
+}
 
 typedef struct bsofi_ctx {
   uint32_t magic;
@@ -33,6 +157,10 @@ typedef struct bsofi_ctx {
   double *dtau;
   void *dws;
   size_t ws_bytes;
+  char *stage[2];       /* pinned host staging buffers */
+  cudaEvent_t stage_ev[2];
+  int stage_next;
+  copy_pool *pool;
 } bsofi_ctx;
 
 /* Layout of the caller's integer handler(10) (40 bytes). */
@@ -102,12 +230,31 @@ static bsofi_ctx *ctx_create(int n, int L, cudaError_t *err) {
     *err = e;
     return NULL;
   }
+  {
+    int b;
+    for (b = 0; b < 2; b++) {
+      if ((e = cudaMallocHost((void **)&c->stage[b], STAGE_BYTES)) != cudaSuccess ||
+          (e = cudaEventCreateWithFlags(&c->stage_ev[b], cudaEventDisableTiming)) != cudaSuccess) {
+        c->stage[b] = NULL;
+        cudaGetLastError();
+        break;
+      }
+    }
+    c->pool = copy_pool_create();
+  }
   *err = cudaSuccess;
   return c;
 }
 
 static void ctx_destroy(bsofi_ctx *c) {
+  int b;
   if (!c) return;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (b = 0; b < 2; b++) {
+    if (c->stage[b]) cudaFreeHost(c->stage[b]);
+    if (c->stage_ev[b]) cudaEventDestroy(c->stage_ev[b]);
+  }
+  copy_pool_destroy(c->pool);
   ctx_free_buffers(c);
   if (c->stream) cudaStreamDestroy(c->stream);
   c->magic = 0;
@@ -126,28 +273,94 @@ static bsofi_ctx *handle_ctx(const int *h) {
 }
 
 /* ---------------------------------------------------------------- copies */
+/* Host (pitch lda) -> device (pitch ldd): `rows` doubles of `cols` columns,
+ * through the pinned staging buffers. */
+static cudaError_t h2d_cols(bsofi_ctx *c, double *dst, int ldd, const double *src, int lda,
+                            int rows, int cols) {
+  const size_t es = sizeof(double), w = (size_t)rows * es;
+  int c0, cpc;
+  cudaError_t e;
+  if (!c->stage[1])
+    return cudaMemcpy2DAsync(dst, es * ldd, src, es * lda, w, cols, cudaMemcpyHostToDevice,
+                             c->stream);
+  cpc = (int)(STAGE_BYTES / w);
+  if (cpc < 1) cpc = 1;
+  for (c0 = 0; c0 < cols; c0 += cpc) {
+    const int nc = cols - c0 < cpc ? cols - c0 : cpc, b = c->stage_next;
+    c->stage_next ^= 1;
+    if ((e = cudaEventSynchronize(c->stage_ev[b])) != cudaSuccess) return e;
+    par_copy2d(c->pool, c->stage[b], w, (const char *)(src + (size_t)c0 * lda), es * lda, w, nc);
+    e = cudaMemcpy2DAsync(dst + (size_t)c0 * ldd, es * ldd, c->stage[b], w, w, nc,
+                          cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(c->stage_ev[b], c->stream);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+/* Device (pitch ldd) -> host (pitch lda), pipelined: the DMA of chunk i+1
+ * runs while the host threads unpack chunk i.  Returns when all of it is on
+ * the host. */
+static cudaError_t d2h_cols(bsofi_ctx *c, double *dst, int lda, const double *src, int ldd,
+                            int rows, int cols) {
+  const size_t es = sizeof(double), w = (size_t)rows * es;
+  int i, nchunks, cpc, prev_c0 = 0, prev_nc = 0, prev_b = 0;
+  cudaError_t e;
+  if (cols <= 0) return cudaSuccess;
+  if (!c->stage[1]) {
+    e = cudaMemcpy2DAsync(dst, es * lda, src, es * ldd, w, cols, cudaMemcpyDeviceToHost,
+                          c->stream);
+    return e == cudaSuccess ? cudaStreamSynchronize(c->stream) : e;
+  }
+  cpc = (int)(STAGE_BYTES / w);
+  if (cpc < 1) cpc = 1;
+  nchunks = (cols + cpc - 1) / cpc;
+  /* Iteration i issues the DMA of chunk i (if any) and unpacks chunk i-1. */
+  for (i = 0; i <= nchunks; i++) {
+    if (i < nchunks) {
+      const int c0 = i * cpc, nc = cols - c0 < cpc ? cols - c0 : cpc, b = c->stage_next;
+      c->stage_next ^= 1;
+      if ((e = cudaEventSynchronize(c->stage_ev[b])) != cudaSuccess) return e;
+      e = cudaMemcpy2DAsync(c->stage[b], w, src + (size_t)c0 * ldd, es * ldd, w, nc,
+                            cudaMemcpyDeviceToHost, c->stream);
+      if (e == cudaSuccess) e = cudaEventRecord(c->stage_ev[b], c->stream);
+      if (e != cudaSuccess) return e;
+      if (i > 0) {
+        if ((e = cudaEventSynchronize(c->stage_ev[prev_b])) != cudaSuccess) return e;
+        par_copy2d(c->pool, (char *)(dst + (size_t)prev_c0 * lda), es * lda, c->stage[prev_b], w,
+                   w, prev_nc);
+      }
+      prev_c0 = c0;
+      prev_nc = nc;
+      prev_b = b;
+    } else {
+      if ((e = cudaEventSynchronize(c->stage_ev[prev_b])) != cudaSuccess) return e;
+      par_copy2d(c->pool, (char *)(dst + (size_t)prev_c0 * lda), es * lda, c->stage[prev_b], w, w,
+                 prev_nc);
+    }
+  }
+  return cudaSuccess;
+}
+
 /* H2D of the p-cyclic blocks of the host matrix (every other block zero). */
 static cudaError_t upload_pcyclic(bsofi_ctx *c, const double *A, int lda) {
   int n = c->n, L = c->L, k;
   size_t es = sizeof(double);
   cudaError_t e = (cudaError_t)bsofi_dev_zero_structural(n, L, c->dA, c->ldd, c->stream);
   if (e != cudaSuccess) return e;
+  (void)es;
   for (k = 0; k < L - 1; k++) { /* diagonal + sub-diagonal block of column block k */
     size_t off_h = (size_t)k * n * lda + (size_t)k * n;
     size_t off_d = (size_t)k * n * c->ldd + (size_t)k * n;
-    e = cudaMemcpy2DAsync(c->dA + off_d, es * c->ldd, A + off_h, es * lda, es * 2 * n, n,
-                          cudaMemcpyHostToDevice, c->stream);
-    if (e != cudaSuccess) return e;
+    if ((e = h2d_cols(c, c->dA + off_d, c->ldd, A + off_h, lda, 2 * n, n)) != cudaSuccess)
+      return e;
   }
   /* last column block: corner (0, L-1) and diagonal (L-1, L-1) */
   {
     size_t col_h = (size_t)(L - 1) * n * lda, col_d = (size_t)(L - 1) * n * c->ldd;
-    e = cudaMemcpy2DAsync(c->dA + col_d, es * c->ldd, A + col_h, es * lda, es * n, n,
-                          cudaMemcpyHostToDevice, c->stream);
-    if (e != cudaSuccess) return e;
-    e = cudaMemcpy2DAsync(c->dA + col_d + (size_t)(L - 1) * n, es * c->ldd,
-                          A + col_h + (size_t)(L - 1) * n, es * lda, es * n, n,
-                          cudaMemcpyHostToDevice, c->stream);
+    if ((e = h2d_cols(c, c->dA + col_d, c->ldd, A + col_h, lda, n, n)) != cudaSuccess) return e;
+    e = h2d_cols(c, c->dA + col_d + (size_t)(L - 1) * n, c->ldd, A + col_h + (size_t)(L - 1) * n,
+                 lda, n, n);
   }
   return e;
 }
@@ -157,16 +370,15 @@ static cudaError_t copy_state(bsofi_ctx *c, double *A, int lda, int to_host) {
   int n = c->n, L = c->L, N = n * L, k;
   size_t es = sizeof(double);
   cudaError_t e = cudaSuccess;
+  (void)es;
   for (k = 0; k < L; k++) {
     int rows = (k + 2) * n < N ? (k + 2) * n : N;
     double *h = A + (size_t)k * n * lda;
     double *d = c->dA + (size_t)k * n * c->ldd;
     if (to_host)
-      e = cudaMemcpy2DAsync(h, es * lda, d, es * c->ldd, es * rows, n, cudaMemcpyDeviceToHost,
-                            c->stream);
+      e = d2h_cols(c, h, lda, d, c->ldd, rows, n);
     else
-      e = cudaMemcpy2DAsync(d, es * c->ldd, h, es * lda, es * rows, n, cudaMemcpyHostToDevice,
-                            c->stream);
+      e = h2d_cols(c, d, c->ldd, h, lda, rows, n);
     if (e != cudaSuccess) return e;
   }
   return e;
@@ -248,9 +460,7 @@ static int drive_bsoi(bsofi_ctx *c, int n, int L, double *A, int lda, const doub
   if (e != cudaSuccess) return cuda_info(e);
   e = (cudaError_t)bsofi_dev_bsoi(n, L, c->dA, c->ldd, c->dtau, c->dws, c->stream);
   if (e != cudaSuccess) return cuda_info(e);
-  e = cudaMemcpy2DAsync(A, sizeof(double) * lda, c->dA, sizeof(double) * c->ldd,
-                        sizeof(double) * N, N, cudaMemcpyDeviceToHost, c->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  e = d2h_cols(c, A, lda, c->dA, c->ldd, N, N);
   return e == cudaSuccess ? 0 : cuda_info(e);
 }
 
