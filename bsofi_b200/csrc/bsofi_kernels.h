@@ -37,7 +37,7 @@ cudaError_t launch_bsof_persistent(double* A, long long ld, int n, int L, double
 cudaError_t launch_trtri_blocks(double* A, long long ld, int n, long long bstride,
                                 int nblk, int* info, cudaStream_t st);
 
-// cfg: 0 = choose by tile count, 1 = 128x128 tiles, 2 = 64x64 tiles.
+// cfg: 0 = choose by tile count, 1 = 128x128 (8 warps), 2 = 64x64, 3 = 128x128 (16 warps).
 cudaError_t launch_gemm(const GemmDims& d, const GemmA& a, const GemmB& b,
                         const GemmC& c, int batch, int cfg, cudaStream_t st);
 cudaError_t gemm_init_attributes();

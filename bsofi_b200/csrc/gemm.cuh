@@ -52,9 +52,9 @@ struct GemmDims {
   int M, N, K;
 };
 
-template <int BM_, int BN_, int WARPS_M_, int WARPS_N_, int STAGES_>
+template <int BM_, int BN_, int WARPS_M_, int WARPS_N_, int STAGES_, int BK_ = 16>
 struct TileCfg {
-  static constexpr int BM = BM_, BN = BN_, BK = 16;
+  static constexpr int BM = BM_, BN = BN_, BK = BK_;
   static constexpr int WARPS_M = WARPS_M_, WARPS_N = WARPS_N_;
   static constexpr int THREADS = 32 * WARPS_M * WARPS_N;
   static constexpr int STAGES = STAGES_;
@@ -70,6 +70,7 @@ struct TileCfg {
 };
 
 using CfgL = TileCfg<128, 128, 2, 4, 3>;  // 256 threads, warp tile 64x32
+using CfgM = TileCfg<128, 128, 4, 4, 3, 32>;  // 512 threads, warp tile 32x32, K stage 32
 using CfgS = TileCfg<64, 64, 2, 2, 3>;    // 128 threads, warp tile 32x32
 
 BSOFI_DEVINL int clamp02(long long v) { return v < 0 ? 0 : (v > 2 ? 2 : (int)v); }

@@ -495,83 +495,147 @@ BSOFI_DEVINL void apply_qt(const double (&v)[R][NB], double* C, long long ld, in
 // fragment loads of both products bank-conflict free.
 constexpr int MS = 20;
 
+// Rows of one staging pass: two thread-owned row slices (R >= 2), i.e. the
+// staged tiles never exceed 2 * BT rows whatever the leaf height.
 template <int R>
-BSOFI_DEVINL void apply_qt_mma(double* sV, double* sC, double* C, long long ld, int m, int w,
-                               Smem<16>& sm) {
-  constexpr int MP = R * BT;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int g = lane >> 2, t = lane & 3;
+struct Pass {
+  static constexpr int SL = R >= 2 ? 2 : 1;      // row slices per pass
+  static constexpr int ROWS = SL * BT;           // staged rows per pass
+  static constexpr int NP = (R + SL - 1) / SL;   // passes
+};
+
+// Fill the staged V rows of pass p.  From registers (the factoring CTA) when
+// VREG, else from the stored reflectors in global memory.
+template <int R, bool VREG>
+BSOFI_DEVINL void stage_v(double* sV, const double (&a)[R][16], const double* P, long long ld,
+                          int m, int w, int p) {
+  constexpr int SL = Pass<R>::SL;
+  const int tid = threadIdx.x;
 #pragma unroll
-  for (int i = 0; i < R; i++) {
-    const int r = tid + BT * i;
+  for (int j = 0; j < SL; j++) {
+    const int i = p * SL + j;
+    const int lr = tid + BT * j;          // row inside the pass
+    const int r = tid + BT * i;           // row of the leaf
+#pragma unroll
+    for (int c = 0; c < 16; c++) {
+      double v = 0.0;
+      if (i < R && r < m && c < w) {
+        if (r == c) v = 1.0;
+        else if (r > c) v = VREG ? a[i < R ? i : 0][c] : __ldcg(P + cm(r, c, ld));
+      }
+      sV[lr * MS + c] = v;
+    }
+  }
+}
+
+template <int R>
+BSOFI_DEVINL void stage_c(double* sC, const double* C, long long ld, int m, int w, int p) {
+  constexpr int SL = Pass<R>::SL;
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int j = 0; j < SL; j++) {
+    const int i = p * SL + j;
+    const int lr = tid + BT * j, r = tid + BT * i;
 #pragma unroll
     for (int cc = 0; cc < 16; cc++)
-      sC[r * MS + cc] = (r < m && cc < w) ? __ldcg(C + cm(r, cc, ld)) : 0.0;
+      sC[lr * MS + cc] = (i < R && r < m && cc < w) ? __ldcg(C + cm(r, cc, ld)) : 0.0;
   }
-  __syncthreads();
-  {  // W partial over this warp's rows
-    double acc[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
-    constexpr int KW = MP / BW;
+}
+
+// 16-wide block reflector applied with DMMA (mma.sync m16n8k8 f64), in passes
+// of at most 2*BT rows staged in shared memory:
+//   W = V^T C (16 x 16; K = rows, split over the 8 warps, summed over passes),
+//   W <- -T^T W,  C <- C + V W  (second sweep over the passes).
+// A stride of MS = 20 doubles makes the fragment loads bank-conflict free.
+// wv: width of the leaf (reflector columns), w: width of the target tile.
+// VPRE: the caller already staged V (single pass only).
+template <int R, bool VREG, bool VPRE = false>
+BSOFI_DEVINL void apply_qt_mma(double* sV, double* sC, const double (&a)[R][16],
+                               const double* P, long long ldp, int wv, double* C, long long ld,
+                               int m, int w, Smem<16>& sm) {
+  static_assert(!VPRE || Pass<R>::NP == 1, "pre-staged V needs a single pass");
+  constexpr int PR = Pass<R>::ROWS, NP = Pass<R>::NP;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  double acc[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
+#pragma unroll 1
+  for (int p = 0; p < NP; p++) {
+    if (!VPRE) stage_v<R, VREG>(sV, a, P, ldp, m, wv, p);
+    stage_c<R>(sC, C, ld, m, w, p);
+    __syncthreads();
+    constexpr int KW = PR / BW;
     const int r0 = warp * KW;
-#pragma unroll 4
-    for (int k0 = r0; k0 < r0 + KW; k0 += 4) {
+#pragma unroll 2
+    for (int k0 = r0; k0 < r0 + KW; k0 += 8) {
       const double a0 = sV[(k0 + t) * MS + g], a1 = sV[(k0 + t) * MS + g + 8];
-      dmma_16x8x4(acc[0], a0, a1, sC[(k0 + t) * MS + g]);
-      dmma_16x8x4(acc[1], a0, a1, sC[(k0 + t) * MS + 8 + g]);
+      const double a2 = sV[(k0 + t + 4) * MS + g], a3 = sV[(k0 + t + 4) * MS + g + 8];
+      dmma_16x8x8(acc[0], a0, a1, a2, a3, sC[(k0 + t) * MS + g], sC[(k0 + t + 4) * MS + g]);
+      dmma_16x8x8(acc[1], a0, a1, a2, a3, sC[(k0 + t) * MS + 8 + g],
+                  sC[(k0 + t + 4) * MS + 8 + g]);
     }
+    __syncthreads();
+  }
 #pragma unroll
-    for (int j = 0; j < 2; j++) {
-      sm.redW[warp][g][8 * j + 2 * t] = acc[j][0];
-      sm.redW[warp][g][8 * j + 2 * t + 1] = acc[j][1];
-      sm.redW[warp][g + 8][8 * j + 2 * t] = acc[j][2];
-      sm.redW[warp][g + 8][8 * j + 2 * t + 1] = acc[j][3];
-    }
+  for (int j = 0; j < 2; j++) {
+    sm.redW[warp][g][8 * j + 2 * t] = acc[j][0];
+    sm.redW[warp][g][8 * j + 2 * t + 1] = acc[j][1];
+    sm.redW[warp][g + 8][8 * j + 2 * t] = acc[j][2];
+    sm.redW[warp][g + 8][8 * j + 2 * t + 1] = acc[j][3];
   }
   __syncthreads();
   {
-    const int a = tid & 15, cc = tid >> 4;
-    double acc = 0.0;
+    const int ai = tid & 15, cc = tid >> 4;
+    double s2 = 0.0;
 #pragma unroll
-    for (int k = 0; k < BW; k++) acc += sm.redW[k][a][cc];
-    sm.W[a][cc] = acc;
+    for (int k = 0; k < BW; k++) s2 += sm.redW[k][ai][cc];
+    sm.W[ai][cc] = s2;
   }
   __syncthreads();
-  {  // -(T^T W)
-    const int a = tid & 15, cc = tid >> 4;
-    double acc = 0.0;
+  {  // -(T^T W); T is zero below its diagonal
+    const int ai = tid & 15, cc = tid >> 4;
+    double s2 = 0.0;
 #pragma unroll
-    for (int b = 0; b < 16; b++) acc = fma(sm.T[b][a], sm.W[b][cc], acc);  // T zero below diag
-    sm.redW[0][a][cc] = -acc;
+    for (int b = 0; b < 16; b++) s2 = fma(sm.T[b][ai], sm.W[b][cc], s2);
+    sm.redW[0][ai][cc] = -s2;
   }
   __syncthreads();
-  {  // C += V W over this warp's rows
-    constexpr int RW = MP / BW;
+#pragma unroll 1
+  for (int p = 0; p < NP; p++) {
+    if (NP > 1) {  // one pass: sV and sC still hold it
+      stage_v<R, VREG>(sV, a, P, ldp, m, wv, p);
+      stage_c<R>(sC, C, ld, m, w, p);
+      __syncthreads();
+    }
+    constexpr int RW = PR / BW;
 #pragma unroll 1
     for (int m0 = warp * RW; m0 < (warp + 1) * RW; m0 += 16) {
 #pragma unroll
       for (int j = 0; j < 2; j++) {
-        double acc[4];
-        acc[0] = sC[(m0 + g) * MS + 8 * j + 2 * t];
-        acc[1] = sC[(m0 + g) * MS + 8 * j + 2 * t + 1];
-        acc[2] = sC[(m0 + g + 8) * MS + 8 * j + 2 * t];
-        acc[3] = sC[(m0 + g + 8) * MS + 8 * j + 2 * t + 1];
+        double d[4];
+        d[0] = sC[(m0 + g) * MS + 8 * j + 2 * t];
+        d[1] = sC[(m0 + g) * MS + 8 * j + 2 * t + 1];
+        d[2] = sC[(m0 + g + 8) * MS + 8 * j + 2 * t];
+        d[3] = sC[(m0 + g + 8) * MS + 8 * j + 2 * t + 1];
 #pragma unroll
-        for (int k4 = 0; k4 < 16; k4 += 4)
-          dmma_16x8x4(acc, sV[(m0 + g) * MS + k4 + t], sV[(m0 + g + 8) * MS + k4 + t],
-                      sm.redW[0][k4 + t][8 * j + g]);
+        for (int k8 = 0; k8 < 16; k8 += 8)
+          dmma_16x8x8(d, sV[(m0 + g) * MS + k8 + t], sV[(m0 + g + 8) * MS + k8 + t],
+                      sV[(m0 + g) * MS + k8 + t + 4], sV[(m0 + g + 8) * MS + k8 + t + 4],
+                      sm.redW[0][k8 + t][8 * j + g], sm.redW[0][k8 + t + 4][8 * j + g]);
         const int c0 = 8 * j + 2 * t;
 #pragma unroll
         for (int h = 0; h < 2; h++) {
-          const int r = m0 + g + 8 * h;
-          if (r < m) {
-            if (c0 < w) __stcg(C + cm(r, c0, ld), acc[2 * h]);
-            if (c0 + 1 < w) __stcg(C + cm(r, c0 + 1, ld), acc[2 * h + 1]);
+          const int lr = m0 + g + 8 * h;            // row inside the pass
+          const int i = p * Pass<R>::SL + lr / BT;  // its thread-owned row slice
+          const int rr = (lr % BT) + BT * i;        // row of the leaf
+          if (i < R && rr < m) {
+            if (c0 < w) __stcg(C + cm(rr, c0, ld), d[2 * h]);
+            if (c0 + 1 < w) __stcg(C + cm(rr, c0 + 1, ld), d[2 * h + 1]);
           }
         }
       }
     }
+    __syncthreads();
   }
-  __syncthreads();
 }
 
 // Materialise the unit lower trapezoidal V of a factored leaf held in a.
@@ -607,9 +671,10 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
       for (int e = tid; e < NB * (NB + 1); e += BT) (&sm.T[0][0])[e] = 0.0;
       if (tid < 2 * NB) (&sm.gsh[0][0])[tid] = 0.0;
       __syncthreads();
-      // 16-wide leaves are factored by 4 warps with 2R rows per thread (the
-      // per-column shuffle reduction costs per warp); the other warps wait.
-      constexpr int FW = (NB == 16) ? 4 : BW;
+      // 16-wide leaves of at most 2*BT rows are factored by 4 warps with 2R
+      // rows per thread (the per-column shuffle reduction costs per warp);
+      // taller leaves use all warps.  The other warps wait.
+      constexpr int FW = (NB == 16 && R <= 2) ? 4 : BW;
       constexpr int FR = R * BW / FW;
       double a[FR][NB];
       if (tid < FW * 32) {
@@ -628,15 +693,13 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
 #pragma unroll
             for (int c = 0; c < NB; c++)
               if (c < f.w) __stcg(P + cm(r, c, st.ld), a[i][c]);
-            if constexpr (NB == 16) {  // reflectors for the next-tile update
+          }
+          if constexpr (NB == 16 && Pass<R>::NP == 1) {  // reflectors for the next-tile update
+            if (r < Pass<R>::ROWS) {
 #pragma unroll
               for (int c = 0; c < 16; c++)
-                sC[r * MS + c] = (c >= f.w) ? 0.0 : (r == c ? 1.0 : (r > c ? a[i][c] : 0.0));
-            }
-          } else if constexpr (NB == 16) {
-            if (r < R * BT) {
-#pragma unroll
-              for (int c = 0; c < 16; c++) sC[r * MS + c] = 0.0;
+                sC[r * MS + c] = (r >= mrows || c >= f.w) ? 0.0
+                                 : (r == c ? 1.0 : (r > c ? a[i][c] : 0.0));
             }
           }
         }
@@ -666,7 +729,11 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
         const int w2 = min(g.NB, g.n - t2 * g.NB);
         if (tid == 0) st.timeline[4 * s + 3] = gtimer();
         if constexpr (NB == 16) {
-          apply_qt_mma<R>(sC, sC + R * BT * MS, C, ldc, mrows, w2, sm);
+          // The factored leaf is re-read from L2 (just written by this CTA)
+          // rather than from the factor's register layout.
+          double none[R][16];
+          apply_qt_mma<R, false, Pass<R>::NP == 1>(sC, sC + Pass<R>::ROWS * MS, none, P, st.ld,
+                                                   f.w, C, ldc, mrows, w2, sm);
         } else {
           double v[R][NB];
           leaf_to_v<R, NB>(a, v, mrows, f.w);
@@ -712,16 +779,10 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
     double* C = tile_ptr(g, st.A, st.ld, st.G, f.k, f.j0, m2, t2, ldc);
     const int w2 = min(g.NB, g.n - t2 * g.NB);
     if constexpr (NB == 16) {
-#pragma unroll
-      for (int i = 0; i < R; i++) {
-        const int r = tid + BT * i;
-#pragma unroll
-        for (int c = 0; c < 16; c++)
-          sC[r * MS + c] = (r >= mrows || c >= f.w) ? 0.0
-                           : (r == c ? 1.0 : (r > c ? __ldcg(P + cm(r, c, st.ld)) : 0.0));
-      }
       if (!block_wait_geq(st, st.cnt + x2, s - lo2, &sm.flag)) return;
-      apply_qt_mma<R>(sC, sC + R * BT * MS, C, ldc, mrows, w2, sm);
+      double none[R][16];
+      apply_qt_mma<R, false>(sC, sC + Pass<R>::ROWS * MS, none, P, st.ld, f.w, C, ldc, mrows, w2,
+                             sm);
     } else {
       double v[R][NB];
       {
@@ -740,15 +801,18 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
 }
 
 // ------------------------------------------------------------------ launcher
-// 16-wide leaves keep V and C rows in registers up to 2n = 512 rows; wider
-// panels use 8-wide leaves (up to 2n = 1536 rows, six rows per thread).
+// 16-wide leaves (DMMA block-reflector update, one 512-row staging pass) up
+// to 2n = 512 rows; taller panels use 8-wide leaves (up to 2n = 1536 rows,
+// six rows per thread), whose CUDA-core update streams rows from registers.
+// (16-wide leaves with two staging passes measured slower at n = 400.)
 int bsof_leaf_width(int n) { return n <= 256 ? 16 : 8; }
 
 int bsof_tiles(int n) { return (n + bsof_leaf_width(n) - 1) / bsof_leaf_width(n); }
 
 template <int R, int NB>
 static size_t dyn_smem() {
-  return NB == 16 ? sizeof(double) * 2 * (size_t)R * BT * MS : sizeof(double) * (size_t)NB * R * BT;
+  return NB == 16 ? sizeof(double) * 2 * (size_t)Pass<R>::ROWS * MS
+                  : sizeof(double) * (size_t)NB * R * BT;
 }
 
 template <int R, int NB>

@@ -23,6 +23,8 @@ cudaError_t gemm_init_attributes() {
   cudaError_t e;
   if ((e = set_attr<CfgL, true>()) != cudaSuccess) return e;
   if ((e = set_attr<CfgL, false>()) != cudaSuccess) return e;
+  if ((e = set_attr<CfgM, true>()) != cudaSuccess) return e;
+  if ((e = set_attr<CfgM, false>()) != cudaSuccess) return e;
   if ((e = set_attr<CfgS, true>()) != cudaSuccess) return e;
   if ((e = set_attr<CfgS, false>()) != cudaSuccess) return e;
   done = true;
@@ -53,9 +55,10 @@ cudaError_t launch_gemm(const GemmDims& d, const GemmA& a, const GemmB& b, const
   if (e != cudaSuccess) return e;
   if (cfg == 0) {
     long long tilesL = (long long)((d.M + 127) / 128) * ((d.N + 127) / 128) * batch;
-    cfg = (tilesL >= 148) ? 1 : 2;
+    cfg = (tilesL >= 148) ? 3 : 2;
   }
   if (cfg == 1) return run<CfgL>(d, a, b, c, batch, st);
+  if (cfg == 3) return run<CfgM>(d, a, b, c, batch, st);
   return run<CfgS>(d, a, b, c, batch, st);
 }
 
