@@ -13,7 +13,7 @@ data path); value = inversions by all ranks / max-over-ranks device time.
 
 Printed JSON line (rank 0): value (device-resident inversions/s), tflops
 (flop model of include/bsofi_flops.h), roofline of the dominant kernel (the
-BSOI step GEMM, FP64 DMMA, against cuBLAS DGEMM measured in the same run),
+persistent BSOI kernel, FP64 DMMA, against cuBLAS DGEMM measured in the same run),
 e2e (the reference handle API hybridxbsoftrih_ + hybridxbsoih_ on host
 buffers, copies included), cpu_baseline (the reference's CPU path,
 oracle/_ref, on the host cores), clocks sampled during the timed region.
@@ -196,8 +196,8 @@ def bsof_chain_ms(api, n, L, ldd, ws):
 
 
 def traffic_per_launch():
-    """DRAM bytes per BSOI GEMM launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "bsoi_gemm_traffic.json")
+    """DRAM bytes per BSOI launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "bsoi_persistent_traffic.json")
     if os.path.exists(path):
         try:
             return json.load(open(path)).get("dram_bytes_per_launch")
@@ -336,14 +336,15 @@ def main():
 
     peak = measure_dgemm_peak(torch, dev)
     achieved = flops_bsoi(n, L) * args.steps / (gemm_ms * 1e-3) / 1e12 if gemm_ms > 0 else None
-    roofline = {"kernel": "BSOI step GEMM (gemm_kernel, FP64 DMMA m16n8k8); dominant by "
-                          "algorithmic work (79% of the flop model)",
+    roofline = {"kernel": "bsoi_persistent_kernel (all p-1 BSOI steps in one cooperative "
+                          "launch, FP64 DMMA m16n8k8); dominant by algorithmic work "
+                          "(79% of the flop model)",
                 "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if achieved else None,
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor)",
                 "launches": gemm_launches,
                 "avg_launch_ms": gemm_ms / max(gemm_launches, 1),
-                "algorithmic_flops_per_launch": flops_bsoi(n, L) / (L - 1),
+                "algorithmic_flops_per_launch": flops_bsoi(n, L) * args.steps / max(gemm_launches, 1),
                 "traffic": traffic_per_launch()}
     # The persistent BSOF kernel is the largest share of device time: a serial
     # Householder chain, latency bound.  Reported against HBM as the panels'

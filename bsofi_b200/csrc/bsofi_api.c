@@ -199,6 +199,8 @@ static cudaError_t ctx_fit(bsofi_ctx *c, int n, int L) {
   if ((e = cudaMalloc((void **)&c->dtau, sizeof(double) * (size_t)N)) != cudaSuccess) goto fail;
   c->ws_bytes = bsofi_dev_ws_bytes(n, L, ldd);
   if ((e = cudaMalloc(&c->dws, c->ws_bytes)) != cudaSuccess) goto fail;
+  /* info words (BSTRI info, BSOF and BSOI error words) start cleared */
+  if ((e = cudaMemset(c->dws, 0, 256)) != cudaSuccess) goto fail;
   c->n = n;
   c->L = L;
   c->ldd = ldd;
@@ -399,10 +401,11 @@ static int check_args(const int *h_ok, int n, int L, const double *A, int lda,
   return 0;
 }
 
-/* Reads the BSTRI info word and the BSOF error word (a bounded wait inside
- * the persistent BSOF kernel that gave up) after synchronising the stream. */
+/* Reads the BSTRI info word and the BSOF and BSOI error words (a bounded
+ * wait inside a persistent kernel that gave up) after synchronising the
+ * stream. */
 static int read_info(bsofi_ctx *c, int *info) {
-  int v[2] = {0, 0};
+  int v[3] = {0, 0, 0};
   cudaError_t e = cudaMemcpyAsync(v, bsofi_dev_info_ptr(c->dws), sizeof(v),
                                   cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
@@ -410,11 +413,11 @@ static int read_info(bsofi_ctx *c, int *info) {
     *info = cuda_info(e);
     return *info;
   }
-  if (v[1] != 0) {
+  if (v[1] != 0 || v[2] != 0) {
     *info = cuda_info(cudaErrorLaunchTimeout);
     return *info;
   }
-  *info = (v[0] >= 0x7f7f7f7f || v[0] < 0) ? 0 : v[0];
+  *info = v[0] >= 0x7f7f7f7f ? 0 : v[0];
   return *info;
 }
 
@@ -461,7 +464,11 @@ static int drive_bsoi(bsofi_ctx *c, int n, int L, double *A, int lda, const doub
   e = (cudaError_t)bsofi_dev_bsoi(n, L, c->dA, c->ldd, c->dtau, c->dws, c->stream);
   if (e != cudaSuccess) return cuda_info(e);
   e = d2h_cols(c, A, lda, c->dA, c->ldd, N, N);
-  return e == cudaSuccess ? 0 : cuda_info(e);
+  if (e != cudaSuccess) return cuda_info(e);
+  {
+    int info = 0;
+    return read_info(c, &info) < 0 ? info : 0;
+  }
 }
 
 /* ================================================================ handle API */

@@ -44,8 +44,9 @@ int bsofi_dev_invert_ex(int n, int L, double *dA, int ldd, double *dtau, void *d
 int bsofi_dev_bsoi(int n, int L, double *dA, int ldd, const double *dtau, void *dws,
                    void *stream);
 
-/* Device address of the int info word inside the workspace (0 = ok,
- * i > 0: R(i,i) exactly zero, 1-based global index). */
+/* Device address of the int info words inside the workspace: [0] BSTRI info
+ * (values >= 0x7f7f7f7f mean 0; i > 0: R(i,i) exactly zero, 1-based global
+ * index), [1] BSOF wait timeout, [2] BSOI wait timeout (nonzero = error). */
 int *bsofi_dev_info_ptr(void *dws);
 
 /* Number of kernels the last bsofi_dev_* call on this thread launched. */

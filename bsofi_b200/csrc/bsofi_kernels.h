@@ -34,6 +34,13 @@ cudaError_t launch_bsof_persistent(double* A, long long ld, int n, int L, double
                                    int* next_task, int* err, unsigned long long* timeline,
                                    int workers, cudaStream_t st);
 
+// Persistent BSOI (kernels_bsoi.cu): all p-1 steps in one cooperative launch.
+// done: (L-1) * bsoi_row_bands(N) ints and next: one int, zeroed before.
+int bsoi_row_bands(int N);
+cudaError_t launch_bsoi_persistent(double* A, long long ld, double* carry0, double* carry1,
+                                   long long ldc, const double* G, int n, int L, int* done,
+                                   int* next, int* err, cudaStream_t st);
+
 cudaError_t launch_trtri_blocks(double* A, long long ld, int n, long long bstride,
                                 int nblk, int* info, cudaStream_t st);
 
@@ -44,9 +51,15 @@ cudaError_t gemm_init_attributes();
 
 cudaError_t launch_set_identity(double* G, long long ld, int m, long long bs, int batch,
                                 cudaStream_t st);
+// Info word value when a bounded wait inside a persistent kernel gave up:
+// BSOFI_INFO_CUDA - cudaErrorLaunchTimeout.
+constexpr int kInfoWaitFailed = -1000 - (int)cudaErrorLaunchTimeout;
 // dst(r,c) = src(r,c), or 0 where r - roff > c (roff = kNoMask copies all).
+// fold (optional): info words {info, BSOF error, BSOI error}; info becomes
+// kInfoWaitFailed when either error word is set.
 cudaError_t launch_copy_masked(double* dst, long long ldd, const double* src, long long lds,
-                               int rows, int cols, int roff, cudaStream_t st);
+                               int rows, int cols, int roff, cudaStream_t st,
+                               int* fold = nullptr);
 // Zero the n x n blocks of A that BSOF reads as structural zeros:
 // superdiagonal blocks (k,k+1) and last-column blocks (k,L-1), 1 <= k <= L-2.
 cudaError_t launch_zero_structural(double* A, long long ld, int n, int L, cudaStream_t st);

@@ -1,0 +1,154 @@
+// BSOI as one persistent kernel: all p-1 steps X(:,k:k+1) <- X(:,k:k+1) Q_k^T.
+//
+// Reference: lapackXbsoi_ormqr / _orgqr, src/bsofi_cpu.c:211-333 (applied
+// from k = L-2 down to 0).  Step k is the product
+//   [X(:,k) | carry] (N x 2n) * Q_k^T (2n x 2n)  ->  [carry' | X(:,k+1) final]
+// on 128 x 128 output tiles.  Rows are independent across steps, so a tile of
+// step k only waits for the tiles of step k+1 in the same row band (they wrote
+// the carry it reads and read the buffers it overwrites), not for the whole
+// step: there is no per-step wave tail and no launch gap.  Tiles are claimed
+// in (step, row band, column) order from a global counter; every wait is on
+// an earlier tile, all CTAs are co-resident (cooperative launch), and every
+// spin is bounded and reports through an error word.
+#include <climits>
+#include "bsofi_common.cuh"
+#include "bsofi_kernels.h"
+
+namespace bsofi {
+
+struct BsoiArgs {
+  double* A;
+  long long ld;
+  double* carry[2];  // ldd x n each; the carry written by step k is carry[(L-1-k) & 1]
+  long long ldc;
+  const double* G;   // (L-1) x (2n)^2, G_k = Q_k^T
+  int n, L, N;
+  int* done;         // (L-1) x row bands: finished column tiles
+  int* next;         // tile counter
+  int* err;
+  long long spin_limit;
+};
+
+BSOFI_DEVINL int ld_acq(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+template <class Cfg, bool ALIGNED>
+__global__ void __launch_bounds__(Cfg::THREADS, 1) bsoi_persistent_kernel(BsoiArgs s) {
+  extern __shared__ __align__(16) double smem_bsoi[];
+  __shared__ int s_tile, s_ok;
+  const int n2 = 2 * s.n;
+  const int RT = (s.N + Cfg::BM - 1) / Cfg::BM, CT = (n2 + Cfg::BN - 1) / Cfg::BN;
+  const long long total = (long long)(s.L - 1) * RT * CT;
+  for (;;) {
+    __syncthreads();  // the previous tile's shared memory is no longer read
+    if (threadIdx.x == 0) s_tile = atomicAdd(s.next, 1);
+    __syncthreads();
+    const long long tile = s_tile;
+    if (tile >= total) return;
+    const int step = (int)(tile / ((long long)RT * CT));  // 0 = k = L-2
+    const int rem = (int)(tile % ((long long)RT * CT));
+    const int rb = rem / CT, cb = rem % CT;
+    const int k = s.L - 2 - step;
+    if (step > 0) {
+      if (threadIdx.x == 0) {
+        const int* flag = s.done + (long long)(step - 1) * RT + rb;
+        long long it = 0;
+        int ok = 1;
+        while (ld_acq(flag) < CT) {
+          if (ld_acq(s.err) != 0 || ++it > s.spin_limit) {
+            atomicExch(s.err, 1);
+            ok = 0;
+            break;
+          }
+          __nanosleep(64);
+        }
+        s_ok = ok;
+      }
+      __syncthreads();
+      if (!s_ok) return;
+    }
+    GemmDims d = {s.N, n2, n2};
+    GemmA a;
+    a.p0 = s.A + cm(0, (long long)k * s.n, s.ld);
+    a.ld0 = s.ld;
+    a.p1 = s.carry[(s.L - 2 - k) & 1];
+    a.ld1 = s.ldc;
+    a.bs0 = a.bs1 = 0;
+    a.ksplit = s.n;
+    a.rlim0 = (k + 1) * s.n;
+    a.roff0 = k * s.n;
+    a.rlim1 = INT_MAX;
+    a.roff1 = kNoMask;
+    GemmB b = {s.G + (long long)k * n2 * n2, n2, 0, kNoMask};
+    GemmC c;
+    c.p0 = s.carry[(s.L - 1 - k) & 1];
+    c.ld0 = s.ldc;
+    c.p1 = s.A + cm(0, (long long)(k + 1) * s.n, s.ld);
+    c.ld1 = s.ld;
+    c.bs0 = c.bs1 = 0;
+    c.nsplit = s.n;
+    c.alpha = 1.0;
+    c.beta0 = c.beta1 = 0.0;
+    gemm_tile<Cfg, ALIGNED>(d, a, b, c, rb * Cfg::BM, cb * Cfg::BN, 0, smem_bsoi);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(s.done + (long long)step * RT + rb)
+                   : "memory");
+    }
+  }
+}
+
+int bsoi_row_bands(int N) { return (N + CfgM::BM - 1) / CfgM::BM; }
+
+template <bool AL>
+static cudaError_t launch_al(const BsoiArgs& s, cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(bsoi_persistent_kernel<CfgM, AL>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)CfgM::SMEM);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bsoi_persistent_kernel<CfgM, AL>,
+                                                CfgM::THREADS, CfgM::SMEM);
+  const int RT = bsoi_row_bands(s.N), CT = (2 * s.n + CfgM::BN - 1) / CfgM::BN;
+  long long tiles = (long long)(s.L - 1) * RT * CT;
+  int grid = sms * (per > 0 ? per : 1);
+  if (tiles < grid) grid = (int)tiles;
+  void* args[] = {(void*)&s};
+  return cudaLaunchCooperativeKernel((const void*)bsoi_persistent_kernel<CfgM, AL>, dim3(grid),
+                                     dim3(CfgM::THREADS), args, CfgM::SMEM, st);
+}
+
+cudaError_t launch_bsoi_persistent(double* A, long long ld, double* carry0, double* carry1,
+                                   long long ldc, const double* G, int n, int L, int* done,
+                                   int* next, int* err, cudaStream_t st) {
+  BsoiArgs s;
+  s.A = A;
+  s.ld = ld;
+  s.carry[0] = carry0;
+  s.carry[1] = carry1;
+  s.ldc = ldc;
+  s.G = G;
+  s.n = n;
+  s.L = L;
+  s.N = n * L;
+  s.done = done;
+  s.next = next;
+  s.err = err;
+  s.spin_limit = 1ll << 22;
+  const bool al = ((uintptr_t)A % 16 == 0) && ((uintptr_t)carry0 % 16 == 0) &&
+                  ((uintptr_t)carry1 % 16 == 0) && ((uintptr_t)G % 16 == 0) && ld % 2 == 0 &&
+                  ldc % 2 == 0 && n % 2 == 0;
+  return al ? launch_al<true>(s, st) : launch_al<false>(s, st);
+}
+
+}  // namespace bsofi

@@ -137,7 +137,11 @@ cudaError_t launch_set_identity(double* G, long long ld, int m, long long bs, in
 }
 
 __global__ void copy_masked_kernel(double* dst, long long ldd, const double* src, long long lds,
-                                   int rows, int cols, int roff) {
+                                   int rows, int cols, int roff, int* fold) {
+  // fold (optional): the workspace info words {BSTRI info, BSOF error, BSOI
+  // error}; a bounded wait that gave up turns the info word into an error.
+  if (fold != nullptr && blockIdx.x == 0 && threadIdx.x == 0 && (fold[1] | fold[2]) != 0)
+    fold[0] = kInfoWaitFailed;
   long long total = (long long)rows * cols;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
@@ -148,11 +152,11 @@ __global__ void copy_masked_kernel(double* dst, long long ldd, const double* src
 }
 
 cudaError_t launch_copy_masked(double* dst, long long ldd, const double* src, long long lds,
-                               int rows, int cols, int roff, cudaStream_t st) {
+                               int rows, int cols, int roff, cudaStream_t st, int* fold) {
   long long total = (long long)rows * cols;
   if (total <= 0) return cudaSuccess;
   int gx = (int)min((total + 255) / 256, (long long)4096);
-  copy_masked_kernel<<<gx, 256, 0, st>>>(dst, ldd, src, lds, rows, cols, roff);
+  copy_masked_kernel<<<gx, 256, 0, st>>>(dst, ldd, src, lds, rows, cols, roff, fold);
   return cudaGetLastError();
 }
 

@@ -67,13 +67,14 @@ extern "C" __attribute__((visibility("default"))) int bsofi_device_invert_noallo
   if (e != cudaSuccess) return BSOFI_INFO_CUDA - (int)e;
   int r = bsofi_dev_prepare();
   if (r == 0) r = bsofi_dev_bsoftri(n, L, dA, ldda, dtau, ws, stream);
-  if (r == 0 && dinfo != nullptr)
-    r = (int)cudaMemcpyAsync(dinfo, bsofi_dev_info_ptr(ws), sizeof(int), cudaMemcpyDeviceToDevice,
-                             (cudaStream_t)stream);
   if (r == 0) {
     long long c = bsofi_dev_launch_count();
     r = bsofi_dev_bsoi(n, L, dA, ldda, dtau, ws, stream);
     bsofi_dev_add_launches(c);
   }
+  // The info word after BSOI also carries the BSOF/BSOI wait error.
+  if (r == 0 && dinfo != nullptr)
+    r = (int)cudaMemcpyAsync(dinfo, bsofi_dev_info_ptr(ws), sizeof(int), cudaMemcpyDeviceToDevice,
+                             (cudaStream_t)stream);
   return r ? BSOFI_INFO_CUDA - r : 0;
 }

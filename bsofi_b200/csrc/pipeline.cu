@@ -40,8 +40,8 @@ struct GemmTimer {
 thread_local GemmTimer g_timer;
 
 struct Layout {
-  size_t info, sync, tl, T, G, W, Y, C0, C1, total;
-  int nbw, maxleaves, tiles, leaves, sync_ints;
+  size_t info, sync, bsync, tl, T, G, W, Y, C0, C1, total;
+  int nbw, maxleaves, tiles, leaves, sync_ints, bsync_ints;
 };
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
@@ -58,6 +58,9 @@ Layout layout(int n, int L, int ldd) {
   off += 256;
   l.sync = off;  // tile counters, leaf flags, task counter, spare
   off += align256(sizeof(int) * (size_t)l.sync_ints);
+  l.bsync_ints = (L - 1) * bsoi_row_bands(n * L) + 2;
+  l.bsync = off;  // BSOI: finished tiles per (step, row band), tile counter
+  off += align256(sizeof(int) * (size_t)l.bsync_ints);
   l.tl = off;    // BSOF timeline: 4 globaltimer stamps per leaf
   off += align256(sizeof(unsigned long long) * 4 * (size_t)l.leaves);
   l.T = off;
@@ -315,33 +318,47 @@ int run_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* ws, cu
   // Carry for the first step: X(:, L-1) with the triangular diagonal block.
   CK(launch_copy_masked(C[0], ldd, dA + cm(0, (long long)(L - 1) * n, ldd), ldd, N, n,
                         (L - 1) * n, st));
-  int cur = 0;
-  for (int k = L - 2; k >= 0; k--) {
-    GemmDims d = {N, n2, n2};
-    GemmA a = {};
-    a.p0 = dA + cm(0, (long long)k * n, ldd);
-    a.ld0 = ldd;
-    a.p1 = C[cur];
-    a.ld1 = ldd;
-    a.ksplit = n;
-    a.rlim0 = (k + 1) * n;
-    a.roff0 = k * n;
-    a.rlim1 = INT_MAX;
-    a.roff1 = kNoMask;
-    GemmB b = {G + (size_t)k * g2, n2, 0, kNoMask};
-    GemmC c = {};
-    c.p0 = C[cur ^ 1];
-    c.ld0 = ldd;
-    c.p1 = dA + cm(0, (long long)(k + 1) * n, ldd);
-    c.ld1 = ldd;
-    c.nsplit = n;
-    c.alpha = 1.0;
+  int* err = at<int>(ws, ly.info) + 2;
+  CKM(cudaMemsetAsync(err, 0, sizeof(int), st));
+  const int row_bands = bsoi_row_bands(N), col_tiles = (n2 + 127) / 128;
+  if (row_bands * col_tiles >= 64) {
+    // One persistent launch over all steps (rows flow from step to step).
+    int* bs = at<int>(ws, ly.bsync);
+    CKM(cudaMemsetAsync(bs, 0, sizeof(int) * ly.bsync_ints, st));
     if (g_timer.on) CKM(g_timer.mark(st));
-    CK(launch_gemm(d, a, b, c, 1, 0, st));
+    CK(launch_bsoi_persistent(dA, ldd, C[0], C[1], ldd, G, n, L, bs, bs + ly.bsync_ints - 2, err,
+                              st));
     if (g_timer.on) CKM(g_timer.mark(st));
-    cur ^= 1;
+  } else {
+    // Small problems: one launch per step with small tiles (more CTAs per step).
+    for (int k = L - 2; k >= 0; k--) {
+      const int rd = (L - 2 - k) & 1;
+      GemmDims d = {N, n2, n2};
+      GemmA a = {};
+      a.p0 = dA + cm(0, (long long)k * n, ldd);
+      a.ld0 = ldd;
+      a.p1 = C[rd];
+      a.ld1 = ldd;
+      a.ksplit = n;
+      a.rlim0 = (k + 1) * n;
+      a.roff0 = k * n;
+      a.rlim1 = INT_MAX;
+      a.roff1 = kNoMask;
+      GemmB b = {G + (size_t)k * g2, n2, 0, kNoMask};
+      GemmC c = {};
+      c.p0 = C[rd ^ 1];
+      c.ld0 = ldd;
+      c.p1 = dA + cm(0, (long long)(k + 1) * n, ldd);
+      c.ld1 = ldd;
+      c.nsplit = n;
+      c.alpha = 1.0;
+      if (g_timer.on) CKM(g_timer.mark(st));
+      CK(launch_gemm(d, a, b, c, 1, 0, st));
+      if (g_timer.on) CKM(g_timer.mark(st));
+    }
   }
-  CK(launch_copy_masked(dA, ldd, C[cur], ldd, N, n, kNoMask, st));
+  const int cur = (L - 1) & 1;  // carry buffer written by step 0
+  CK(launch_copy_masked(dA, ldd, C[cur], ldd, N, n, kNoMask, st, at<int>(ws, ly.info)));
   return 0;
 }
 

@@ -149,7 +149,10 @@ unsigned long long bsofi_device_workspace_bytes(int n, int L, int ldda);
  * doubles), dwork device memory of bsofi_device_workspace_bytes.  dA must
  * hold the p-cyclic input with every other block zero.  Returns 0 or
  * BSOFI_INFO_CUDA - cudaError_t; the BSTRI info word is at
- * bsofi_device_info(dwork) (device int, values >= 0x7f7f7f7f mean 0). */
+ * bsofi_device_info(dwork) (device int, values >= 0x7f7f7f7f mean 0; after
+ * bsofi_device_invert or bsofi_device_bsoi it is BSOFI_INFO_CUDA -
+ * cudaErrorLaunchTimeout if a bounded wait inside a persistent kernel gave
+ * up; words 1 and 2 are the BSOF and BSOI wait error flags). */
 int bsofi_device_invert(int n, int L, double *dA, int ldda, double *dtau, void *dwork,
                         void *stream);
 int bsofi_device_bsoftri(int n, int L, double *dA, int ldda, double *dtau, void *dwork,
@@ -208,7 +211,8 @@ void bsofi_server_destroy(bsofi_server *server);
  * The first call on a device looks up the array's device address (with that
  * device current) and should come before any stream capture.  All calls share
  * the array: calls that overlap on the GPU race.  dinfo (device int, may be
- * NULL) receives the BSTRI info word (values >= 0x7f7f7f7f mean 0).
+ * NULL) receives the info word as bsofi_device_info describes it (values
+ * >= 0x7f7f7f7f mean 0).
  * Returns 0, -1 for an illegal argument, BSOFI_NOALLOC_TOO_LARGE, or
  * BSOFI_INFO_CUDA - cudaError_t. */
 #define BSOFI_NOALLOC_TOO_LARGE (-2000)
