@@ -7,9 +7,11 @@
 // step k only waits for the tiles of step k+1 in the same row band (they wrote
 // the carry it reads and read the buffers it overwrites), not for the whole
 // step: there is no per-step wave tail and no launch gap.  Tiles are claimed
-// in (step, row band, column) order from a global counter; every wait is on
-// an earlier tile, all CTAs are co-resident (cooperative launch), and every
-// spin is bounded and reports through an error word.
+// in (step, row band, column) order from a global counter and every wait is
+// on a tile claimed earlier, whose CTA is already running: progress needs no
+// co-residency, so the launch is an ordinary one (a cooperative launch would
+// wait for the whole GPU and serialise batched inversions on other streams).
+// Every spin is bounded and reports through an error word.
 #include <climits>
 #include "bsofi_common.cuh"
 #include "bsofi_kernels.h"
@@ -123,9 +125,8 @@ static cudaError_t launch_al(const BsoiArgs& s, cudaStream_t st) {
   long long tiles = (long long)(s.L - 1) * RT * CT;
   int grid = sms * (per > 0 ? per : 1);
   if (tiles < grid) grid = (int)tiles;
-  void* args[] = {(void*)&s};
-  return cudaLaunchCooperativeKernel((const void*)bsoi_persistent_kernel<CfgM, AL>, dim3(grid),
-                                     dim3(CfgM::THREADS), args, CfgM::SMEM, st);
+  bsoi_persistent_kernel<CfgM, AL><<<grid, CfgM::THREADS, CfgM::SMEM, st>>>(s);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_bsoi_persistent(double* A, long long ld, double* carry0, double* carry1,
