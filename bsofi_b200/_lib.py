@@ -67,6 +67,12 @@ _SIGS = {
     "bsofi_server_poll": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int]),
     "bsofi_server_pending": (ctypes.c_int, [_vp]),
     "bsofi_server_destroy": (None, [_vp]),
+    "bsofi_device_assemble": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp,
+                                             ctypes.c_int, _vp]),
+    "bsofi_device_hubbard_assemble": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp,
+                                                     ctypes.c_double, _vp, ctypes.c_int, _vp]),
+    "bsofi_device_logdet": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp,
+                                           ctypes.c_int, _vp, _vp]),
     "bsofi_noalloc_scratch_bytes": (ctypes.c_ulonglong, []),
     "bsofi_device_invert_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int,
                                                    _vp, _vp, _vp]),

@@ -120,6 +120,21 @@ def device_bsoi(n, L, dA, ldda, dtau, dwork, stream=0):
     return load().bsofi_device_bsoi(n, L, dA, ldda, dtau, dwork, stream)
 
 
+def device_assemble(n, L, dD, dS, dA, ldda, stream=0):
+    """bsofi_device_assemble: p-cyclic input from packed blocks (dD may be 0 = identity)."""
+    return load().bsofi_device_assemble(n, L, dD or None, dS, dA, ldda, stream)
+
+
+def device_hubbard_assemble(n, L, dExpK, dh, lam, dA, ldda, stream=0):
+    """bsofi_device_hubbard_assemble: the DQMC matrix from expm(dtau t K) and the fields."""
+    return load().bsofi_device_hubbard_assemble(n, L, dExpK, dh, float(lam), dA, ldda, stream)
+
+
+def device_logdet(n, L, dA, ldda, dtau, inverted, dout, stream=0):
+    """bsofi_device_logdet: dout[0] = sign(det M), dout[1] = log|det M|."""
+    return load().bsofi_device_logdet(n, L, dA, ldda, dtau, 1 if inverted else 0, dout, stream)
+
+
 def device_info_ptr(dwork):
     return load().bsofi_device_info(dwork)
 

@@ -34,7 +34,7 @@ cudaError_t launch_bsof_persistent(double* A, long long ld, int n, int L, double
                                    int* next_task, int* err, unsigned long long* timeline,
                                    int workers, cudaStream_t st);
 
-// Persistent BSOI (kernels_bsoi.cu): all p-1 steps in one cooperative launch.
+// Persistent BSOI (kernels_bsoi.cu): all p-1 steps in one launch.
 // done: (L-1) * bsoi_row_bands(N) ints and next: one int, zeroed before.
 int bsoi_row_bands(int N);
 cudaError_t launch_bsoi_persistent(double* A, long long ld, double* carry0, double* carry1,

@@ -163,6 +163,39 @@ int *bsofi_device_info(void *dwork);
 /* Kernels launched by the last bsofi_device_* call on this thread. */
 long long bsofi_device_last_launches(void);
 
+/* DQMC producer and consumer on the device (no reference counterpart: the
+ * reference takes the dense N x N matrix on the host and leaves the
+ * determinant to the caller, examples/ftest_hybrid/ftest_hybrid.f90:12-52
+ * and :141-145).
+ *
+ * bsofi_device_assemble writes the p-cyclic input into dA from packed blocks:
+ * dD holds the L diagonal blocks (n x n column-major, block k at dD + k n^2;
+ * NULL = identity blocks), dS the L coupling blocks, dS[k] placed at block
+ * (k+1, k) for k < L-1 and dS[L-1] at block (0, L-1).  It also zeroes the
+ * blocks the factorization reads as zeros; no other block is written (none
+ * other is read by bsofi_device_*).
+ *
+ * bsofi_device_hubbard_assemble builds the DQMC matrix itself: identity
+ * diagonal, -B_k at block (k, k-1) (k = 1..L-1) and +B_L at block (0, L-1),
+ * with B_k = dExpK diag(exp(lambda h_k)); dExpK is expm(dtau t K) (n x n,
+ * times exp(dtau mu) if mu != 0), dh the L x n fields (h_k = dh + (k-1) n).
+ *
+ * bsofi_device_logdet writes dout[0] = sign(det M) (+1, -1, or 0 when a
+ * diagonal entry of R is zero or not finite) and dout[1] = log|det M| from
+ * the factorization state: diag(dA) holds R_jj after bsofi_device_bsoftri's
+ * BSOF phase only (inverted = 0) or 1/R_jj after BSTRI (inverted = 1, the
+ * state bsofi_device_bsoftri and hybridxbsoftrih_ leave), and
+ * sign(det M) = (-1)^{#(tau_j != 0)} prod sign(R_jj).  (The reference example
+ * flips the sign for tau_j == 0 instead; the two agree when N is even.)
+ * All three enqueue on `stream` and return 0, -1 for an illegal argument or
+ * BSOFI_INFO_CUDA - cudaError_t. */
+int bsofi_device_assemble(int n, int L, const double *dD, const double *dS, double *dA, int ldda,
+                          void *stream);
+int bsofi_device_hubbard_assemble(int n, int L, const double *dExpK, const double *dh,
+                                  double lambda, double *dA, int ldda, void *stream);
+int bsofi_device_logdet(int n, int L, const double *dA, int ldda, const double *dtau,
+                        int inverted, double *dout, void *stream);
+
 /* Batched inversion of `count` independent matrices (no reference
  * counterpart: the reference inverts one walker per call).  Instance i has
  * block size n[i], L[i] blocks, device matrix dA[i] (ldda[i]) and device tau
