@@ -502,6 +502,10 @@ struct Pass {
   static constexpr int SL = R >= 2 ? 2 : 1;      // row slices per pass
   static constexpr int ROWS = SL * BT;           // staged rows per pass
   static constexpr int NP = (R + SL - 1) / SL;   // passes
+  // V is staged column-major with this column stride (ROWS + 4: 4 mod 16
+  // doubles), so that writes of whole rows by their owning threads and both
+  // DMMA fragment patterns read below are free of bank conflicts.
+  static constexpr int SV = ROWS + 4;
 };
 
 // Fill the staged V rows of pass p.  From registers (the factoring CTA) when
@@ -523,22 +527,32 @@ BSOFI_DEVINL void stage_v(double* sV, const double (&a)[R][16], const double* P,
         if (r == c) v = 1.0;
         else if (r > c) v = VREG ? a[i < R ? i : 0][c] : __ldcg(P + cm(r, c, ld));
       }
-      sV[lr * MS + c] = v;
+      sV[c * Pass<R>::SV + lr] = v;
     }
   }
 }
 
+// Staged C of pass p: row-major with stride MS.  Each warp instruction copies
+// an 8-row x 4-column block (lane = 4 * row + column), which reads four 64-byte
+// column segments from global memory and writes shared memory without bank
+// conflicts.  Staged row lr is row p * ROWS + lr of the tile.
 template <int R>
 BSOFI_DEVINL void stage_c(double* sC, const double* C, long long ld, int m, int w, int p) {
-  constexpr int SL = Pass<R>::SL;
-  const int tid = threadIdx.x;
+  constexpr int PR = Pass<R>::ROWS, NB8 = PR / 8 * 4 / BW;  // blocks per warp
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int rg = lane >> 2, cg = lane & 3;
+  double v[NB8];
 #pragma unroll
-  for (int j = 0; j < SL; j++) {
-    const int i = p * SL + j;
-    const int lr = tid + BT * j, r = tid + BT * i;
+  for (int q = 0; q < NB8; q++) {
+    const int b = warp + BW * q;
+    const int lr = (b >> 2) * 8 + rg, cc = (b & 3) * 4 + cg;
+    const int r = p * PR + lr;
+    v[q] = (r < m && cc < w) ? __ldcg(C + cm(r, cc, ld)) : 0.0;
+  }
 #pragma unroll
-    for (int cc = 0; cc < 16; cc++)
-      sC[lr * MS + cc] = (i < R && r < m && cc < w) ? __ldcg(C + cm(r, cc, ld)) : 0.0;
+  for (int q = 0; q < NB8; q++) {
+    const int b = warp + BW * q;
+    sC[((b >> 2) * 8 + rg) * MS + (b & 3) * 4 + cg] = v[q];
   }
 }
 
@@ -567,8 +581,9 @@ BSOFI_DEVINL void apply_qt_mma(double* sV, double* sC, const double (&a)[R][16],
     const int r0 = warp * KW;
 #pragma unroll 2
     for (int k0 = r0; k0 < r0 + KW; k0 += 8) {
-      const double a0 = sV[(k0 + t) * MS + g], a1 = sV[(k0 + t) * MS + g + 8];
-      const double a2 = sV[(k0 + t + 4) * MS + g], a3 = sV[(k0 + t + 4) * MS + g + 8];
+      constexpr int SV = Pass<R>::SV;
+      const double a0 = sV[g * SV + k0 + t], a1 = sV[(g + 8) * SV + k0 + t];
+      const double a2 = sV[g * SV + k0 + t + 4], a3 = sV[(g + 8) * SV + k0 + t + 4];
       dmma_16x8x8(acc[0], a0, a1, a2, a3, sC[(k0 + t) * MS + g], sC[(k0 + t + 4) * MS + g]);
       dmma_16x8x8(acc[1], a0, a1, a2, a3, sC[(k0 + t) * MS + 8 + g],
                   sC[(k0 + t + 4) * MS + 8 + g]);
@@ -616,10 +631,11 @@ BSOFI_DEVINL void apply_qt_mma(double* sV, double* sC, const double (&a)[R][16],
         d[1] = sC[(m0 + g) * MS + 8 * j + 2 * t + 1];
         d[2] = sC[(m0 + g + 8) * MS + 8 * j + 2 * t];
         d[3] = sC[(m0 + g + 8) * MS + 8 * j + 2 * t + 1];
+        constexpr int SV = Pass<R>::SV;
 #pragma unroll
         for (int k8 = 0; k8 < 16; k8 += 8)
-          dmma_16x8x8(d, sV[(m0 + g) * MS + k8 + t], sV[(m0 + g + 8) * MS + k8 + t],
-                      sV[(m0 + g) * MS + k8 + t + 4], sV[(m0 + g + 8) * MS + k8 + t + 4],
+          dmma_16x8x8(d, sV[(k8 + t) * SV + m0 + g], sV[(k8 + t) * SV + m0 + g + 8],
+                      sV[(k8 + t + 4) * SV + m0 + g], sV[(k8 + t + 4) * SV + m0 + g + 8],
                       sm.redW[0][k8 + t][8 * j + g], sm.redW[0][k8 + t + 4][8 * j + g]);
         const int c0 = 8 * j + 2 * t;
 #pragma unroll
@@ -698,7 +714,7 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
             if (r < Pass<R>::ROWS) {
 #pragma unroll
               for (int c = 0; c < 16; c++)
-                sC[r * MS + c] = (r >= mrows || c >= f.w) ? 0.0
+                sC[c * Pass<R>::SV + r] = (r >= mrows || c >= f.w) ? 0.0
                                  : (r == c ? 1.0 : (r > c ? a[i][c] : 0.0));
             }
           }
