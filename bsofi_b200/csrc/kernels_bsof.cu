@@ -217,6 +217,8 @@ BSOFI_DEVINL bool block_wait_geq(const BsofState& st, const int* p, int target, 
 
 // Barrier among the first `count` threads of the CTA (id 1; id 0 is __syncthreads).
 BSOFI_DEVINL void named_bar(int count) { asm volatile("bar.sync 1, %0;" ::"r"(count) : "memory"); }
+// Barrier id 2: the panel CTA's prefetch warps (concurrent with barrier 1).
+BSOFI_DEVINL void named_bar2(int count) { asm volatile("bar.sync 2, %0;" ::"r"(count) : "memory"); }
 
 // Sum NB values per lane over a warp (transpose reduction): lane l ends with
 // the warp sum of value (l >> (5 - log2 NB)) & (NB - 1).
@@ -251,6 +253,7 @@ struct Smem {
   double W[NB][NB + 1];
   int flag;
   int task;
+  int pflag;  // next-tile prefetch of the panel CTA succeeded
 };
 
 // Load rows [row0 + r] (thread-owned rows r = tid + BT*i) of NB columns.
@@ -535,24 +538,30 @@ BSOFI_DEVINL void stage_v(double* sV, const double (&a)[R][16], const double* P,
 // Staged C of pass p: row-major with stride MS.  Each warp instruction copies
 // an 8-row x 4-column block (lane = 4 * row + column), which reads four 64-byte
 // column segments from global memory and writes shared memory without bank
-// conflicts.  Staged row lr is row p * ROWS + lr of the tile.
-template <int R>
-BSOFI_DEVINL void stage_c(double* sC, const double* C, long long ld, int m, int w, int p) {
-  constexpr int PR = Pass<R>::ROWS, NB8 = PR / 8 * 4 / BW;  // blocks per warp
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+// conflicts.  Staged row lr is row p * ROWS + lr of the tile.  NW warps take
+// part; wid is this warp's index among them.
+template <int R, int NW = BW>
+BSOFI_DEVINL void stage_c(double* sC, const double* C, long long ld, int m, int w, int p,
+                          int wid = threadIdx.x >> 5) {
+  constexpr int PR = Pass<R>::ROWS, NBK = PR / 8 * 4 / NW;  // blocks per warp
+  constexpr int CH = NBK > 32 ? 32 : NBK;                   // loads in flight per chunk
+  const int lane = threadIdx.x & 31;
   const int rg = lane >> 2, cg = lane & 3;
-  double v[NB8];
 #pragma unroll
-  for (int q = 0; q < NB8; q++) {
-    const int b = warp + BW * q;
-    const int lr = (b >> 2) * 8 + rg, cc = (b & 3) * 4 + cg;
-    const int r = p * PR + lr;
-    v[q] = (r < m && cc < w) ? __ldcg(C + cm(r, cc, ld)) : 0.0;
-  }
+  for (int q0 = 0; q0 < NBK; q0 += CH) {
+    double v[CH];
 #pragma unroll
-  for (int q = 0; q < NB8; q++) {
-    const int b = warp + BW * q;
-    sC[((b >> 2) * 8 + rg) * MS + (b & 3) * 4 + cg] = v[q];
+    for (int q = 0; q < CH; q++) {
+      const int b = wid + NW * (q0 + q);
+      const int lr = (b >> 2) * 8 + rg, cc = (b & 3) * 4 + cg;
+      const int r = p * PR + lr;
+      v[q] = (r < m && cc < w) ? __ldcg(C + cm(r, cc, ld)) : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < CH; q++) {
+      const int b = wid + NW * (q0 + q);
+      sC[((b >> 2) * 8 + rg) * MS + (b & 3) * 4 + cg] = v[q];
+    }
   }
 }
 
@@ -562,12 +571,13 @@ BSOFI_DEVINL void stage_c(double* sC, const double* C, long long ld, int m, int 
 //   W <- -T^T W,  C <- C + V W  (second sweep over the passes).
 // A stride of MS = 20 doubles makes the fragment loads bank-conflict free.
 // wv: width of the leaf (reflector columns), w: width of the target tile.
-// VPRE: the caller already staged V (single pass only).
-template <int R, bool VREG, bool VPRE = false>
+// VPRE / CPRE: the caller already staged V / C (single pass only).
+template <int R, bool VREG, bool VPRE = false, bool CPRE = false>
 BSOFI_DEVINL void apply_qt_mma(double* sV, double* sC, const double (&a)[R][16],
                                const double* P, long long ldp, int wv, double* C, long long ld,
                                int m, int w, Smem<16>& sm) {
   static_assert(!VPRE || Pass<R>::NP == 1, "pre-staged V needs a single pass");
+  static_assert(!CPRE || Pass<R>::NP == 1, "pre-staged C needs a single pass");
   constexpr int PR = Pass<R>::ROWS, NP = Pass<R>::NP;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
@@ -575,7 +585,7 @@ BSOFI_DEVINL void apply_qt_mma(double* sV, double* sC, const double (&a)[R][16],
 #pragma unroll 1
   for (int p = 0; p < NP; p++) {
     if (!VPRE) stage_v<R, VREG>(sV, a, P, ldp, m, wv, p);
-    stage_c<R>(sC, C, ld, m, w, p);
+    if (!CPRE) stage_c<R>(sC, C, ld, m, w, p);
     __syncthreads();
     constexpr int KW = PR / BW;
     const int r0 = warp * KW;
@@ -675,23 +685,42 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
 
   if (blockIdx.x == 0) {
     // ---------------------------------------------------------- panel chain
+    // 16-wide leaves of at most 2*BT rows are factored by 4 warps with 2R rows
+    // per thread (the per-column shuffle reduction costs per warp); the other
+    // 4 warps meanwhile wait for the next leaf's tile to be ready and stage it
+    // in shared memory for the update that follows (PREFETCH).  Taller leaves
+    // use all warps for the factorization.
+    constexpr int FW = (NB == 16 && R <= 2) ? 4 : BW;
+    constexpr int FR = R * BW / FW;
+    constexpr bool PREFETCH = NB == 16 && FW < BW && Pass<R>::NP == 1;
+    const int warp = tid >> 5;
+    // own: this CTA applied the last update to the current leaf's tile, so it
+    // needs no wait (shared barriers order its own global writes).
+    bool own = false;
     for (int s = 0; s < g.S; s++) {
       const Leaf f = leaf_of(g, s);
       int lo, hi;
       tile_range(g, f.m, f.t, lo, hi);
       if (tid == 0) st.timeline[4 * s + 0] = gtimer();
-      if (!block_wait_geq(st, st.cnt + tile_id(g, f.m, f.t), hi - lo, &sm.flag)) return;
+      if (!own && !block_wait_geq(st, st.cnt + tile_id(g, f.m, f.t), hi - lo, &sm.flag)) return;
       if (tid == 0) st.timeline[4 * s + 1] = gtimer();
       const int mrows = 2 * g.n - f.j0;
       double* P = st.A + cm((long long)f.k * g.n + f.j0, (long long)f.m * g.n + f.t * g.NB, st.ld);
+      // Target 0 of leaf s: the tile of leaf s+1.
+      const bool next = ntargets(g, f) > 0;
+      int m2 = 0, t2 = 0, lo2 = 0, hi2 = 0;
+      if (next) {
+        target_of(g, f, 0, m2, t2);
+        tile_range(g, m2, t2, lo2, hi2);
+      }
+      const int x2 = tile_id(g, m2, t2);
+      long long ldc = st.ld;
+      double* C = next ? tile_ptr(g, st.A, st.ld, st.G, f.k, f.j0, m2, t2, ldc) : nullptr;
+      const int w2 = min(g.NB, g.n - t2 * g.NB);
       for (int e = tid; e < NB * (NB + 1); e += BT) (&sm.T[0][0])[e] = 0.0;
       if (tid < 2 * NB) (&sm.gsh[0][0])[tid] = 0.0;
+      if (tid == 0) sm.pflag = 1;
       __syncthreads();
-      // 16-wide leaves of at most 2*BT rows are factored by 4 warps with 2R
-      // rows per thread (the per-column shuffle reduction costs per warp);
-      // taller leaves use all warps.  The other warps wait.
-      constexpr int FW = (NB == 16 && R <= 2) ? 4 : BW;
-      constexpr int FR = R * BW / FW;
       double a[FR][NB];
       if (tid < FW * 32) {
 #pragma unroll
@@ -719,47 +748,65 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
             }
           }
         }
+      } else {
+        if constexpr (PREFETCH) {
+          if (next) {
+            // Wait (bounded) until every update of the next tile before leaf
+            // s is done, then stage it.
+            constexpr int PT = BT - FW * 32;
+            if (tid == FW * 32) {
+              const int* flag = st.cnt + x2;
+              int ok = 1;
+              long long it = 0;
+              while (ld_acquire(flag) < s - lo2) {
+                if (ld_acquire(st.err) != 0 || ++it > st.spin_limit) {
+                  atomicExch(st.err, 1);
+                  ok = 0;
+                  break;
+                }
+                __nanosleep(64);
+              }
+              sm.pflag = ok;
+            }
+            named_bar2(PT);
+            if (sm.pflag)
+              stage_c<R, BW - FW>(sC + Pass<R>::ROWS * MS, C, ldc, mrows, w2, 0, warp - FW);
+          }
+        }
       }
       __syncthreads();
+      if (!sm.pflag) return;
       double* Tout = st.T + ((long long)f.k * st.maxleaves + f.l) * 256;
       for (int e = tid; e < 256; e += BT) {
         const int rr = e % 16, cc = e / 16;
         Tout[e] = (rr < NB && cc < NB && rr < f.w && cc < f.w) ? sm.T[rr][cc] : 0.0;
       }
       __syncthreads();
-      if (tid == 0) {
-        __threadfence();
-        red_release_add(st.factored + s, 1);
-        st.timeline[4 * s + 2] = gtimer();
-      }
-      // Apply leaf s to the tile of leaf s+1 (target 0).
-      if (ntargets(g, f) > 0) {
-        int m2, t2;
-        target_of(g, f, 0, m2, t2);
-        int lo2, hi2;
-        tile_range(g, m2, t2, lo2, hi2);
-        const int x2 = tile_id(g, m2, t2);
-        if (!block_wait_geq(st, st.cnt + x2, s - lo2, &sm.flag)) return;
-        long long ldc;
-        double* C = tile_ptr(g, st.A, st.ld, st.G, f.k, f.j0, m2, t2, ldc);
-        const int w2 = min(g.NB, g.n - t2 * g.NB);
+      // Apply leaf s to the tile of leaf s+1.  That is the tile's last update
+      // and only this CTA reads the tile next, so it is not published; the
+      // leaf itself (reflectors and T) is published after the update, with one
+      // fence for both.
+      if (next) {
+        if (!PREFETCH && !block_wait_geq(st, st.cnt + x2, s - lo2, &sm.flag)) return;
         if (tid == 0) st.timeline[4 * s + 3] = gtimer();
         if constexpr (NB == 16) {
-          // The factored leaf is re-read from L2 (just written by this CTA)
-          // rather than from the factor's register layout.
+          // V is staged from the factor's registers when one pass covers the
+          // leaf, else re-read from L2 (just written by this CTA).
           double none[R][16];
-          apply_qt_mma<R, false, Pass<R>::NP == 1>(sC, sC + Pass<R>::ROWS * MS, none, P, st.ld,
-                                                   f.w, C, ldc, mrows, w2, sm);
+          apply_qt_mma<R, false, Pass<R>::NP == 1, PREFETCH>(
+              sC, sC + Pass<R>::ROWS * MS, none, P, st.ld, f.w, C, ldc, mrows, w2, sm);
         } else {
           double v[R][NB];
           leaf_to_v<R, NB>(a, v, mrows, f.w);
           apply_qt<R, NB>(v, C, ldc, mrows, w2, sm, sC);
         }
-        if (tid == 0) {
-          __threadfence();
-          red_release_add(st.cnt + x2, 1);
-        }
       }
+      if (tid == 0) {
+        __threadfence();
+        red_release_add(st.factored + s, 1);
+        st.timeline[4 * s + 2] = gtimer();
+      }
+      own = next;
     }
     return;
   }
