@@ -14,8 +14,9 @@ data path); value = inversions by all ranks / max-over-ranks device time.
 Printed JSON line (rank 0): value (device-resident inversions/s), tflops
 (flop model of include/bsofi_flops.h), roofline of the dominant kernel (the
 persistent BSOI kernel, FP64 DMMA, against cuBLAS DGEMM measured in the same run),
-e2e (the reference handle API hybridxbsoftrih_ + hybridxbsoih_ on host
-buffers, copies included), cpu_baseline (the reference's CPU path,
+e2e (the reference handle API hybridxbsoftrih_ + hybridxbsoih_ on pinned host
+buffers, copies included; e2e_pageable the same on pageable numpy arrays),
+cpu_baseline (the reference's CPU path,
 oracle/_ref, on the host cores), clocks sampled during the timed region.
 
 --impl reference times the reference's own CPU implementation (the compiled
@@ -382,9 +383,11 @@ def main():
     if args.serve > 0:
         served = run_serving(api, torch, dev, args.serve, args.serve_rate, 31 + rank)
 
-    e2e = None
+    e2e = e2e_pageable = None
     if not args.no_e2e and args.e2e_steps > 0:
         e2e = run_e2e(api, torch, dist, world, side, L, U, rank, args.e2e_steps)
+        e2e_pageable = run_e2e(api, torch, dist, world, side, L, U, rank, args.e2e_steps,
+                               pinned=False)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu and args.cpu_sample > 0:
@@ -406,7 +409,7 @@ def main():
                 "tflops": bsofi_flops(n, L) * value / world / 1e12,
                 "residual": resid,
                 "roofline": roofline, "roofline_bsof": roofline_bsof,
-                "cpu_baseline": cpu, "e2e": e2e,
+                "cpu_baseline": cpu, "e2e": e2e, "e2e_pageable": e2e_pageable,
                 "batched": batched, "batched_mixed_sizes": batched_mixed, "served": served,
                 "gpu_launches": launches_per_step * args.steps,
                 "clocks": clk}
@@ -527,15 +530,22 @@ def run_serving(api, torch, dev, nreq, rate, seed):
                         % nreq}
 
 
-def run_e2e(api, torch, dist, world, side, L, U, rank, steps):
+def run_e2e(api, torch, dist, world, side, L, U, rank, steps, pinned=True):
     """The reference-facing handle API on host buffers: hybridxbsoftrih_ +
-    hybridxbsoih_ per step, every copy between host and device included."""
+    hybridxbsoih_ per step, every copy between host and device included.
+    pinned: the caller's A and tau are page-locked (torch pinned memory);
+    otherwise ordinary pageable numpy arrays."""
     from bsofi_b200.hubbard import hubbard_matrix
     n = side * side
     N = n * L
     M = hubbard_matrix(side, L, U, seed=777 + rank)
-    A = np.empty_like(M, order="F")
-    tau = np.zeros(N)
+    if pinned:
+        # Column-major N x N view of a pinned row-major buffer.
+        A = torch.empty((N, N), dtype=torch.float64, pin_memory=True).numpy().T
+        tau = torch.zeros(N, dtype=torch.float64, pin_memory=True).numpy()
+    else:
+        A = np.empty_like(M, order="F")
+        tau = np.zeros(N)
     h = api.Handle(n, L)
     times = []
     for i in range(steps + 1):
@@ -569,7 +579,8 @@ def run_e2e(api, torch, dist, world, side, L, U, rank, steps):
     d2h = state_bytes + N * 8 + N * N * 8
     return {"value": world * len(times) / tot, "unit": "inversions/s",
             "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-            "api": "hybridxbsoftrih_ + hybridxbsoih_ (host pageable buffers)",
+            "api": "hybridxbsoftrih_ + hybridxbsoih_ (host %s buffers)"
+                   % ("pinned" if pinned else "pageable"),
             "steps": len(times), "residual": resid}
 
 

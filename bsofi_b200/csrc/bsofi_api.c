@@ -27,10 +27,11 @@
 #define CTX_MAGIC 0x58544342u
 
 /* ------------------------------------------------------------------------
- * Host staging.  The caller's arrays are pageable; copies go through two
- * pinned buffers (double buffering against the DMA engine), packed and
- * unpacked column by column by a small pool of host threads so that host
- * memory bandwidth, not one core, bounds the transfer.
+ * Host staging.  Pageable caller arrays are copied through two pinned
+ * buffers (double buffering against the DMA engine), packed and unpacked
+ * column by column by a small pool of host threads so that host memory
+ * bandwidth, not one core, bounds the transfer.  Page-locked caller arrays
+ * (cudaMallocHost, cudaHostRegister) are copied by the DMA engine directly.
  * ---------------------------------------------------------------------- */
 #define STAGE_BYTES ((size_t)64 << 20)
 #define MAX_COPY_THREADS 16
@@ -161,6 +162,12 @@ typedef struct bsofi_ctx {
   cudaEvent_t stage_ev[2];
   int stage_next;
   copy_pool *pool;
+  /* Pipelined BSOI on page-locked caller arrays: copy-in and copy-out
+   * streams and per-column-block events (created on first use). */
+  cudaStream_t s_in, s_out;
+  cudaEvent_t *ev;      /* 2 * nev: [0, nev) uploaded, [nev, 2 nev) finished */
+  cudaEvent_t ev_refl, ev_start;
+  int nev;
 } bsofi_ctx;
 
 /* Layout of the caller's integer handler(10) (40 bytes). */
@@ -258,6 +265,18 @@ static void ctx_destroy(bsofi_ctx *c) {
   }
   copy_pool_destroy(c->pool);
   ctx_free_buffers(c);
+  if (c->s_in) {
+    cudaStreamSynchronize(c->s_in);
+    cudaStreamDestroy(c->s_in);
+  }
+  if (c->s_out) {
+    cudaStreamSynchronize(c->s_out);
+    cudaStreamDestroy(c->s_out);
+  }
+  for (b = 0; b < 2 * c->nev; b++) cudaEventDestroy(c->ev[b]);
+  free(c->ev);
+  if (c->ev_refl) cudaEventDestroy(c->ev_refl);
+  if (c->ev_start) cudaEventDestroy(c->ev_start);
   if (c->stream) cudaStreamDestroy(c->stream);
   c->magic = 0;
   free(c);
@@ -277,12 +296,35 @@ static bsofi_ctx *handle_ctx(const int *h) {
 /* ---------------------------------------------------------------- copies */
 /* Host (pitch lda) -> device (pitch ldd): `rows` doubles of `cols` columns,
  * through the pinned staging buffers. */
+/* True when the host range [p, p + bytes) is page-locked (cudaMallocHost or
+ * cudaHostRegister): the DMA engine then reads or writes it directly. */
+static int host_pinned(const void *p, size_t bytes) {
+  struct cudaPointerAttributes a;
+  const char *q = (const char *)p;
+  if (bytes == 0) return 0;
+  if (cudaPointerGetAttributes(&a, q) != cudaSuccess || a.type != cudaMemoryTypeHost) {
+    cudaGetLastError();
+    return 0;
+  }
+  if (cudaPointerGetAttributes(&a, q + bytes - 1) != cudaSuccess || a.type != cudaMemoryTypeHost) {
+    cudaGetLastError();
+    return 0;
+  }
+  return 1;
+}
+
+/* Span of a column-major host block (rows x cols, pitch lda doubles). */
+static size_t host_span(int lda, int rows, int cols) {
+  return cols > 0 ? ((size_t)(cols - 1) * lda + rows) * sizeof(double) : 0;
+}
+
 static cudaError_t h2d_cols(bsofi_ctx *c, double *dst, int ldd, const double *src, int lda,
                             int rows, int cols) {
   const size_t es = sizeof(double), w = (size_t)rows * es;
   int c0, cpc;
   cudaError_t e;
-  if (!c->stage[1])
+  if (cols <= 0 || rows <= 0) return cudaSuccess;
+  if (!c->stage[1] || host_pinned(src, host_span(lda, rows, cols)))
     return cudaMemcpy2DAsync(dst, es * ldd, src, es * lda, w, cols, cudaMemcpyHostToDevice,
                              c->stream);
   cpc = (int)(STAGE_BYTES / w);
@@ -308,8 +350,8 @@ static cudaError_t d2h_cols(bsofi_ctx *c, double *dst, int lda, const double *sr
   const size_t es = sizeof(double), w = (size_t)rows * es;
   int i, nchunks, cpc, prev_c0 = 0, prev_nc = 0, prev_b = 0;
   cudaError_t e;
-  if (cols <= 0) return cudaSuccess;
-  if (!c->stage[1]) {
+  if (cols <= 0 || rows <= 0) return cudaSuccess;
+  if (!c->stage[1] || host_pinned(dst, host_span(lda, rows, cols))) {
     e = cudaMemcpy2DAsync(dst, es * lda, src, es * ldd, w, cols, cudaMemcpyDeviceToHost,
                           c->stream);
     return e == cudaSuccess ? cudaStreamSynchronize(c->stream) : e;
@@ -372,7 +414,22 @@ static cudaError_t copy_state(bsofi_ctx *c, double *A, int lda, int to_host) {
   int n = c->n, L = c->L, N = n * L, k;
   size_t es = sizeof(double);
   cudaError_t e = cudaSuccess;
-  (void)es;
+  if (host_pinned(A, host_span(lda, N, N))) {
+    /* Page-locked caller array: direct DMA of every block column, one wait. */
+    for (k = 0; k < L && e == cudaSuccess; k++) {
+      int rows = (k + 2) * n < N ? (k + 2) * n : N;
+      double *h = A + (size_t)k * n * lda;
+      double *d = c->dA + (size_t)k * n * c->ldd;
+      if (to_host)
+        e = cudaMemcpy2DAsync(h, es * lda, d, es * c->ldd, es * rows, n, cudaMemcpyDeviceToHost,
+                              c->stream);
+      else
+        e = cudaMemcpy2DAsync(d, es * c->ldd, h, es * lda, es * rows, n, cudaMemcpyHostToDevice,
+                              c->stream);
+    }
+    if (e == cudaSuccess && to_host) e = cudaStreamSynchronize(c->stream);
+    return e;
+  }
   for (k = 0; k < L; k++) {
     int rows = (k + 2) * n < N ? (k + 2) * n : N;
     double *h = A + (size_t)k * n * lda;
@@ -454,10 +511,120 @@ static int drive_bsoftri(bsofi_ctx *c, int n, int L, double *A, int lda, double 
   return e == cudaSuccess ? 0 : cuda_info(e);
 }
 
+/* Streams and L events of each kind for the pipelined BSOI. */
+static cudaError_t pipe_fit(bsofi_ctx *c, int L) {
+  cudaError_t e = cudaSuccess;
+  int i;
+  if (!c->s_in && (e = cudaStreamCreateWithFlags(&c->s_in, cudaStreamNonBlocking)) != cudaSuccess)
+    return e;
+  if (!c->s_out && (e = cudaStreamCreateWithFlags(&c->s_out, cudaStreamNonBlocking)) != cudaSuccess)
+    return e;
+  if (!c->ev_refl && (e = cudaEventCreateWithFlags(&c->ev_refl, cudaEventDisableTiming)) != cudaSuccess)
+    return e;
+  if (!c->ev_start && (e = cudaEventCreateWithFlags(&c->ev_start, cudaEventDisableTiming)) != cudaSuccess)
+    return e;
+  if (c->nev >= L) return cudaSuccess;
+  for (i = 0; i < 2 * c->nev; i++) cudaEventDestroy(c->ev[i]);
+  free(c->ev);
+  c->nev = 0;
+  c->ev = (cudaEvent_t *)calloc(2 * (size_t)L, sizeof(cudaEvent_t));
+  if (!c->ev) return cudaErrorMemoryAllocation;
+  for (i = 0; i < 2 * L; i++) {
+    if ((e = cudaEventCreateWithFlags(&c->ev[i], cudaEventDisableTiming)) != cudaSuccess) {
+      while (--i >= 0) cudaEventDestroy(c->ev[i]);
+      free(c->ev);
+      c->ev = NULL;
+      return e;
+    }
+  }
+  c->nev = L;
+  return cudaSuccess;
+}
+
+/* BSOI on a page-locked caller array, as a three-stream pipeline:
+ *   copy-in:  tau and the reflector rows of every block column (what Q
+ *             formation reads), then the rest of block columns L-1, ..., 0;
+ *   compute:  Q formation, then step k as soon as block column k is on the
+ *             device (one GEMM launch per step);
+ *   copy-out: block column k+1 as soon as step k has finished it.
+ * The upload of later block columns and the download of finished ones run
+ * under the GEMM steps. */
+static cudaError_t bsoi_pipelined(bsofi_ctx *c, int n, int L, double *A, int lda,
+                                  const double *tau) {
+  const size_t es = sizeof(double), sh = es * (size_t)lda, sd = es * (size_t)c->ldd;
+  const int N = n * L;
+  cudaError_t e;
+  int k, r;
+  if ((e = pipe_fit(c, L)) != cudaSuccess) return e;
+  cudaEvent_t *up = c->ev, *done = c->ev + c->nev;
+  /* Copies start after whatever the context's stream still has queued. */
+  if ((e = cudaEventRecord(c->ev_start, c->stream)) != cudaSuccess) return e;
+  if ((e = cudaStreamWaitEvent(c->s_in, c->ev_start, 0)) != cudaSuccess) goto drain;
+  if ((e = cudaStreamWaitEvent(c->s_out, c->ev_start, 0)) != cudaSuccess) goto drain;
+  e = cudaMemcpyAsync(c->dtau, tau, es * N, cudaMemcpyHostToDevice, c->s_in);
+  for (k = 0; k < L && e == cudaSuccess; k++) {
+    const int r0 = k * n, r1 = (k + 2) * n < N ? (k + 2) * n : N;
+    e = cudaMemcpy2DAsync(c->dA + (size_t)k * n * c->ldd + r0, sd, A + (size_t)k * n * lda + r0,
+                          sh, es * (r1 - r0), n, cudaMemcpyHostToDevice, c->s_in);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(c->ev_refl, c->s_in);
+  for (k = L - 1; k >= 0 && e == cudaSuccess; k--) {
+    if (k > 0)
+      e = cudaMemcpy2DAsync(c->dA + (size_t)k * n * c->ldd, sd, A + (size_t)k * n * lda, sh,
+                            es * (size_t)k * n, n, cudaMemcpyHostToDevice, c->s_in);
+    if (e == cudaSuccess) e = cudaEventRecord(up[k], c->s_in);
+  }
+  if (e != cudaSuccess) goto drain;
+  /* compute */
+  if ((e = cudaStreamWaitEvent(c->stream, c->ev_refl, 0)) != cudaSuccess) goto drain;
+  if ((r = bsofi_dev_bsoi_form_q(n, L, c->dA, c->ldd, c->dtau, c->dws, c->stream)) != 0) {
+    e = (cudaError_t)r;
+    goto drain;
+  }
+  if ((e = cudaStreamWaitEvent(c->stream, up[L - 1], 0)) != cudaSuccess) goto drain;
+  if ((r = bsofi_dev_bsoi_carry(n, L, c->dA, c->ldd, c->dws, c->stream)) != 0) {
+    e = (cudaError_t)r;
+    goto drain;
+  }
+  for (k = L - 2; k >= 0; k--) {
+    if ((e = cudaStreamWaitEvent(c->stream, up[k], 0)) != cudaSuccess) goto drain;
+    if ((r = bsofi_dev_bsoi_step(n, L, k, c->dA, c->ldd, c->dws, c->stream)) != 0) {
+      e = (cudaError_t)r;
+      goto drain;
+    }
+    if ((e = cudaEventRecord(done[k + 1], c->stream)) != cudaSuccess) goto drain;
+  }
+  if ((r = bsofi_dev_bsoi_finish(n, L, c->dA, c->ldd, c->dws, c->stream)) != 0) {
+    e = (cudaError_t)r;
+    goto drain;
+  }
+  if ((e = cudaEventRecord(done[0], c->stream)) != cudaSuccess) goto drain;
+  /* copy-out, right to left as the block columns finish */
+  for (k = L - 1; k >= 0 && e == cudaSuccess; k--) {
+    e = cudaStreamWaitEvent(c->s_out, done[k], 0);
+    if (e == cudaSuccess)
+      e = cudaMemcpy2DAsync(A + (size_t)k * n * lda, sh, c->dA + (size_t)k * n * c->ldd, sd,
+                            es * N, n, cudaMemcpyDeviceToHost, c->s_out);
+  }
+drain: {
+  /* Nothing may still touch the caller's arrays when this returns. */
+  cudaError_t e1 = cudaStreamSynchronize(c->s_in);
+  cudaError_t e2 = cudaStreamSynchronize(c->s_out);
+  cudaError_t e3 = cudaStreamSynchronize(c->stream);
+  if (e == cudaSuccess) e = e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3);
+}
+  return e;
+}
+
 static int drive_bsoi(bsofi_ctx *c, int n, int L, double *A, int lda, const double *tau) {
   cudaError_t e;
   int N = n * L;
   if ((e = ctx_fit(c, n, L)) != cudaSuccess) return cuda_info(e);
+  if (L >= 2 && host_pinned(A, host_span(lda, N, N))) {
+    int info = 0;
+    if ((e = bsoi_pipelined(c, n, L, A, lda, tau)) != cudaSuccess) return cuda_info(e);
+    return read_info(c, &info) < 0 ? info : 0;
+  }
   if ((e = copy_state(c, A, lda, 0)) != cudaSuccess) return cuda_info(e);
   e = cudaMemcpyAsync(c->dtau, tau, sizeof(double) * N, cudaMemcpyHostToDevice, c->stream);
   if (e != cudaSuccess) return cuda_info(e);

@@ -44,6 +44,17 @@ int bsofi_dev_invert_ex(int n, int L, double *dA, int ldd, double *dtau, void *d
 int bsofi_dev_bsoi(int n, int L, double *dA, int ldd, const double *dtau, void *dws,
                    void *stream);
 
+/* BSOI in pieces, for callers that overlap it with host copies:
+ * form_q builds every G_k = Q_k^T (needs the reflectors and tau);
+ * carry seeds the first step (needs column block L-1);
+ * step k needs column block k and leaves column block k+1 final;
+ * finish writes column block 0 and folds the wait errors into the info word. */
+int bsofi_dev_bsoi_form_q(int n, int L, double *dA, int ldd, const double *dtau, void *dws,
+                          void *stream);
+int bsofi_dev_bsoi_carry(int n, int L, double *dA, int ldd, void *dws, void *stream);
+int bsofi_dev_bsoi_step(int n, int L, int k, double *dA, int ldd, void *dws, void *stream);
+int bsofi_dev_bsoi_finish(int n, int L, double *dA, int ldd, void *dws, void *stream);
+
 /* Device address of the int info words inside the workspace: [0] BSTRI info
  * (values >= 0x7f7f7f7f mean 0; i > 0: R(i,i) exactly zero, 1-based global
  * index), [1] BSOF wait timeout, [2] BSOI wait timeout (nonzero = error). */

@@ -277,18 +277,14 @@ int run_bstri(int n, int L, double* dA, int ldd, void* ws, cudaStream_t st) {
   return 0;
 }
 
-int run_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* ws, cudaStream_t st,
-             bool q_ready) {
+// G_k = Q_k^T of every panel from the stored reflectors and tau: compact-WY
+// factors first, then the block reflectors applied to identity matrices.
+int bsoi_form_q(int n, int L, double* dA, int ldd, const double* dtau, void* ws, cudaStream_t st) {
   Layout ly = layout(n, L, ldd);
   double* Tb = at<double>(ws, ly.T);
   double* G = at<double>(ws, ly.G);
-  double* C[2] = {at<double>(ws, ly.C0), at<double>(ws, ly.C1)};
-  const int N = n * L, n2 = 2 * n;
+  const int n2 = 2 * n;
   const long long g2 = (long long)n2 * n2;
-
-  // Compact-WY factors from the stored reflectors, then G_k = Q_k^T (unless
-  // the factorization already formed G_k).
-  if (!q_ready) {
   build_leaf_t_kernel<<<dim3(ly.maxleaves, L - 1), 256, 0, st>>>(dA, ldd, n, L, dtau, Tb,
                                                                   ly.maxleaves, ly.nbw);
   CK(cudaGetLastError());
@@ -313,53 +309,90 @@ int run_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* ws, cu
       CK(launch_wy_apply(a, batch, st));
     }
   }
-  }
+  return 0;
+}
 
-  // Carry for the first step: X(:, L-1) with the triangular diagonal block.
-  CK(launch_copy_masked(C[0], ldd, dA + cm(0, (long long)(L - 1) * n, ldd), ldd, N, n,
-                        (L - 1) * n, st));
-  int* err = at<int>(ws, ly.info) + 2;
-  CKM(cudaMemsetAsync(err, 0, sizeof(int), st));
+// Carry for the first BSOI step: X(:, L-1) with the triangular diagonal
+// block; also clears the BSOI error word.
+int bsoi_carry(int n, int L, double* dA, int ldd, void* ws, cudaStream_t st) {
+  Layout ly = layout(n, L, ldd);
+  const int N = n * L;
+  CK(launch_copy_masked(at<double>(ws, ly.C0), ldd, dA + cm(0, (long long)(L - 1) * n, ldd), ldd,
+                        N, n, (L - 1) * n, st));
+  CKM(cudaMemsetAsync(at<int>(ws, ly.info) + 2, 0, sizeof(int), st));
+  return 0;
+}
+
+// BSOI step k as one GEMM launch: [X(:,k) | carry] Q_k^T -> [carry' | X(:,k+1)].
+int bsoi_step(int n, int L, int k, double* dA, int ldd, void* ws, cudaStream_t st) {
+  Layout ly = layout(n, L, ldd);
+  double* G = at<double>(ws, ly.G);
+  double* C[2] = {at<double>(ws, ly.C0), at<double>(ws, ly.C1)};
+  const int N = n * L, n2 = 2 * n;
+  const long long g2 = (long long)n2 * n2;
+  const int rd = (L - 2 - k) & 1;
+  GemmDims d = {N, n2, n2};
+  GemmA a = {};
+  a.p0 = dA + cm(0, (long long)k * n, ldd);
+  a.ld0 = ldd;
+  a.p1 = C[rd];
+  a.ld1 = ldd;
+  a.ksplit = n;
+  a.rlim0 = (k + 1) * n;
+  a.roff0 = k * n;
+  a.rlim1 = INT_MAX;
+  a.roff1 = kNoMask;
+  GemmB b = {G + (size_t)k * g2, n2, 0, kNoMask};
+  GemmC c = {};
+  c.p0 = C[rd ^ 1];
+  c.ld0 = ldd;
+  c.p1 = dA + cm(0, (long long)(k + 1) * n, ldd);
+  c.ld1 = ldd;
+  c.nsplit = n;
+  c.alpha = 1.0;
+  if (g_timer.on) CKM(g_timer.mark(st));
+  CK(launch_gemm(d, a, b, c, 1, 0, st));
+  if (g_timer.on) CKM(g_timer.mark(st));
+  return 0;
+}
+
+// X(:, 0) from the last carry; the info word absorbs the wait error words.
+int bsoi_finish(int n, int L, double* dA, int ldd, void* ws, cudaStream_t st) {
+  Layout ly = layout(n, L, ldd);
+  double* C[2] = {at<double>(ws, ly.C0), at<double>(ws, ly.C1)};
+  const int cur = (L - 1) & 1;  // carry buffer written by step 0
+  CK(launch_copy_masked(dA, ldd, C[cur], ldd, n * L, n, kNoMask, st, at<int>(ws, ly.info)));
+  return 0;
+}
+
+int run_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* ws, cudaStream_t st,
+             bool q_ready) {
+  Layout ly = layout(n, L, ldd);
+  double* G = at<double>(ws, ly.G);
+  double* C[2] = {at<double>(ws, ly.C0), at<double>(ws, ly.C1)};
+  const int N = n * L, n2 = 2 * n;
+  // G_k = Q_k^T unless the factorization already formed it.
+  if (!q_ready) {
+    int e = bsoi_form_q(n, L, dA, ldd, dtau, ws, st);
+    if (e) return e;
+  }
+  int e = bsoi_carry(n, L, dA, ldd, ws, st);
+  if (e) return e;
   const int row_bands = bsoi_row_bands(N), col_tiles = (n2 + 127) / 128;
   if (row_bands * col_tiles >= 64) {
     // One persistent launch over all steps (rows flow from step to step).
     int* bs = at<int>(ws, ly.bsync);
     CKM(cudaMemsetAsync(bs, 0, sizeof(int) * ly.bsync_ints, st));
     if (g_timer.on) CKM(g_timer.mark(st));
-    CK(launch_bsoi_persistent(dA, ldd, C[0], C[1], ldd, G, n, L, bs, bs + ly.bsync_ints - 2, err,
-                              st));
+    CK(launch_bsoi_persistent(dA, ldd, C[0], C[1], ldd, G, n, L, bs, bs + ly.bsync_ints - 2,
+                              at<int>(ws, ly.info) + 2, st));
     if (g_timer.on) CKM(g_timer.mark(st));
   } else {
     // Small problems: one launch per step with small tiles (more CTAs per step).
-    for (int k = L - 2; k >= 0; k--) {
-      const int rd = (L - 2 - k) & 1;
-      GemmDims d = {N, n2, n2};
-      GemmA a = {};
-      a.p0 = dA + cm(0, (long long)k * n, ldd);
-      a.ld0 = ldd;
-      a.p1 = C[rd];
-      a.ld1 = ldd;
-      a.ksplit = n;
-      a.rlim0 = (k + 1) * n;
-      a.roff0 = k * n;
-      a.rlim1 = INT_MAX;
-      a.roff1 = kNoMask;
-      GemmB b = {G + (size_t)k * g2, n2, 0, kNoMask};
-      GemmC c = {};
-      c.p0 = C[rd ^ 1];
-      c.ld0 = ldd;
-      c.p1 = dA + cm(0, (long long)(k + 1) * n, ldd);
-      c.ld1 = ldd;
-      c.nsplit = n;
-      c.alpha = 1.0;
-      if (g_timer.on) CKM(g_timer.mark(st));
-      CK(launch_gemm(d, a, b, c, 1, 0, st));
-      if (g_timer.on) CKM(g_timer.mark(st));
-    }
+    for (int k = L - 2; k >= 0; k--)
+      if ((e = bsoi_step(n, L, k, dA, ldd, ws, st)) != 0) return e;
   }
-  const int cur = (L - 1) & 1;  // carry buffer written by step 0
-  CK(launch_copy_masked(dA, ldd, C[cur], ldd, N, n, kNoMask, st, at<int>(ws, ly.info)));
-  return 0;
+  return bsoi_finish(n, L, dA, ldd, ws, st);
 }
 
 }  // namespace
@@ -398,6 +431,23 @@ int bsofi_dev_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* 
                    void* stream) {
   g_launches = 0;
   return run_bsoi(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, false);
+}
+
+int bsofi_dev_bsoi_form_q(int n, int L, double* dA, int ldd, const double* dtau, void* dws,
+                          void* stream) {
+  return bsoi_form_q(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream);
+}
+
+int bsofi_dev_bsoi_carry(int n, int L, double* dA, int ldd, void* dws, void* stream) {
+  return bsoi_carry(n, L, dA, ldd, dws, (cudaStream_t)stream);
+}
+
+int bsofi_dev_bsoi_step(int n, int L, int k, double* dA, int ldd, void* dws, void* stream) {
+  return bsoi_step(n, L, k, dA, ldd, dws, (cudaStream_t)stream);
+}
+
+int bsofi_dev_bsoi_finish(int n, int L, double* dA, int ldd, void* dws, void* stream) {
+  return bsoi_finish(n, L, dA, ldd, dws, (cudaStream_t)stream);
 }
 
 int bsofi_dev_invert(int n, int L, double* dA, int ldd, double* dtau, void* dws, void* stream) {

@@ -170,3 +170,30 @@ def test_gpu_names_on_device_memory(cuda_device):
                          None, None, 0, ctypes.byref(info))
     assert info.value == 0
     assert rel_fro(from_device_colmajor(dA, N), Xh) < 1e-13
+
+
+@pytest.mark.parametrize("n,L", [(37, 6), (128, 10), (256, 8)])
+def test_handle_api_pinned_host_arrays(cuda_device, n, L):
+    """Page-locked caller arrays take the direct-DMA path (BSOI pipelined
+    with the copies, one GEMM launch per step); the state is bitwise the
+    pageable path's and the inverse agrees within the parity tolerance."""
+    import torch
+    N = n * L
+    M = random_pcyclic(n, L, seed=4242 + n)
+    Xp, state_p, tau_p, info = api.invert(M, n, L)
+    assert info == 0
+    A = torch.empty((N, N), dtype=torch.float64, pin_memory=True).numpy().T
+    tau = torch.zeros(N, dtype=torch.float64, pin_memory=True).numpy()
+    A[:] = M
+    with api.Handle(n, L) as h:
+        assert h.bsoftri(A, tau) == 0
+        np.testing.assert_array_equal(tau, tau_p)
+        np.testing.assert_array_equal(A, state_p)
+        assert h.bsoi(A, tau) == 0
+        assert rel_fro(A, Xp) < inverse_tolerance(M, Xp)
+        assert residual(M, A) < 1e-13
+        # A second call on the same handle (events and streams reused).
+        A[:] = M
+        assert h.bsoftri(A, tau) == 0
+        assert h.bsoi(A, tau) == 0
+        assert residual(M, A) < 1e-13
