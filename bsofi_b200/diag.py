@@ -1,0 +1,85 @@
+"""Diagnostics of the device pipeline through the C ABI.
+
+    python -m bsofi_b200.diag bsof-timeline N_BLOCK L [REPS]
+
+inverts a seeded Hubbard matrix (a random p-cyclic one when n is not a square)
+with bsofi_device_invert and prints, for the last run, the BSOF chain length
+and the per-leaf phases recorded by the persistent BSOF kernel's critical CTA
+(bsofi_device_bsof_timeline: globaltimer stamps at loop start, tile ready,
+next-tile update start and leaf published).
+"""
+import sys
+
+import numpy as np
+
+from . import _lib, api
+from .hubbard import hubbard_matrix, random_pcyclic
+
+
+def bsof_leaves(n, L):
+    nb = 16 if n <= 256 else 8
+    nl = (n + nb - 1) // nb
+    return (L - 2) * nl + 2 * nl
+
+
+def bsof_timeline(n, L, reps=3):
+    import torch
+    side = int(round(n ** 0.5))
+    N = n * L
+    ldd = (N + 31) // 32 * 32
+    M = hubbard_matrix(side, L, 4.0, seed=1) if side * side == n else random_pcyclic(n, L, seed=1)
+    dev = torch.device("cuda:0")
+    src = torch.zeros((N, ldd), dtype=torch.float64, device=dev)
+    src[:, :N] = torch.from_numpy(np.ascontiguousarray(M.T)).to(dev)
+    dA = torch.empty_like(src)
+    dtau = torch.zeros(N, dtype=torch.float64, device=dev)
+    ws = torch.empty(api.workspace_bytes(n, L, ldd), dtype=torch.uint8, device=dev)
+    S = bsof_leaves(n, L)
+    out = {}
+    for _ in range(reps):
+        dA.copy_(src)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        stream = torch.cuda.current_stream()
+        e0.record(stream)
+        rc = api.device_invert(n, L, dA.data_ptr(), ldd, dtau.data_ptr(), ws.data_ptr(),
+                               stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if rc != 0:
+            raise RuntimeError("bsofi_device_invert failed (%d)" % rc)
+        buf = np.zeros(4 * S, dtype=np.uint64)
+        cnt = _lib.load().bsofi_device_bsof_timeline(n, L, ldd, ws.data_ptr(), buf.ctypes.data, S)
+        if cnt != S:
+            raise RuntimeError("timeline holds %d leaves, expected %d" % (cnt, S))
+        t = buf.reshape(S, 4).astype(np.int64)
+        has = t[:-1]
+        out = {
+            "invert_ms": e0.elapsed_time(e1),
+            "chain_ms": (t[-1, 2] - t[0, 0]) / 1e6,
+            "leaves": S,
+            "wait_tile_us": (t[:, 1] - t[:, 0]).mean() / 1e3,
+            "factor_us": (has[:, 3] - has[:, 1]).mean() / 1e3,
+            "update_publish_us": (has[:, 2] - has[:, 3]).mean() / 1e3,
+            "to_next_leaf_us": (t[1:, 0] - t[:-1, 2]).mean() / 1e3,
+        }
+    return out
+
+
+def main(argv):
+    if len(argv) >= 3 and argv[0] == "bsof-timeline":
+        n, L = int(argv[1]), int(argv[2])
+        reps = int(argv[3]) if len(argv) > 3 else 3
+        r = bsof_timeline(n, L, reps)
+        print("n %d L %d: invert %.3f ms, BSOF chain %.3f ms over %d leaves" %
+              (n, L, r["invert_ms"], r["chain_ms"], r["leaves"]))
+        print("per leaf: wait for tile %.2f us, factor (tile ready -> next-tile update) %.2f us, "
+              "next-tile update + publish %.2f us, publish -> next leaf %.2f us" %
+              (r["wait_tile_us"], r["factor_us"], r["update_publish_us"], r["to_next_leaf_us"]))
+        return 0
+    print(__doc__)
+    return 2
+
+
+if __name__ == "__main__":
+    sys.exit(main(sys.argv[1:]))
