@@ -466,10 +466,33 @@ def run_batched(api, torch, dev, specs, steps, stream):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     ms_max = replicas.max_over_ranks(total_ms, dev)
     rate = world * len(specs) * steps / (ms_max * 1e-3)
+    launches = api.last_launches()
+    # The same batch captured once into a CUDA graph and replayed.
+    graph_ms = 0.0
+    g = api.BatchGraph(ns, Ls, [w.data_ptr() for w in work], lds, [t.data_ptr() for t in taus],
+                       ws.data_ptr(), 8)
+    for it in range(steps + 1):
+        for w, p0 in zip(work, pristine):
+            w.copy_(p0)
+        torch.cuda.synchronize()
+        replicas.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rc = g.launch(sp)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if rc != 0:
+            raise RuntimeError("bsofi_batch_graph_launch failed: %d" % rc)
+        if it > 0:
+            graph_ms += e0.elapsed_time(e1)
+    g.close()
+    graph_ms = replicas.max_over_ranks(graph_ms, dev)
     out = {"value": rate, "unit": "inversions/s", "steps": steps,
            "ms_per_step": ms_max / steps, "tflops": flops * steps * world / (ms_max * 1e-3) / 1e12,
            "instances_per_step": len(specs), "residual_first_instance": resid,
-           "gpu_launches_per_step": api.last_launches()}
+           "gpu_launches_per_step": launches,
+           "graph_value": world * len(specs) * steps / (graph_ms * 1e-3)}
     del work, pristine, ws
     torch.cuda.empty_cache()
     return out

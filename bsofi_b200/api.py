@@ -186,6 +186,39 @@ def device_invert_batched(ns, Ls, dAs, lddas, dtaus, dwork, streams=8, stream=0)
                                               stream)
 
 
+class BatchGraph:
+    """bsofi_batch_graph_*: a batch of inversions captured once into a CUDA
+    graph; launch(stream) replays it on the same device buffers."""
+
+    def __init__(self, ns, Ls, dAs, lddas, dtaus, dwork, streams=8):
+        import numpy as _np
+        self._n = _np.ascontiguousarray(ns, dtype=_np.int32)
+        self._L = _np.ascontiguousarray(Ls, dtype=_np.int32)
+        self._ld = _np.ascontiguousarray(lddas, dtype=_np.int32)
+        self._pa = _np.ascontiguousarray(dAs, dtype=_np.uint64)
+        self._pt = _np.ascontiguousarray(dtaus, dtype=_np.uint64)
+        self.h = load().bsofi_batch_graph_create(len(self._n), self._n.ctypes.data,
+                                                 self._L.ctypes.data, self._pa.ctypes.data,
+                                                 self._ld.ctypes.data, self._pt.ctypes.data,
+                                                 dwork, streams)
+        if not self.h:
+            raise RuntimeError("bsofi_batch_graph_create failed")
+
+    def launch(self, stream):
+        return load().bsofi_batch_graph_launch(self.h, stream)
+
+    def close(self):
+        if self.h:
+            load().bsofi_batch_graph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Server:
     """Continuous-batching inversion server (bsofi_server_*): submit
     device-resident matrices, poll for finished requests."""

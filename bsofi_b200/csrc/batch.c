@@ -143,3 +143,63 @@ fail:
   free(off);
   return BSOFI_INFO_CUDA - (int)e;
 }
+
+/* ------------------------------------------------------------ graph */
+struct bsofi_batch_graph {
+  cudaGraph_t graph;
+  cudaGraphExec_t exec;
+};
+
+bsofi_batch_graph *bsofi_batch_graph_create(int count, const int *n, const int *L,
+                                            double *const *dA, const int *ldda,
+                                            double *const *dtau, void *dwork, int streams) {
+  bsofi_batch_graph *g;
+  cudaStream_t cs = NULL;
+  cudaError_t e;
+  int r;
+  if (count < 1) return NULL;
+  /* Kernel attributes and the stream pool are set up outside the capture. */
+  if (bsofi_dev_prepare() != 0) return NULL;
+  {
+    stream_pool *p;
+    int want = streams < 1 ? 8 : (streams > MAX_STREAMS ? MAX_STREAMS : streams);
+    if (pool_get(want, &p) != cudaSuccess) return NULL;
+  }
+  g = (bsofi_batch_graph *)calloc(1, sizeof(bsofi_batch_graph));
+  if (!g) return NULL;
+  if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) goto fail;
+  if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed) != cudaSuccess) goto fail;
+  r = bsofi_device_invert_batched(count, n, L, dA, ldda, dtau, dwork, streams, cs);
+  e = cudaStreamEndCapture(cs, &g->graph);
+  if (r != 0 || e != cudaSuccess) goto fail;
+  if (cudaGraphInstantiate(&g->exec, g->graph, 0) != cudaSuccess) goto fail;
+  cudaStreamDestroy(cs);
+  return g;
+fail:
+  if (cs) {
+    enum cudaStreamCaptureStatus st;
+    if (cudaStreamIsCapturing(cs, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone) {
+      cudaGraph_t junk = NULL;
+      cudaStreamEndCapture(cs, &junk);
+      if (junk) cudaGraphDestroy(junk);
+    }
+    cudaStreamDestroy(cs);
+  }
+  cudaGetLastError();
+  bsofi_batch_graph_destroy(g);
+  return NULL;
+}
+
+int bsofi_batch_graph_launch(bsofi_batch_graph *g, void *stream) {
+  cudaError_t e;
+  if (!g || !g->exec || !stream) return -1;
+  e = cudaGraphLaunch(g->exec, (cudaStream_t)stream);
+  return e == cudaSuccess ? 0 : BSOFI_INFO_CUDA - (int)e;
+}
+
+void bsofi_batch_graph_destroy(bsofi_batch_graph *g) {
+  if (!g) return;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  free(g);
+}

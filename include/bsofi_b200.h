@@ -210,6 +210,21 @@ int bsofi_device_invert_batched(int count, const int *n, const int *L, double *c
                                 const int *ldda, double *const *dtau, void *dwork, int streams,
                                 void *stream);
 
+/* The same batch captured once into a CUDA graph and replayed (no reference
+ * counterpart).  A Monte Carlo sweep re-inverts the same walkers' buffers
+ * every step; a graph replays the ~40 launches per walker with one call.
+ * bsofi_batch_graph_create captures the batch (arguments as for
+ * bsofi_device_invert_batched; the buffers are bound into the graph) and
+ * returns NULL on failure; bsofi_batch_graph_launch enqueues one replay on
+ * `stream` (not the legacy default stream) and returns 0 or
+ * BSOFI_INFO_CUDA - cudaError_t; the caller refills dA between replays. */
+typedef struct bsofi_batch_graph bsofi_batch_graph;
+bsofi_batch_graph *bsofi_batch_graph_create(int count, const int *n, const int *L,
+                                            double *const *dA, const int *ldda,
+                                            double *const *dtau, void *dwork, int streams);
+int bsofi_batch_graph_launch(bsofi_batch_graph *graph, void *stream);
+void bsofi_batch_graph_destroy(bsofi_batch_graph *graph);
+
 /* Continuous-batching inversion server (no reference counterpart: the
  * reference's calls are synchronous, one matrix at a time).  Requests invert
  * caller-owned device-resident matrices; up to `slots` run at once, each on

@@ -43,3 +43,42 @@ def test_batched_matches_single(cuda_device):
 def test_batched_rejects_bad_sizes(cuda_device):
     rc = api.device_invert_batched([0], [4], [16], [4], [16], 16)
     assert rc == -1
+
+
+def test_batch_graph_replays_match_direct(cuda_device):
+    """A batch captured into a CUDA graph and replayed twice (inputs refilled
+    between replays) gives the direct batched call's results."""
+    import torch
+    from gpu_util import from_device_colmajor, to_device_colmajor
+    specs = [(64, 6, 11), (81, 4, 12), (144, 5, 13), (256, 3, 14), (16, 10, 15)]
+    mats = [hubbard_matrix(int(round(n ** 0.5)), L, 4.0, seed=s) for n, L, s in specs]
+    ns = [sp[0] for sp in specs]
+    Ls = [sp[1] for sp in specs]
+    ldds = [n * L for n, L in zip(ns, Ls)]
+    pristine = [to_device_colmajor(torch, M) for M in mats]
+    direct = [p.clone() for p in pristine]
+    work = [torch.empty_like(p) for p in pristine]
+    taus_d = [torch.zeros(n * L, dtype=torch.float64, device=cuda_device) for n, L in zip(ns, Ls)]
+    taus_g = [torch.zeros(n * L, dtype=torch.float64, device=cuda_device) for n, L in zip(ns, Ls)]
+    nbytes = api.batch_workspace_bytes(ns, Ls, ldds)
+    ws_d = torch.zeros(nbytes // 8 + 1, dtype=torch.float64, device=cuda_device)
+    ws_g = torch.zeros(nbytes // 8 + 1, dtype=torch.float64, device=cuda_device)
+    rc = api.device_invert_batched(ns, Ls, [t.data_ptr() for t in direct], ldds,
+                                   [t.data_ptr() for t in taus_d], ws_d.data_ptr(), streams=4)
+    torch.cuda.synchronize()
+    assert rc == 0
+    g = api.BatchGraph(ns, Ls, [t.data_ptr() for t in work], ldds,
+                       [t.data_ptr() for t in taus_g], ws_g.data_ptr(), streams=4)
+    stream = torch.cuda.Stream()
+    for _ in range(2):
+        for w, p in zip(work, pristine):
+            w.copy_(p)
+        torch.cuda.synchronize()
+        assert g.launch(stream.cuda_stream) == 0
+        stream.synchronize()
+        for M, n, L, A, D in zip(mats, ns, Ls, work, direct):
+            X = from_device_colmajor(A, n * L)
+            Xd = from_device_colmajor(D, n * L)
+            assert rel_fro(X, Xd) < inverse_tolerance(M, Xd)
+            assert residual(M, X) < 1e-13
+    g.close()
