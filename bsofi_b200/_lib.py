@@ -63,6 +63,10 @@ _SIGS = {
     "bsofi_batch_graph_create": (_vp, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int]),
     "bsofi_batch_graph_launch": (ctypes.c_int, [_vp, _vp]),
     "bsofi_batch_graph_destroy": (None, [_vp]),
+    "bsofi_autotune": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "bsofi_plan_get": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp]),
+    "bsofi_plan_set": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp]),
+    "bsofi_plan_clear": (None, []),
     "bsofi_server_create": (_vp, [ctypes.c_int, ctypes.c_ulonglong]),
     "bsofi_server_request_bytes": (ctypes.c_ulonglong, [ctypes.c_int] * 3),
     "bsofi_server_submit": (ctypes.c_longlong, [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int,

@@ -186,6 +186,32 @@ def device_invert_batched(ns, Ls, dAs, lddas, dtaus, dwork, streams=8, stream=0)
                                               stream)
 
 
+def autotune(n, L, reps=3, stream=0):
+    """bsofi_autotune: time the launch-plan candidates for (n, L) on the
+    device and keep the fastest; returns the plan (4 ints)."""
+    plan = np.zeros(4, dtype=np.int32)
+    rc = load().bsofi_autotune(n, L, reps, stream, plan.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("bsofi_autotune failed (%d)" % rc)
+    return [int(v) for v in plan]
+
+
+def plan_get(n, L):
+    """(tuned, plan) for (n, L): tuned is False for the default plan."""
+    plan = np.zeros(4, dtype=np.int32)
+    tuned = load().bsofi_plan_get(n, L, plan.ctypes.data)
+    return bool(tuned), [int(v) for v in plan]
+
+
+def plan_set(n, L, plan):
+    p = np.ascontiguousarray(plan, dtype=np.int32)
+    return load().bsofi_plan_set(n, L, p.ctypes.data)
+
+
+def plan_clear():
+    load().bsofi_plan_clear()
+
+
 class BatchGraph:
     """bsofi_batch_graph_*: a batch of inversions captured once into a CUDA
     graph; launch(stream) replays it on the same device buffers."""

@@ -60,6 +60,16 @@ int bsofi_dev_bsoi_finish(int n, int L, double *dA, int ldd, void *dws, void *st
  * index), [1] BSOF wait timeout, [2] BSOI wait timeout (nonzero = error). */
 int *bsofi_dev_info_ptr(void *dws);
 
+/* Launch plans per (n, L): plan[0] BSOI mode (0 persistent, 1 per-step by
+ * tile count, 2/3/4 per-step 64x64 / 128x128 16-warp / 128x128 8-warp
+ * tiles), plan[1] BSTRI recurrence tile shape (launch_gemm cfg), plan[2]
+ * BSOF worker CTAs, plan[3] reserved.  get returns 1 for a tuned plan, 0 for
+ * the default (plan still filled); set returns -1 for an invalid plan. */
+int bsofi_dev_plan_get(int n, int L, int *plan);
+int bsofi_dev_plan_set(int n, int L, const int *plan);
+void bsofi_dev_plan_clear(void);
+void bsofi_dev_plan_clear_one(int n, int L);
+
 /* Number of kernels the last bsofi_dev_* call on this thread launched. */
 long long bsofi_dev_launch_count(void);
 void bsofi_dev_add_launches(long long c);

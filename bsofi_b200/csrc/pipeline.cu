@@ -11,6 +11,9 @@
 //   Y      (L-1) x (n x n)          BSTRI scratch  R_{i,L-1} R_{L-1,L-1}^{-1}
 //   carry  2 x (ldd x n)            BSOI ping-pong block column
 #include <climits>
+#include <map>
+#include <mutex>
+#include <utility>
 #include <vector>
 #include "bsofi_device.h"
 #include "bsofi_kernels.h"
@@ -38,6 +41,42 @@ struct GemmTimer {
   }
 };
 thread_local GemmTimer g_timer;
+
+// Launch plan of one problem size: how BSOI runs (0: one persistent launch;
+// 1: one GEMM launch per step with the tile shape chosen by tile count; 2, 3,
+// 4: per step with 64x64, 128x128/16-warp, 128x128/8-warp tiles), the tile
+// shape of the BSTRI row-recurrence GEMMs (launch_gemm's cfg) and the number
+// of BSOF worker CTAs of a single inversion.  Tuned plans (bsofi_autotune)
+// live in a process-wide table; other sizes use the default below.
+struct Plan {
+  int bsoi, bstri_cfg, workers;
+};
+std::mutex g_plan_mu;
+std::map<std::pair<int, int>, Plan> g_plans;
+
+Plan default_plan(int n, int L) {
+  // The persistent BSOI kernel pays off once a step fills every SM with
+  // 128 x 128 tiles; below that, per-step launches of smaller tiles win.
+  const int tiles = bsoi_row_bands(n * L) * ((2 * n + 127) / 128);
+  return Plan{tiles >= 148 ? 0 : 1, 2, 32};
+}
+
+Plan plan_for(int n, int L) {
+  std::lock_guard<std::mutex> lk(g_plan_mu);
+  auto it = g_plans.find({n, L});
+  return it == g_plans.end() ? default_plan(n, L) : it->second;
+}
+
+// Diagnostics override of the BSOF worker count (0 = the plan's).
+thread_local int g_workers_override = 0;
+
+// Worker CTAs of one BSOF launch: the caller's count, else the override, else
+// the plan's.
+int bsof_workers(int n, int L, int requested) {
+  if (requested > 0) return requested;
+  if (g_workers_override > 0) return g_workers_override;
+  return plan_for(n, L).workers;
+}
 
 struct Layout {
   size_t info, sync, bsync, tl, T, G, W, Y, C0, C1, total;
@@ -150,11 +189,10 @@ __global__ void __launch_bounds__(256) build_leaf_t_kernel(const double* __restr
   Tout[tid] = sT[tid % 16][tid / 16];
 }
 
-thread_local int g_bsof_workers = 32;
-
 // BSOF.  form_q: the persistent kernel also forms G_k = Q_k^T for BSOI.
+// workers: worker CTAs for 16-wide leaves (four times as many for 8-wide).
 int run_bsof(int n, int L, double* dA, int ldd, double* dtau, void* ws, cudaStream_t st,
-             bool form_q) {
+             bool form_q, int base_workers) {
   Layout ly = layout(n, L, ldd);
   double* Tb = at<double>(ws, ly.T);
   double* G = at<double>(ws, ly.G);
@@ -165,7 +203,7 @@ int run_bsof(int n, int L, double* dA, int ldd, double* dtau, void* ws, cudaStre
   if (form_q) CK(launch_set_identity(G, 2 * n, 2 * n, 4ll * n * n, L - 1, st));
   // 16-wide leaves apply with DMMA and need few workers; 8-wide leaves
   // (n > 256) have three times the tasks per leaf and use every SM.
-  int workers = bsof_leaf_width(n) == 16 ? g_bsof_workers : 4 * g_bsof_workers;
+  int workers = bsof_leaf_width(n) == 16 ? base_workers : 4 * base_workers;
   if (form_q) workers *= 2;
   CK(launch_bsof_persistent(dA, ldd, n, L, dtau, Tb, form_q ? G : nullptr, ly.maxleaves, sync,
                             sync + ntiles, sync + ntiles + ly.leaves, at<int>(ws, ly.info) + 1,
@@ -272,7 +310,7 @@ int run_bstri(int n, int L, double* dA, int ldd, void* ws, cudaStream_t st) {
     c.alpha = 1.0;
     c.beta0 = 0.0;
     c.beta1 = 1.0;
-    CK(launch_gemm(dr, a, b, c, 1, 2, st));
+    CK(launch_gemm(dr, a, b, c, 1, plan_for(n, L).bstri_cfg, st));
   }
   return 0;
 }
@@ -323,8 +361,9 @@ int bsoi_carry(int n, int L, double* dA, int ldd, void* ws, cudaStream_t st) {
   return 0;
 }
 
-// BSOI step k as one GEMM launch: [X(:,k) | carry] Q_k^T -> [carry' | X(:,k+1)].
-int bsoi_step(int n, int L, int k, double* dA, int ldd, void* ws, cudaStream_t st) {
+// BSOI step k as one GEMM launch: [X(:,k) | carry] Q_k^T -> [carry' | X(:,k+1)]
+// (cfg: launch_gemm's tile shape, 0 = by tile count).
+int bsoi_step(int n, int L, int k, double* dA, int ldd, void* ws, cudaStream_t st, int cfg = 0) {
   Layout ly = layout(n, L, ldd);
   double* G = at<double>(ws, ly.G);
   double* C[2] = {at<double>(ws, ly.C0), at<double>(ws, ly.C1)};
@@ -351,7 +390,7 @@ int bsoi_step(int n, int L, int k, double* dA, int ldd, void* ws, cudaStream_t s
   c.nsplit = n;
   c.alpha = 1.0;
   if (g_timer.on) CKM(g_timer.mark(st));
-  CK(launch_gemm(d, a, b, c, 1, 0, st));
+  CK(launch_gemm(d, a, b, c, 1, cfg, st));
   if (g_timer.on) CKM(g_timer.mark(st));
   return 0;
 }
@@ -370,7 +409,6 @@ int run_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* ws, cu
   Layout ly = layout(n, L, ldd);
   double* G = at<double>(ws, ly.G);
   double* C[2] = {at<double>(ws, ly.C0), at<double>(ws, ly.C1)};
-  const int N = n * L, n2 = 2 * n;
   // G_k = Q_k^T unless the factorization already formed it.
   if (!q_ready) {
     int e = bsoi_form_q(n, L, dA, ldd, dtau, ws, st);
@@ -378,8 +416,8 @@ int run_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* ws, cu
   }
   int e = bsoi_carry(n, L, dA, ldd, ws, st);
   if (e) return e;
-  const int row_bands = bsoi_row_bands(N), col_tiles = (n2 + 127) / 128;
-  if (row_bands * col_tiles >= 64) {
+  const Plan plan = plan_for(n, L);
+  if (plan.bsoi == 0) {
     // One persistent launch over all steps (rows flow from step to step).
     int* bs = at<int>(ws, ly.bsync);
     CKM(cudaMemsetAsync(bs, 0, sizeof(int) * ly.bsync_ints, st));
@@ -388,9 +426,11 @@ int run_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* ws, cu
                               at<int>(ws, ly.info) + 2, st));
     if (g_timer.on) CKM(g_timer.mark(st));
   } else {
-    // Small problems: one launch per step with small tiles (more CTAs per step).
+    // One launch per step (small problems: more, smaller tiles per step).
+    static const int cfg_of[5] = {0, 0, 2, 3, 1};
+    const int cfg = cfg_of[plan.bsoi >= 1 && plan.bsoi <= 4 ? plan.bsoi : 1];
     for (int k = L - 2; k >= 0; k--)
-      if ((e = bsoi_step(n, L, k, dA, ldd, ws, st)) != 0) return e;
+      if ((e = bsoi_step(n, L, k, dA, ldd, ws, st, cfg)) != 0) return e;
   }
   return bsoi_finish(n, L, dA, ldd, ws, st);
 }
@@ -411,7 +451,7 @@ int bsofi_dev_zero_structural(int n, int L, double* dA, int ldd, void* stream) {
 
 int bsofi_dev_bsof(int n, int L, double* dA, int ldd, double* dtau, void* dws, void* stream) {
   g_launches = 0;
-  return run_bsof(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, false);
+  return run_bsof(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, false, bsof_workers(n, L, 0));
 }
 
 int bsofi_dev_bstri(int n, int L, double* dA, int ldd, void* dws, void* stream) {
@@ -422,7 +462,7 @@ int bsofi_dev_bstri(int n, int L, double* dA, int ldd, void* dws, void* stream) 
 int bsofi_dev_bsoftri(int n, int L, double* dA, int ldd, double* dtau, void* dws,
                       void* stream) {
   g_launches = 0;
-  int e = run_bsof(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, false);
+  int e = run_bsof(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, false, bsof_workers(n, L, 0));
   if (e) return e;
   return run_bstri(n, L, dA, ldd, dws, (cudaStream_t)stream);
 }
@@ -457,10 +497,8 @@ int bsofi_dev_invert(int n, int L, double* dA, int ldd, double* dtau, void* dws,
 int bsofi_dev_invert_ex(int n, int L, double* dA, int ldd, double* dtau, void* dws, void* stream,
                         int workers) {
   g_launches = 0;
-  const int saved = g_bsof_workers;
-  if (workers > 0) g_bsof_workers = workers;
-  int e = run_bsof(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, true);
-  g_bsof_workers = saved;
+  int e = run_bsof(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, true,
+                   bsof_workers(n, L, workers));
   if (!e) e = run_bstri(n, L, dA, ldd, dws, (cudaStream_t)stream);
   if (!e) e = run_bsoi(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, true);
   return e;
@@ -474,7 +512,37 @@ int bsofi_dev_bsof_timeline(int n, int L, int ldd, void* dws, unsigned long long
   return ly.leaves;
 }
 
-void bsofi_dev_set_bsof_workers(int w) { g_bsof_workers = w > 0 ? w : 32; }
+void bsofi_dev_set_bsof_workers(int w) { g_workers_override = w > 0 ? w : 0; }
+
+int bsofi_dev_plan_get(int n, int L, int* plan) {
+  std::lock_guard<std::mutex> lk(g_plan_mu);
+  auto it = g_plans.find({n, L});
+  const Plan p = it == g_plans.end() ? default_plan(n, L) : it->second;
+  plan[0] = p.bsoi;
+  plan[1] = p.bstri_cfg;
+  plan[2] = p.workers;
+  plan[3] = 0;
+  return it == g_plans.end() ? 0 : 1;
+}
+
+int bsofi_dev_plan_set(int n, int L, const int* plan) {
+  if (n < 1 || L < 2 || plan[0] < 0 || plan[0] > 4 || plan[1] < 0 || plan[1] > 3 ||
+      plan[2] < 1 || plan[2] > 1024)
+    return -1;
+  std::lock_guard<std::mutex> lk(g_plan_mu);
+  g_plans[{n, L}] = Plan{plan[0], plan[1], plan[2]};
+  return 0;
+}
+
+void bsofi_dev_plan_clear(void) {
+  std::lock_guard<std::mutex> lk(g_plan_mu);
+  g_plans.clear();
+}
+
+void bsofi_dev_plan_clear_one(int n, int L) {
+  std::lock_guard<std::mutex> lk(g_plan_mu);
+  g_plans.erase({n, L});
+}
 
 int bsofi_dev_selftest_gemm(int M, int N, int K, double alpha, const double* dA, int lda,
                             int upper_a, const double* dB, int ldb, int upper_b, double beta,

@@ -225,6 +225,29 @@ bsofi_batch_graph *bsofi_batch_graph_create(int count, const int *n, const int *
 int bsofi_batch_graph_launch(bsofi_batch_graph *graph, void *stream);
 void bsofi_batch_graph_destroy(bsofi_batch_graph *graph);
 
+/* Launch plans and the autotuner (no reference counterpart).  A plan is
+ * four ints: [0] BSOI form (0 one persistent launch over all steps; 1 one
+ * GEMM launch per step, tile shape by tile count; 2 / 3 / 4 per step with
+ * 64x64 / 128x128 16-warp / 128x128 8-warp tiles), [1] tile shape of the BSTRI
+ * row-recurrence GEMMs (0 by tile count, 1 128x128 8-warp, 2 64x64, 3 128x128
+ * 16-warp), [2] BSOF worker CTAs of a single inversion, [3] reserved (0).
+ * Every inversion of block size n with L blocks uses the tuned plan of (n, L)
+ * if there is one, else a default (persistent BSOI when a step has at least
+ * 148 tiles of 128 x 128, per-step otherwise; 64x64 recurrence tiles; 32
+ * workers).  bsofi_autotune times the candidates one knob at a time on a
+ * synthetic matrix of that size (reps timed runs each, fastest kept; it
+ * allocates its own buffers) on `stream`, stores the winner and copies it to
+ * plan_out (may be NULL); it returns 0, -1 for an illegal size or
+ * BSOFI_INFO_CUDA - cudaError_t.  While it runs, other inversions of the same
+ * size see its trial plans.  bsofi_plan_get fills plan and returns 1 for a
+ * tuned plan, 0 for the default; bsofi_plan_set stores a plan (e.g. one saved
+ * from an earlier run) and returns -1 if it is invalid; bsofi_plan_clear
+ * forgets every tuned plan. */
+int bsofi_autotune(int n, int L, int reps, void *stream, int *plan_out);
+int bsofi_plan_get(int n, int L, int *plan);
+int bsofi_plan_set(int n, int L, const int *plan);
+void bsofi_plan_clear(void);
+
 /* Continuous-batching inversion server (no reference counterpart: the
  * reference's calls are synchronous, one matrix at a time).  Requests invert
  * caller-owned device-resident matrices; up to `slots` run at once, each on

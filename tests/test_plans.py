@@ -1,0 +1,32 @@
+"""Launch-plan table (bsofi_plan_get / _set / _clear): host logic, no GPU."""
+import pytest
+
+from bsofi_b200 import api
+
+
+@pytest.fixture(autouse=True)
+def _clear_plans():
+    api.plan_clear()
+    yield
+    api.plan_clear()
+
+
+def test_default_plan_follows_bsoi_tile_count():
+    # n = 256, L = 32: 64 row bands x 4 column tiles per step -> persistent BSOI.
+    assert api.plan_get(256, 32) == (False, [0, 2, 32, 0])
+    # n = 144, L = 20: 23 x 3 tiles per step -> one GEMM launch per step.
+    assert api.plan_get(144, 20) == (False, [1, 2, 32, 0])
+
+
+def test_set_get_clear_roundtrip():
+    assert api.plan_set(100, 8, [3, 0, 48, 0]) == 0
+    assert api.plan_get(100, 8) == (True, [3, 0, 48, 0])
+    assert api.plan_get(100, 9)[0] is False
+    api.plan_clear()
+    assert api.plan_get(100, 8)[0] is False
+
+
+@pytest.mark.parametrize("plan", [[5, 2, 32, 0], [-1, 2, 32, 0], [0, 4, 32, 0], [0, 2, 0, 0]])
+def test_invalid_plans_rejected(plan):
+    assert api.plan_set(64, 4, plan) == -1
+    assert api.plan_get(64, 4)[0] is False
