@@ -17,7 +17,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libbsofi_b200.so")
 ROOT = os.path.dirname(HERE)
 
-CU_SOURCES = ["kernels_bsof.cu", "kernels_bsoi.cu", "kernels_panel.cu", "kernels_tri.cu", "kernels_gemm.cu", "pipeline.cu", "kernels_dqmc.cu", "autotune.cu", "noalloc.cu"]
+CU_SOURCES = ["kernels_bsof.cu", "kernels_bsoi.cu", "kernels_bstri.cu", "kernels_panel.cu", "kernels_tri.cu", "kernels_gemm.cu", "pipeline.cu", "kernels_dqmc.cu", "autotune.cu", "noalloc.cu"]
 C_SOURCES = ["bsofi_api.c", "batch.c", "server.c"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -462,7 +462,7 @@ static int check_args(const int *h_ok, int n, int L, const double *A, int lda,
  * wait inside a persistent kernel that gave up) after synchronising the
  * stream. */
 static int read_info(bsofi_ctx *c, int *info) {
-  int v[3] = {0, 0, 0};
+  int v[4] = {0, 0, 0, 0};
   cudaError_t e = cudaMemcpyAsync(v, bsofi_dev_info_ptr(c->dws), sizeof(v),
                                   cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
@@ -470,7 +470,7 @@ static int read_info(bsofi_ctx *c, int *info) {
     *info = cuda_info(e);
     return *info;
   }
-  if (v[1] != 0 || v[2] != 0) {
+  if (v[1] != 0 || v[2] != 0 || v[3] != 0) {
     *info = cuda_info(cudaErrorLaunchTimeout);
     return *info;
   }

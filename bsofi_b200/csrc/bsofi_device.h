@@ -57,12 +57,13 @@ int bsofi_dev_bsoi_finish(int n, int L, double *dA, int ldd, void *dws, void *st
 
 /* Device address of the int info words inside the workspace: [0] BSTRI info
  * (values >= 0x7f7f7f7f mean 0; i > 0: R(i,i) exactly zero, 1-based global
- * index), [1] BSOF wait timeout, [2] BSOI wait timeout (nonzero = error). */
+ * index), [1] BSOF, [2] BSOI, [3] BSTRI wait timeout (nonzero = error). */
 int *bsofi_dev_info_ptr(void *dws);
 
 /* Launch plans per (n, L): plan[0] BSOI mode (0 persistent, 1 per-step by
  * tile count, 2/3/4 per-step 64x64 / 128x128 16-warp / 128x128 8-warp
- * tiles), plan[1] BSTRI recurrence tile shape (launch_gemm cfg), plan[2]
+ * tiles), plan[1] BSTRI recurrence (launch_gemm cfg per step, or 4 for the
+ * persistent recurrence kernel), plan[2]
  * BSOF worker CTAs, plan[3] reserved.  get returns 1 for a tuned plan, 0 for
  * the default (plan still filled); set returns -1 for an invalid plan. */
 int bsofi_dev_plan_get(int n, int L, int *plan);

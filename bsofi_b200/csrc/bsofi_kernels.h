@@ -34,6 +34,12 @@ cudaError_t launch_bsof_persistent(double* A, long long ld, int n, int L, double
                                    int* next_task, int* err, unsigned long long* timeline,
                                    int workers, cudaStream_t st);
 
+// Persistent BSTRI row recurrence (kernels_bstri.cu): done is (L-2) x
+// bstri_recurrence_ctmax(n, L) ints and next one int, zeroed before.
+int bstri_recurrence_ctmax(int n, int L);
+cudaError_t launch_bstri_recurrence(double* A, long long ld, const double* W, int n, int L,
+                                    int* done, int* next, int* err, cudaStream_t st);
+
 // Persistent BSOI (kernels_bsoi.cu): all p-1 steps in one launch.
 // done: (L-1) * bsoi_row_bands(N) ints and next: one int, zeroed before.
 int bsoi_row_bands(int N);
@@ -55,8 +61,8 @@ cudaError_t launch_set_identity(double* G, long long ld, int m, long long bs, in
 // BSOFI_INFO_CUDA - cudaErrorLaunchTimeout.
 constexpr int kInfoWaitFailed = -1000 - (int)cudaErrorLaunchTimeout;
 // dst(r,c) = src(r,c), or 0 where r - roff > c (roff = kNoMask copies all).
-// fold (optional): info words {info, BSOF error, BSOI error}; info becomes
-// kInfoWaitFailed when either error word is set.
+// fold (optional): info words {info, BSOF error, BSOI error, BSTRI error};
+// info becomes kInfoWaitFailed when any error word is set.
 cudaError_t launch_copy_masked(double* dst, long long ldd, const double* src, long long lds,
                                int rows, int cols, int roff, cudaStream_t st,
                                int* fold = nullptr);

@@ -139,8 +139,9 @@ cudaError_t launch_set_identity(double* G, long long ld, int m, long long bs, in
 __global__ void copy_masked_kernel(double* dst, long long ldd, const double* src, long long lds,
                                    int rows, int cols, int roff, int* fold) {
   // fold (optional): the workspace info words {BSTRI info, BSOF error, BSOI
-  // error}; a bounded wait that gave up turns the info word into an error.
-  if (fold != nullptr && blockIdx.x == 0 && threadIdx.x == 0 && (fold[1] | fold[2]) != 0)
+  // error, BSTRI error}; a bounded wait that gave up turns the info word into
+  // an error.
+  if (fold != nullptr && blockIdx.x == 0 && threadIdx.x == 0 && (fold[1] | fold[2] | fold[3]) != 0)
     fold[0] = kInfoWaitFailed;
   long long total = (long long)rows * cols;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;

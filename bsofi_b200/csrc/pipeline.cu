@@ -44,8 +44,9 @@ thread_local GemmTimer g_timer;
 
 // Launch plan of one problem size: how BSOI runs (0: one persistent launch;
 // 1: one GEMM launch per step with the tile shape chosen by tile count; 2, 3,
-// 4: per step with 64x64, 128x128/16-warp, 128x128/8-warp tiles), the tile
-// shape of the BSTRI row-recurrence GEMMs (launch_gemm's cfg) and the number
+// 4: per step with 64x64, 128x128/16-warp, 128x128/8-warp tiles), the BSTRI
+// row recurrence (launch_gemm's cfg per step, or 4: one persistent launch)
+// and the number
 // of BSOF worker CTAs of a single inversion.  Tuned plans (bsofi_autotune)
 // live in a process-wide table; other sizes use the default below.
 struct Plan {
@@ -79,8 +80,8 @@ int bsof_workers(int n, int L, int requested) {
 }
 
 struct Layout {
-  size_t info, sync, bsync, tl, T, G, W, Y, C0, C1, total;
-  int nbw, maxleaves, tiles, leaves, sync_ints, bsync_ints;
+  size_t info, sync, bsync, rsync, tl, T, G, W, Y, C0, C1, total;
+  int nbw, maxleaves, tiles, leaves, sync_ints, bsync_ints, rsync_ints;
 };
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
@@ -93,13 +94,16 @@ Layout layout(int n, int L, int ldd) {
   l.maxleaves = max((2 * n + l.nbw - 1) / l.nbw, 2 * l.tiles);
   l.sync_ints = (L + 2 * (L - 1)) * l.tiles + l.leaves + 2;
   size_t off = 0;
-  l.info = off;  // int info, int bsof error word
+  l.info = off;  // BSTRI info, BSOF / BSOI / BSTRI wait error words
   off += 256;
   l.sync = off;  // tile counters, leaf flags, task counter, spare
   off += align256(sizeof(int) * (size_t)l.sync_ints);
   l.bsync_ints = (L - 1) * bsoi_row_bands(n * L) + 2;
   l.bsync = off;  // BSOI: finished tiles per (step, row band), tile counter
   off += align256(sizeof(int) * (size_t)l.bsync_ints);
+  l.rsync_ints = (L > 2 ? (L - 2) * bstri_recurrence_ctmax(n, L) : 0) + 2;
+  l.rsync = off;  // BSTRI recurrence: finished row tiles per (step, column tile), tile counter
+  off += align256(sizeof(int) * (size_t)l.rsync_ints);
   l.tl = off;    // BSOF timeline: 4 globaltimer stamps per leaf
   off += align256(sizeof(unsigned long long) * 4 * (size_t)l.leaves);
   l.T = off;
@@ -288,6 +292,17 @@ int run_bstri(int n, int L, double* dA, int ldd, void* ws, cudaStream_t st) {
     CK(launch_gemm(d, a, b, c, L - 2, 0, st));
   }
   // Row recurrence: X_{i, i+1:L} = W_i X_{i+1, i+1:L} (+ Z_i on the last block).
+  const int rec = plan_for(n, L).bstri_cfg;
+  CKM(cudaMemsetAsync(info + 3, 0, sizeof(int), st));
+  if (rec == 4) {
+    // One persistent launch, column tiles pipelined across the steps.
+    if (L >= 3) {
+      int* rs = at<int>(ws, ly.rsync);
+      CKM(cudaMemsetAsync(rs, 0, sizeof(int) * ly.rsync_ints, st));
+      CK(launch_bstri_recurrence(dA, ldd, W, n, L, rs, rs + ly.rsync_ints - 2, info + 3, st));
+    }
+    return 0;
+  }
   for (int i = L - 3; i >= 0; i--) {
     const int ncol = (L - 1 - i) * n;
     GemmDims dr = {n, ncol, n};
@@ -310,7 +325,7 @@ int run_bstri(int n, int L, double* dA, int ldd, void* ws, cudaStream_t st) {
     c.alpha = 1.0;
     c.beta0 = 0.0;
     c.beta1 = 1.0;
-    CK(launch_gemm(dr, a, b, c, 1, plan_for(n, L).bstri_cfg, st));
+    CK(launch_gemm(dr, a, b, c, 1, rec, st));
   }
   return 0;
 }
@@ -526,7 +541,7 @@ int bsofi_dev_plan_get(int n, int L, int* plan) {
 }
 
 int bsofi_dev_plan_set(int n, int L, const int* plan) {
-  if (n < 1 || L < 2 || plan[0] < 0 || plan[0] > 4 || plan[1] < 0 || plan[1] > 3 ||
+  if (n < 1 || L < 2 || plan[0] < 0 || plan[0] > 4 || plan[1] < 0 || plan[1] > 4 ||
       plan[2] < 1 || plan[2] > 1024)
     return -1;
   std::lock_guard<std::mutex> lk(g_plan_mu);

@@ -43,7 +43,7 @@ typedef struct {
   size_t off, len;
   cudaStream_t stream;
   cudaEvent_t done;
-  int *hinfo; /* pinned: BSTRI info word, BSOF and BSOI error words */
+  int *hinfo; /* pinned: BSTRI info word, BSOF / BSOI / BSTRI wait error words */
 } slot;
 
 typedef struct {
@@ -157,7 +157,7 @@ bsofi_server *bsofi_server_create(int slots, unsigned long long pool_bytes) {
   for (i = 0; i < slots; i++) {
     if (cudaStreamCreateWithFlags(&sv->s[i].stream, cudaStreamNonBlocking) != cudaSuccess) goto fail;
     if (cudaEventCreateWithFlags(&sv->s[i].done, cudaEventDisableTiming) != cudaSuccess) goto fail;
-    if (cudaMallocHost((void **)&sv->s[i].hinfo, 3 * sizeof(int)) != cudaSuccess) goto fail;
+    if (cudaMallocHost((void **)&sv->s[i].hinfo, 4 * sizeof(int)) != cudaSuccess) goto fail;
   }
   return sv;
 fail:
@@ -210,7 +210,7 @@ static int launch(bsofi_server *sv, slot *sl, const request *r) {
   void *ws = sv->pool + sl->off;
   e = bsofi_dev_invert_ex(r->n, r->L, r->dA, r->ldda, r->dtau, ws, sl->stream, workers);
   if (!e)
-    e = (int)cudaMemcpyAsync(sl->hinfo, bsofi_dev_info_ptr(ws), 3 * sizeof(int),
+    e = (int)cudaMemcpyAsync(sl->hinfo, bsofi_dev_info_ptr(ws), 4 * sizeof(int),
                              cudaMemcpyDeviceToHost, sl->stream);
   if (!e) e = (int)cudaEventRecord(sl->done, sl->stream);
   return e;
@@ -268,7 +268,7 @@ int bsofi_server_poll(bsofi_server *sv, long long *done_ids, int *done_status, i
     if (q == cudaErrorNotReady) continue;
     done_ids[ndone] = sl->id;
     if (q != cudaSuccess) done_status[ndone] = BSOFI_INFO_CUDA - (int)q;
-    else if (sl->hinfo[1] != 0 || sl->hinfo[2] != 0)
+    else if (sl->hinfo[1] != 0 || sl->hinfo[2] != 0 || sl->hinfo[3] != 0)
       done_status[ndone] = BSOFI_INFO_CUDA - (int)cudaErrorLaunchTimeout;
     else done_status[ndone] = sl->hinfo[0] >= 0x7f7f7f7f ? 0 : sl->hinfo[0];
     ndone++;

@@ -152,7 +152,7 @@ unsigned long long bsofi_device_workspace_bytes(int n, int L, int ldda);
  * bsofi_device_info(dwork) (device int, values >= 0x7f7f7f7f mean 0; after
  * bsofi_device_invert or bsofi_device_bsoi it is BSOFI_INFO_CUDA -
  * cudaErrorLaunchTimeout if a bounded wait inside a persistent kernel gave
- * up; words 1 and 2 are the BSOF and BSOI wait error flags). */
+ * up; words 1, 2 and 3 are the BSOF, BSOI and BSTRI wait error flags). */
 int bsofi_device_invert(int n, int L, double *dA, int ldda, double *dtau, void *dwork,
                         void *stream);
 int bsofi_device_bsoftri(int n, int L, double *dA, int ldda, double *dtau, void *dwork,
@@ -228,9 +228,10 @@ void bsofi_batch_graph_destroy(bsofi_batch_graph *graph);
 /* Launch plans and the autotuner (no reference counterpart).  A plan is
  * four ints: [0] BSOI form (0 one persistent launch over all steps; 1 one
  * GEMM launch per step, tile shape by tile count; 2 / 3 / 4 per step with
- * 64x64 / 128x128 16-warp / 128x128 8-warp tiles), [1] tile shape of the BSTRI
- * row-recurrence GEMMs (0 by tile count, 1 128x128 8-warp, 2 64x64, 3 128x128
- * 16-warp), [2] BSOF worker CTAs of a single inversion, [3] reserved (0).
+ * 64x64 / 128x128 16-warp / 128x128 8-warp tiles), [1] the BSTRI row
+ * recurrence (one GEMM launch per step with tiles 0 by tile count, 1 128x128
+ * 8-warp, 2 64x64, 3 128x128 16-warp; or 4: one persistent launch of 64x64
+ * tiles pipelined across the steps), [2] BSOF worker CTAs of a single inversion, [3] reserved (0).
  * Every inversion of block size n with L blocks uses the tuned plan of (n, L)
  * if there is one, else a default (persistent BSOI when a step has at least
  * 148 tiles of 128 x 128, per-step otherwise; 64x64 recurrence tiles; 32

@@ -37,7 +37,7 @@ def test_every_plan_inverts(cuda_device, n, L):
     assert info == 0
     tol = inverse_tolerance(M, Xref)
     for bsoi in range(5):
-        for rc in (0, 1, 2, 3):
+        for rc in (0, 1, 2, 3, 4):
             assert api.plan_set(n, L, [bsoi, rc, 24, 0]) == 0
             X = _device_invert(torch, M, n, L)
             assert rel_fro(X, Xref) < tol, (bsoi, rc)

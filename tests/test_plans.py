@@ -26,7 +26,7 @@ def test_set_get_clear_roundtrip():
     assert api.plan_get(100, 8)[0] is False
 
 
-@pytest.mark.parametrize("plan", [[5, 2, 32, 0], [-1, 2, 32, 0], [0, 4, 32, 0], [0, 2, 0, 0]])
+@pytest.mark.parametrize("plan", [[5, 2, 32, 0], [-1, 2, 32, 0], [0, 5, 32, 0], [0, 2, 0, 0]])
 def test_invalid_plans_rejected(plan):
     assert api.plan_set(64, 4, plan) == -1
     assert api.plan_get(64, 4)[0] is False
