@@ -61,7 +61,7 @@ int bsofi_dev_bsoi_finish(int n, int L, double *dA, int ldd, void *dws, void *st
 int *bsofi_dev_info_ptr(void *dws);
 
 /* Launch plans per (n, L): plan[0] BSOI mode (0 persistent, 1 per-step by
- * tile count, 2/3/4 per-step 64x64 / 128x128 16-warp / 128x128 8-warp
+ * tile count, 2/3/4 per-step 64x64 / 128x128 K-stage 32 / 128x128 K-stage 16
  * tiles), plan[1] BSTRI recurrence (launch_gemm cfg per step, or 4 for the
  * persistent recurrence kernel), plan[2]
  * BSOF worker CTAs, plan[3] reserved.  get returns 1 for a tuned plan, 0 for

@@ -50,7 +50,7 @@ cudaError_t launch_bsoi_persistent(double* A, long long ld, double* carry0, doub
 cudaError_t launch_trtri_blocks(double* A, long long ld, int n, long long bstride,
                                 int nblk, int* info, cudaStream_t st);
 
-// cfg: 0 = choose by tile count, 1 = 128x128 (8 warps), 2 = 64x64, 3 = 128x128 (16 warps).
+// cfg: 0 = choose by tile count, 1 = 128x128 (K stage 16), 2 = 64x64, 3 = 128x128 (K stage 32).
 cudaError_t launch_gemm(const GemmDims& d, const GemmA& a, const GemmB& b,
                         const GemmC& c, int batch, int cfg, cudaStream_t st);
 cudaError_t gemm_init_attributes();

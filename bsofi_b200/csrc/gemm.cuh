@@ -70,7 +70,7 @@ struct TileCfg {
 };
 
 using CfgL = TileCfg<128, 128, 2, 4, 3>;  // 256 threads, warp tile 64x32
-using CfgM = TileCfg<128, 128, 4, 4, 3, 32>;  // 512 threads, warp tile 32x32, K stage 32
+using CfgM = TileCfg<128, 128, 2, 4, 3, 32>;  // 256 threads, warp tile 64x32, K stage 32
 using CfgS = TileCfg<64, 64, 2, 2, 3>;    // 128 threads, warp tile 32x32
 
 BSOFI_DEVINL int clamp02(long long v) { return v < 0 ? 0 : (v > 2 ? 2 : (int)v); }

@@ -44,7 +44,7 @@ thread_local GemmTimer g_timer;
 
 // Launch plan of one problem size: how BSOI runs (0: one persistent launch;
 // 1: one GEMM launch per step with the tile shape chosen by tile count; 2, 3,
-// 4: per step with 64x64, 128x128/16-warp, 128x128/8-warp tiles), the BSTRI
+// 4: per step with 64x64, 128x128 K32, 128x128 K16 tiles), the BSTRI
 // row recurrence (launch_gemm's cfg per step, or 4: one persistent launch)
 // and the number
 // of BSOF worker CTAs of a single inversion.  Tuned plans (bsofi_autotune)

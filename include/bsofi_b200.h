@@ -228,10 +228,11 @@ void bsofi_batch_graph_destroy(bsofi_batch_graph *graph);
 /* Launch plans and the autotuner (no reference counterpart).  A plan is
  * four ints: [0] BSOI form (0 one persistent launch over all steps; 1 one
  * GEMM launch per step, tile shape by tile count; 2 / 3 / 4 per step with
- * 64x64 / 128x128 16-warp / 128x128 8-warp tiles), [1] the BSTRI row
- * recurrence (one GEMM launch per step with tiles 0 by tile count, 1 128x128
- * 8-warp, 2 64x64, 3 128x128 16-warp; or 4: one persistent launch of 64x64
- * tiles pipelined across the steps), [2] BSOF worker CTAs of a single inversion, [3] reserved (0).
+ * 64x64 / 128x128 with 32-deep K stages / 128x128 with 16-deep K stages),
+ * [1] the BSTRI row recurrence (one GEMM launch per step with tiles 0 by
+ * tile count, 1 128x128 K16, 2 64x64, 3 128x128 K32; or 4: one persistent
+ * launch of 64x64 tiles pipelined across the steps), [2] BSOF worker CTAs of
+ * a single inversion, [3] reserved (0).
  * Every inversion of block size n with L blocks uses the tuned plan of (n, L)
  * if there is one, else a default (persistent BSOI when a step has at least
  * 148 tiles of 128 x 128, per-step otherwise; 64x64 recurrence tiles; 32
