@@ -101,11 +101,11 @@ BSOFI_API int bsofi_autotune(int n, int L, int reps, void* stream, int* plan_out
   if ((c = time_plan(n, L, ldd, b, st, plan, reps, &best)) != cudaSuccess) goto fail;
   {
     // Knob 0: BSOI form; knob 1: BSTRI recurrence tiles; knob 2: BSOF workers.
-    static const int cand0[] = {0, 1, 2, 3, 4};
+    static const int cand0[] = {0, 5, 1, 2, 3, 4};
     static const int cand1[] = {2, 4, 0, 3, 1};
     static const int cand2[] = {32, 48, 16, 64};
     const int* cands[3] = {cand0, cand1, cand2};
-    const int ncand[3] = {5, 5, 4};
+    const int ncand[3] = {6, 5, 4};
     for (int knob = 0; knob < 3; knob++) {
       for (int i = 0; i < ncand[knob]; i++) {
         if (cands[knob][i] == plan[knob]) continue;

@@ -41,11 +41,12 @@ cudaError_t launch_bstri_recurrence(double* A, long long ld, const double* W, in
                                     int* done, int* next, int* err, cudaStream_t st);
 
 // Persistent BSOI (kernels_bsoi.cu): all p-1 steps in one launch.
-// done: (L-1) * bsoi_row_bands(N) ints and next: one int, zeroed before.
+// done: (L-1) * bsoi_row_bands(N) ints and next: one int, zeroed before;
+// small: 64 x 64 tiles instead of 128 x 128.
 int bsoi_row_bands(int N);
 cudaError_t launch_bsoi_persistent(double* A, long long ld, double* carry0, double* carry1,
                                    long long ldc, const double* G, int n, int L, int* done,
-                                   int* next, int* err, cudaStream_t st);
+                                   int* next, int* err, bool small, cudaStream_t st);
 
 cudaError_t launch_trtri_blocks(double* A, long long ld, int n, long long bstride,
                                 int nblk, int* info, cudaStream_t st);

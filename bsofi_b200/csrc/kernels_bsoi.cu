@@ -104,34 +104,36 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) bsoi_persistent_kernel(BsoiAr
   }
 }
 
-int bsoi_row_bands(int N) { return (N + CfgM::BM - 1) / CfgM::BM; }
+// Row bands of the smallest tile height (sizes the done counters for every
+// tile configuration).
+int bsoi_row_bands(int N) { return (N + CfgS::BM - 1) / CfgS::BM; }
 
-template <bool AL>
+template <class Cfg, bool AL>
 static cudaError_t launch_al(const BsoiArgs& s, cudaStream_t st) {
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(bsoi_persistent_kernel<CfgM, AL>,
+    cudaError_t e = cudaFuncSetAttribute(bsoi_persistent_kernel<Cfg, AL>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)CfgM::SMEM);
+                                         (int)Cfg::SMEM);
     if (e != cudaSuccess) return e;
     attr = true;
   }
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bsoi_persistent_kernel<CfgM, AL>,
-                                                CfgM::THREADS, CfgM::SMEM);
-  const int RT = bsoi_row_bands(s.N), CT = (2 * s.n + CfgM::BN - 1) / CfgM::BN;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bsoi_persistent_kernel<Cfg, AL>,
+                                                Cfg::THREADS, Cfg::SMEM);
+  const int RT = (s.N + Cfg::BM - 1) / Cfg::BM, CT = (2 * s.n + Cfg::BN - 1) / Cfg::BN;
   long long tiles = (long long)(s.L - 1) * RT * CT;
   int grid = sms * (per > 0 ? per : 1);
   if (tiles < grid) grid = (int)tiles;
-  bsoi_persistent_kernel<CfgM, AL><<<grid, CfgM::THREADS, CfgM::SMEM, st>>>(s);
+  bsoi_persistent_kernel<Cfg, AL><<<grid, Cfg::THREADS, Cfg::SMEM, st>>>(s);
   return cudaGetLastError();
 }
 
 cudaError_t launch_bsoi_persistent(double* A, long long ld, double* carry0, double* carry1,
                                    long long ldc, const double* G, int n, int L, int* done,
-                                   int* next, int* err, cudaStream_t st) {
+                                   int* next, int* err, bool small, cudaStream_t st) {
   BsoiArgs s;
   s.A = A;
   s.ld = ld;
@@ -149,7 +151,8 @@ cudaError_t launch_bsoi_persistent(double* A, long long ld, double* carry0, doub
   const bool al = ((uintptr_t)A % 16 == 0) && ((uintptr_t)carry0 % 16 == 0) &&
                   ((uintptr_t)carry1 % 16 == 0) && ((uintptr_t)G % 16 == 0) && ld % 2 == 0 &&
                   ldc % 2 == 0 && n % 2 == 0;
-  return al ? launch_al<true>(s, st) : launch_al<false>(s, st);
+  if (small) return al ? launch_al<CfgS, true>(s, st) : launch_al<CfgS, false>(s, st);
+  return al ? launch_al<CfgM, true>(s, st) : launch_al<CfgM, false>(s, st);
 }
 
 }  // namespace bsofi

@@ -42,9 +42,10 @@ struct GemmTimer {
 };
 thread_local GemmTimer g_timer;
 
-// Launch plan of one problem size: how BSOI runs (0: one persistent launch;
-// 1: one GEMM launch per step with the tile shape chosen by tile count; 2, 3,
-// 4: per step with 64x64, 128x128 K32, 128x128 K16 tiles), the BSTRI
+// Launch plan of one problem size: how BSOI runs (0 / 5: one persistent
+// launch of 128x128 / 64x64 tiles; 1: one GEMM launch per step with the tile
+// shape chosen by tile count; 2, 3, 4: per step with 64x64, 128x128 K32,
+// 128x128 K16 tiles), the BSTRI
 // row recurrence (launch_gemm's cfg per step, or 4: one persistent launch)
 // and the number
 // of BSOF worker CTAs of a single inversion.  Tuned plans (bsofi_autotune)
@@ -56,10 +57,21 @@ std::mutex g_plan_mu;
 std::map<std::pair<int, int>, Plan> g_plans;
 
 Plan default_plan(int n, int L) {
-  // The persistent BSOI kernel pays off once a step fills every SM with
-  // 128 x 128 tiles; below that, per-step launches of smaller tiles win.
-  const int tiles = bsoi_row_bands(n * L) * ((2 * n + 127) / 128);
-  return Plan{tiles >= 148 ? 0 : 1, 2, 32};
+  // From autotuned sizes (n, p): 128 x 128 tiles pay off when 2n is a
+  // multiple of 128 and a step fills the GPU (256, 32: persistent); otherwise
+  // 64 x 64 tiles waste less of the 2n columns: one persistent launch for
+  // mid-size N (100/64, 196/40, 324/40), per-step launches for N of 20k and
+  // more (400/64, 576/80) and for small N (64/16, 144/20).  The persistent
+  // recurrence helped at 64/16 and 400/64 and tied elsewhere.
+  const int N = n * L;
+  const int tiles = ((N + 127) / 128) * ((2 * n + 127) / 128);
+  int bsoi;
+  if ((2 * n) % 128 == 0 && tiles >= 148) bsoi = 0;
+  else if (N >= 20000) bsoi = 2;
+  else if (N >= 4000) bsoi = 5;
+  else bsoi = 1;
+  const int rec = (N <= 2048 || (N >= 20000 && N < 40000)) ? 4 : 2;
+  return Plan{bsoi, rec, 32};
 }
 
 Plan plan_for(int n, int L) {
@@ -432,13 +444,13 @@ int run_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* ws, cu
   int e = bsoi_carry(n, L, dA, ldd, ws, st);
   if (e) return e;
   const Plan plan = plan_for(n, L);
-  if (plan.bsoi == 0) {
+  if (plan.bsoi == 0 || plan.bsoi == 5) {
     // One persistent launch over all steps (rows flow from step to step).
     int* bs = at<int>(ws, ly.bsync);
     CKM(cudaMemsetAsync(bs, 0, sizeof(int) * ly.bsync_ints, st));
     if (g_timer.on) CKM(g_timer.mark(st));
     CK(launch_bsoi_persistent(dA, ldd, C[0], C[1], ldd, G, n, L, bs, bs + ly.bsync_ints - 2,
-                              at<int>(ws, ly.info) + 2, st));
+                              at<int>(ws, ly.info) + 2, plan.bsoi == 5, st));
     if (g_timer.on) CKM(g_timer.mark(st));
   } else {
     // One launch per step (small problems: more, smaller tiles per step).
@@ -541,7 +553,7 @@ int bsofi_dev_plan_get(int n, int L, int* plan) {
 }
 
 int bsofi_dev_plan_set(int n, int L, const int* plan) {
-  if (n < 1 || L < 2 || plan[0] < 0 || plan[0] > 4 || plan[1] < 0 || plan[1] > 4 ||
+  if (n < 1 || L < 2 || plan[0] < 0 || plan[0] > 5 || plan[1] < 0 || plan[1] > 4 ||
       plan[2] < 1 || plan[2] > 1024)
     return -1;
   std::lock_guard<std::mutex> lk(g_plan_mu);

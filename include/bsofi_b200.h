@@ -226,7 +226,8 @@ int bsofi_batch_graph_launch(bsofi_batch_graph *graph, void *stream);
 void bsofi_batch_graph_destroy(bsofi_batch_graph *graph);
 
 /* Launch plans and the autotuner (no reference counterpart).  A plan is
- * four ints: [0] BSOI form (0 one persistent launch over all steps; 1 one
+ * four ints: [0] BSOI form (0 / 5 one persistent launch over all steps with
+ * 128x128 / 64x64 tiles; 1 one
  * GEMM launch per step, tile shape by tile count; 2 / 3 / 4 per step with
  * 64x64 / 128x128 with 32-deep K stages / 128x128 with 16-deep K stages),
  * [1] the BSTRI row recurrence (one GEMM launch per step with tiles 0 by
@@ -234,9 +235,8 @@ void bsofi_batch_graph_destroy(bsofi_batch_graph *graph);
  * launch of 64x64 tiles pipelined across the steps), [2] BSOF worker CTAs of
  * a single inversion, [3] reserved (0).
  * Every inversion of block size n with L blocks uses the tuned plan of (n, L)
- * if there is one, else a default (persistent BSOI when a step has at least
- * 148 tiles of 128 x 128, per-step otherwise; 64x64 recurrence tiles; 32
- * workers).  bsofi_autotune times the candidates one knob at a time on a
+ * if there is one, else a default fitted to the sizes tuned on a B200
+ * (bsofi_plan_get shows it).  bsofi_autotune times the candidates one knob at a time on a
  * synthetic matrix of that size (reps timed runs each, fastest kept; it
  * allocates its own buffers) on `stream`, stores the winner and copies it to
  * plan_out (may be NULL); it returns 0, -1 for an illegal size or

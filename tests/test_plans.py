@@ -11,11 +11,15 @@ def _clear_plans():
     api.plan_clear()
 
 
-def test_default_plan_follows_bsoi_tile_count():
-    # n = 256, L = 32: 64 row bands x 4 column tiles per step -> persistent BSOI.
+def test_default_plan_follows_the_tuned_sizes():
+    # 2n = 512 fills 128-wide tiles and 256 tiles per step: persistent 128x128.
     assert api.plan_get(256, 32) == (False, [0, 2, 32, 0])
-    # n = 144, L = 20: 23 x 3 tiles per step -> one GEMM launch per step.
+    # Small N: one GEMM launch per step; persistent recurrence for N <= 2048.
     assert api.plan_get(144, 20) == (False, [1, 2, 32, 0])
+    assert api.plan_get(64, 16) == (False, [1, 4, 32, 0])
+    # 2n = 392: 64x64 tiles, persistent for mid-size N, per step for N >= 20k.
+    assert api.plan_get(196, 40) == (False, [5, 2, 32, 0])
+    assert api.plan_get(400, 64) == (False, [2, 4, 32, 0])
 
 
 def test_set_get_clear_roundtrip():
@@ -26,7 +30,7 @@ def test_set_get_clear_roundtrip():
     assert api.plan_get(100, 8)[0] is False
 
 
-@pytest.mark.parametrize("plan", [[5, 2, 32, 0], [-1, 2, 32, 0], [0, 5, 32, 0], [0, 2, 0, 0]])
+@pytest.mark.parametrize("plan", [[6, 2, 32, 0], [-1, 2, 32, 0], [0, 5, 32, 0], [0, 2, 0, 0]])
 def test_invalid_plans_rejected(plan):
     assert api.plan_set(64, 4, plan) == -1
     assert api.plan_get(64, 4)[0] is False
