@@ -54,6 +54,16 @@ BSOFI_DEVINL void dmma_16x8x8(double (&d)[4], double a0, double a1, double a2, d
       : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
 }
 
+// D = A(8x4, row) * B(4x8, col) + D, FP64.  a0 = A[g][t]; b0 = B[t][g];
+// d0, d1 = D[g][2t], D[g][2t+1].
+BSOFI_DEVINL void dmma_8x8x4(double (&d)[2], double a0, double b0) {
+  asm volatile(
+      "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 "
+      "{%0,%1}, {%2}, {%3}, {%0,%1};\n"
+      : "+d"(d[0]), "+d"(d[1])
+      : "d"(a0), "d"(b0));
+}
+
 // ---------------------------------------------------------------- warp sums
 BSOFI_DEVINL double warp_sum(double v) {
 #pragma unroll

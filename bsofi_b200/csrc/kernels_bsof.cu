@@ -256,30 +256,6 @@ struct Smem {
   int pflag;  // next-tile prefetch of the panel CTA succeeded
 };
 
-// Load rows [row0 + r] (thread-owned rows r = tid + BT*i) of NB columns.
-template <int R, int NB>
-BSOFI_DEVINL void load_rows(double (&a)[R][NB], const double* P, long long ld, int m, int w) {
-#pragma unroll
-  for (int i = 0; i < R; i++) {
-    const int r = threadIdx.x + BT * i;
-#pragma unroll
-    for (int c = 0; c < NB; c++) a[i][c] = (r < m && c < w) ? __ldcg(P + cm(r, c, ld)) : 0.0;
-  }
-}
-
-template <int R, int NB>
-BSOFI_DEVINL void store_rows(const double (&a)[R][NB], double* P, long long ld, int m, int w) {
-#pragma unroll
-  for (int i = 0; i < R; i++) {
-    const int r = threadIdx.x + BT * i;
-    if (r < m) {
-#pragma unroll
-      for (int c = 0; c < NB; c++)
-        if (c < w) __stcg(P + cm(r, c, ld), a[i][c]);
-    }
-  }
-}
-
 // T(0:I, I) = -tau_I T(0:I,0:I) g_I (LAPACK dlarft), run by one warp one
 // column behind the factorization; T and g are zero outside their ranges.
 template <int NB>
@@ -423,71 +399,6 @@ BSOFI_DEVINL void factor_leaf(double (&a)[R][NB], Smem<NB>& sm, int m, int w, do
       a[i][NB - 1] = t0;
     }
   }
-}
-
-// C <- (I - V T V^T)^T C on the tile at C (m rows, w columns, thread-owned
-// rows); v holds the reflectors with the unit diagonal and the zeros above it
-// materialised, T is in sm.T.  C columns are streamed from L2 twice (for
-// W = V^T C and for C -= V (T^T W)) so that only V stays in registers.
-template <int R, int NB>
-BSOFI_DEVINL void apply_qt(const double (&v)[R][NB], double* C, long long ld, int m, int w,
-                           Smem<NB>& sm, double* sC) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  constexpr int SH = (NB == 16) ? 1 : 2;
-  constexpr int MP = R * BT;  // row stride of the staged tile
-  // Stage the thread's own rows of C (all loads in flight at once).
-#pragma unroll
-  for (int i = 0; i < R; i++) {
-    const int r = tid + BT * i;
-#pragma unroll
-    for (int cc = 0; cc < NB; cc++)
-      sC[cc * MP + r] = (r < m && cc < w) ? __ldcg(C + cm(r, cc, ld)) : 0.0;
-  }
-#pragma unroll 1
-  for (int cc = 0; cc < NB; cc++) {
-    double part[NB];
-#pragma unroll
-    for (int a = 0; a < NB; a++) {
-      double t = 0.0;
-#pragma unroll
-      for (int i = 0; i < R; i++) t = fma(v[i][a], sC[cc * MP + tid + BT * i], t);
-      part[a] = t;
-    }
-    double sum = wsum_t<NB>(part, lane);
-    if ((lane & ((1 << SH) - 1)) == 0) sm.redW[warp][cc][(lane >> SH) & (NB - 1)] = sum;
-  }
-  __syncthreads();
-  for (int e = tid; e < NB * NB; e += BT) {
-    const int a = e % NB, cc = e / NB;
-    double acc = 0.0;
-#pragma unroll
-    for (int k = 0; k < BW; k++) acc += sm.redW[k][cc][a];
-    sm.W[a][cc] = acc;
-  }
-  __syncthreads();
-  for (int e = tid; e < NB * NB; e += BT) {
-    const int a = e % NB, cc = e / NB;
-    double acc = 0.0;
-    for (int b = 0; b <= a; b++) acc = fma(sm.T[b][a], sm.W[b][cc], acc);
-    sm.redW[0][cc][a] = acc;
-  }
-  __syncthreads();
-#pragma unroll 1
-  for (int cc = 0; cc < w; cc++) {
-    {
-#pragma unroll
-      for (int i = 0; i < R; i++) {
-        const int r = tid + BT * i;
-        if (r < m) {
-          double acc = 0.0;
-#pragma unroll
-          for (int a = 0; a < NB; a++) acc = fma(v[i][a], sm.redW[0][cc][a], acc);
-          __stcg(C + cm(r, cc, ld), sC[cc * MP + r] - acc);
-        }
-      }
-    }
-  }
-  __syncthreads();
 }
 
 // 16-wide block reflector applied with DMMA (mma.sync m16n8k4 f64):
@@ -664,16 +575,80 @@ BSOFI_DEVINL void apply_qt_mma(double* sV, double* sC, const double (&a)[R][16],
   }
 }
 
-// Materialise the unit lower trapezoidal V of a factored leaf held in a.
-template <int R, int NB>
-BSOFI_DEVINL void leaf_to_v(const double (&a)[R][NB], double (&v)[R][NB], int m, int w) {
+// 8-wide block reflector with DMMA m8n8k4 (f64), all rows in one pass:
+//   W = V^T C (8 x 8; K = the leaf's rows, split over the 8 warps),
+//   W <- -T^T W,  C <- C + V W  (rows split over the warps).
+// V and C are staged column-major with column stride S8 = R*BT + 4 (4 mod 16
+// doubles): the staging writes (one row per thread) and the fragment loads of
+// both products are free of bank conflicts.  VREG: V comes from the factoring
+// CTA's registers (thread t owns rows t + BT*i), else from the stored leaf.
+// wv: width of the leaf, w: width of the target tile.
+template <int R>
+struct Stage8 {
+  static constexpr int S8 = R * BT + 4;
+};
+
+template <int R, bool VREG>
+BSOFI_DEVINL void apply_qt_mma8(double* sV, double* sC, const double (&a)[R][8],
+                                const double* P, long long ldp, int wv, double* C, long long ld,
+                                int m, int w, Smem<8>& sm) {
+  constexpr int S8 = Stage8<R>::S8, KW = R * BT / BW;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
 #pragma unroll
   for (int i = 0; i < R; i++) {
-    const int r = threadIdx.x + BT * i;
+    const int r = tid + BT * i;
 #pragma unroll
-    for (int c = 0; c < NB; c++)
-      v[i][c] = (c >= w || r >= m) ? 0.0 : (r == c ? 1.0 : (r > c ? a[i][c] : 0.0));
+    for (int c = 0; c < 8; c++) {
+      double v = 0.0;
+      if (r < m && c < wv) {
+        if (r == c) v = 1.0;
+        else if (r > c) v = VREG ? a[i][c] : __ldcg(P + cm(r, c, ldp));
+      }
+      sV[c * S8 + r] = v;
+      sC[c * S8 + r] = (r < m && c < w) ? __ldcg(C + cm(r, c, ld)) : 0.0;
+    }
   }
+  __syncthreads();
+  {
+    double acc[2] = {0.0, 0.0};
+    const int k1 = warp * KW;
+#pragma unroll 4
+    for (int k0 = k1; k0 < k1 + KW; k0 += 4)
+      dmma_8x8x4(acc, sV[g * S8 + k0 + t], sC[g * S8 + k0 + t]);
+    sm.redW[warp][g][2 * t] = acc[0];
+    sm.redW[warp][g][2 * t + 1] = acc[1];
+  }
+  __syncthreads();
+  if (tid < 64) {
+    const int ai = tid & 7, cc = tid >> 3;
+    double s2 = 0.0;
+#pragma unroll
+    for (int k = 0; k < BW; k++) s2 += sm.redW[k][ai][cc];
+    sm.W[ai][cc] = s2;
+  }
+  __syncthreads();
+  if (tid < 64) {  // -(T^T W); T is zero below its diagonal
+    const int ai = tid & 7, cc = tid >> 3;
+    double s2 = 0.0;
+#pragma unroll
+    for (int b = 0; b < 8; b++) s2 = fma(sm.T[b][ai], sm.W[b][cc], s2);
+    sm.redW[0][ai][cc] = -s2;
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (int m0 = warp * KW; m0 < (warp + 1) * KW; m0 += 8) {
+    double d[2] = {sC[(2 * t) * S8 + m0 + g], sC[(2 * t + 1) * S8 + m0 + g]};
+#pragma unroll
+    for (int k0 = 0; k0 < 8; k0 += 4)
+      dmma_8x8x4(d, sV[(k0 + t) * S8 + m0 + g], sm.redW[0][k0 + t][g]);
+    const int rr = m0 + g;
+    if (rr < m) {
+      if (2 * t < w) __stcg(C + cm(rr, 2 * t, ld), d[0]);
+      if (2 * t + 1 < w) __stcg(C + cm(rr, 2 * t + 1, ld), d[1]);
+    }
+  }
+  __syncthreads();
 }
 
 template <int R, int NB>
@@ -796,9 +771,8 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
           apply_qt_mma<R, false, Pass<R>::NP == 1, PREFETCH>(
               sC, sC + Pass<R>::ROWS * MS, none, P, st.ld, f.w, C, ldc, mrows, w2, sm);
         } else {
-          double v[R][NB];
-          leaf_to_v<R, NB>(a, v, mrows, f.w);
-          apply_qt<R, NB>(v, C, ldc, mrows, w2, sm, sC);
+          apply_qt_mma8<R, true>(sC, sC + 8 * Stage8<R>::S8, a, P, st.ld, f.w, C, ldc, mrows, w2,
+                                 sm);
         }
       }
       if (tid == 0) {
@@ -847,14 +821,10 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
       apply_qt_mma<R, false>(sC, sC + Pass<R>::ROWS * MS, none, P, st.ld, f.w, C, ldc, mrows, w2,
                              sm);
     } else {
-      double v[R][NB];
-      {
-        double a[R][NB];
-        load_rows<R, NB>(a, P, st.ld, mrows, f.w);
-        leaf_to_v<R, NB>(a, v, mrows, f.w);
-      }
       if (!block_wait_geq(st, st.cnt + x2, s - lo2, &sm.flag)) return;
-      apply_qt<R, NB>(v, C, ldc, mrows, w2, sm, sC);
+      double none[R][8];
+      apply_qt_mma8<R, false>(sC, sC + 8 * Stage8<R>::S8, none, P, st.ld, f.w, C, ldc, mrows, w2,
+                              sm);
     }
     if (tid == 0) {
       __threadfence();
@@ -875,7 +845,7 @@ int bsof_tiles(int n) { return (n + bsof_leaf_width(n) - 1) / bsof_leaf_width(n)
 template <int R, int NB>
 static size_t dyn_smem() {
   return NB == 16 ? sizeof(double) * 2 * (size_t)Pass<R>::ROWS * MS
-                  : sizeof(double) * (size_t)NB * R * BT;
+                  : sizeof(double) * 2 * 8 * (size_t)Stage8<R>::S8;
 }
 
 template <int R, int NB>
