@@ -52,7 +52,7 @@ def parse():
     p.add_argument("--L", type=int, default=32)
     p.add_argument("--U", type=float, default=4.0)
     p.add_argument("--e2e-steps", type=int, default=5)
-    p.add_argument("--cpu-sample", type=int, default=2, help="reference inversions in cpu_baseline")
+    p.add_argument("--cpu-sample", type=int, default=10, help="reference inversions in cpu_baseline")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--batch", type=int, default=16,
