@@ -1,12 +1,16 @@
 """Diagnostics of the device pipeline through the C ABI.
 
     python -m bsofi_b200.diag bsof-timeline N_BLOCK L [REPS]
+    python -m bsofi_b200.diag invert N_BLOCK L [REPS] [U]
 
-inverts a seeded Hubbard matrix (a random p-cyclic one when n is not a square)
-with bsofi_device_invert and prints, for the last run, the BSOF chain length
-and the per-leaf phases recorded by the persistent BSOF kernel's critical CTA
-(bsofi_device_bsof_timeline: globaltimer stamps at loop start, tile ready,
-next-tile update start and leaf published).
+bsof-timeline inverts a seeded Hubbard matrix (a random p-cyclic one when n is
+not a square) with bsofi_device_invert and prints, for the last run, the BSOF
+chain length and the per-leaf phases recorded by the persistent BSOF kernel's
+critical CTA (bsofi_device_bsof_timeline: globaltimer stamps at loop start,
+tile ready, next-tile update start and leaf published).  invert times REPS
+device-resident inversions of the Hubbard matrix (U = 4 unless given) with the
+size's launch plan and prints the fastest with its TFLOP/s, the BSOI time
+(CUDA events around its launches) and the BSOF chain.
 """
 import sys
 
@@ -66,6 +70,48 @@ def bsof_timeline(n, L, reps=3):
     return out
 
 
+def invert_timing(n, L, reps=3, U=4.0):
+    import torch
+    from .flops import bsofi_flops, flops_bsoi
+    side = int(round(n ** 0.5))
+    N = n * L
+    ldd = (N + 31) // 32 * 32
+    M = hubbard_matrix(side, L, U, seed=1) if side * side == n else random_pcyclic(n, L, seed=1)
+    dev = torch.device("cuda:0")
+    src = torch.zeros((N, ldd), dtype=torch.float64, device=dev)
+    src[:, :N] = torch.from_numpy(np.ascontiguousarray(M.T)).to(dev)
+    del M
+    dA = torch.empty_like(src)
+    dtau = torch.zeros(N, dtype=torch.float64, device=dev)
+    ws = torch.empty(api.workspace_bytes(n, L, ldd), dtype=torch.uint8, device=dev)
+    best, bsoi = float("inf"), float("inf")
+    stream = torch.cuda.current_stream()
+    for r in range(reps + 1):  # the first run is a warm-up
+        dA.copy_(src)
+        api.timing(True)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rc = api.device_invert(n, L, dA.data_ptr(), ldd, dtau.data_ptr(), ws.data_ptr(),
+                               stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms, _ = api.timing_read()
+        api.timing(False)
+        if rc != 0:
+            raise RuntimeError("bsofi_device_invert failed (%d)" % rc)
+        if r > 0:
+            best = min(best, e0.elapsed_time(e1))
+            bsoi = min(bsoi, ms)
+    S = bsof_leaves(n, L)
+    buf = np.zeros(4 * S, dtype=np.uint64)
+    _lib.load().bsofi_device_bsof_timeline(n, L, ldd, ws.data_ptr(), buf.ctypes.data, S)
+    t = buf.reshape(S, 4).astype(np.int64)
+    return {"invert_ms": best, "tflops": bsofi_flops(n, L) / best / 1e9, "bsoi_ms": bsoi,
+            "bsoi_tflops": flops_bsoi(n, L) / bsoi / 1e9, "chain_ms": (t[-1, 2] - t[0, 0]) / 1e6,
+            "plan": api.plan_get(n, L)}
+
+
 def main(argv):
     if len(argv) >= 3 and argv[0] == "bsof-timeline":
         n, L = int(argv[1]), int(argv[2])
@@ -76,6 +122,15 @@ def main(argv):
         print("per leaf: wait for tile %.2f us, factor (tile ready -> next-tile update) %.2f us, "
               "next-tile update + publish %.2f us, publish -> next leaf %.2f us" %
               (r["wait_tile_us"], r["factor_us"], r["update_publish_us"], r["to_next_leaf_us"]))
+        return 0
+    if len(argv) >= 3 and argv[0] == "invert":
+        n, L = int(argv[1]), int(argv[2])
+        reps = int(argv[3]) if len(argv) > 3 else 3
+        U = float(argv[4]) if len(argv) > 4 else 4.0
+        r = invert_timing(n, L, reps, U)
+        print("n %d L %d (plan %s): invert %.3f ms = %.2f TFLOP/s of the flop model; BSOI %.3f ms "
+              "= %.2f TFLOP/s; BSOF chain %.3f ms" % (n, L, r["plan"], r["invert_ms"], r["tflops"],
+                                                      r["bsoi_ms"], r["bsoi_tflops"], r["chain_ms"]))
         return 0
     print(__doc__)
     return 2
