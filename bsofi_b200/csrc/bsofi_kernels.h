@@ -5,6 +5,24 @@
 
 namespace bsofi {
 
+// Kernel attributes (cudaFuncSetAttribute) apply to the current device only:
+// set-up that is done once is done once per device.  Devices beyond the table
+// redo it every time (harmless: the call is idempotent).
+constexpr int kMaxDevices = 64;
+struct PerDevice {
+  bool done[kMaxDevices] = {};
+  // Device index whose set-up is still to do, or -1 if it is done.
+  int pending() const {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (dev < 0 || dev >= kMaxDevices) return dev;
+    return done[dev] ? -1 : dev;
+  }
+  void mark(int dev) {
+    if (dev >= 0 && dev < kMaxDevices) done[dev] = true;
+  }
+};
+
 struct WySeg {
   double* p;
   long long ld, bs;
@@ -48,8 +66,10 @@ cudaError_t launch_bsoi_persistent(double* A, long long ld, double* carry0, doub
                                    long long ldc, const double* G, int n, int L, int* done,
                                    int* next, int* err, bool small, cudaStream_t st);
 
+// In-place inversion of the upper triangles of nblk n x n blocks (block b at
+// A + b * bstride); tmp: device scratch of nblk * n * n / 4 doubles.
 cudaError_t launch_trtri_blocks(double* A, long long ld, int n, long long bstride,
-                                int nblk, int* info, cudaStream_t st);
+                                int nblk, int* info, double* tmp, cudaStream_t st);
 
 // cfg: 0 = choose by tile count, 1 = 128x128 (K stage 16), 2 = 64x64, 3 = 128x128 (K stage 32).
 cudaError_t launch_gemm(const GemmDims& d, const GemmA& a, const GemmB& b,

@@ -110,13 +110,14 @@ int bsoi_row_bands(int N) { return (N + CfgS::BM - 1) / CfgS::BM; }
 
 template <class Cfg, bool AL>
 static cudaError_t launch_al(const BsoiArgs& s, cudaStream_t st) {
-  static bool attr = false;
-  if (!attr) {
+  static PerDevice once;
+  const int pend = once.pending();
+  if (pend >= 0) {
     cudaError_t e = cudaFuncSetAttribute(bsoi_persistent_kernel<Cfg, AL>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)Cfg::SMEM);
     if (e != cudaSuccess) return e;
-    attr = true;
+    once.mark(pend);
   }
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);

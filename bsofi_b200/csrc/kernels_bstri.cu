@@ -122,13 +122,14 @@ int bstri_recurrence_ctmax(int n, int L) { return ((L - 1) * n + CfgS::BN - 1) /
 
 template <bool AL>
 static cudaError_t rec_launch(const RecArgs& s, long long tiles, cudaStream_t st) {
-  static bool attr = false;
-  if (!attr) {
+  static PerDevice once;
+  const int pend = once.pending();
+  if (pend >= 0) {
     cudaError_t e = cudaFuncSetAttribute(bstri_recurrence_kernel<CfgS, AL>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)CfgS::SMEM);
     if (e != cudaSuccess) return e;
-    attr = true;
+    once.mark(pend);
   }
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);

@@ -18,8 +18,9 @@ static cudaError_t set_attr() {
 }
 
 cudaError_t gemm_init_attributes() {
-  static bool done = false;
-  if (done) return cudaSuccess;
+  static PerDevice once;
+  const int dev = once.pending();
+  if (dev < 0) return cudaSuccess;
   cudaError_t e;
   if ((e = set_attr<CfgL, true>()) != cudaSuccess) return e;
   if ((e = set_attr<CfgL, false>()) != cudaSuccess) return e;
@@ -27,7 +28,7 @@ cudaError_t gemm_init_attributes() {
   if ((e = set_attr<CfgM, false>()) != cudaSuccess) return e;
   if ((e = set_attr<CfgS, true>()) != cudaSuccess) return e;
   if ((e = set_attr<CfgS, false>()) != cudaSuccess) return e;
-  done = true;
+  once.mark(dev);
   return cudaSuccess;
 }
 

@@ -3,117 +3,140 @@
 //
 // Reference: lapackXbstri, src/bsofi_cpu.c:146-177 (dtrtri of the 3n corner
 // and of each n x n diagonal block).  The diagonal blocks are independent of
-// the block recurrence, so all of them are inverted in one launch (one CTA
-// per block), in place in the upper triangle; the strict lower part, which
-// holds Householder vectors, is never touched (as with LAPACK dtrtri).
+// the block recurrence, so all of them are inverted together, in place in the
+// upper triangle; the strict lower part, which holds Householder vectors, is
+// never touched (as with LAPACK dtrtri).
 #include <climits>
+#include <vector>
 #include "bsofi_common.cuh"
 #include "bsofi_kernels.h"
 
 namespace bsofi {
 
-constexpr int TB = 32;
+// Recursive inversion of the upper-triangular diagonal blocks, in place:
+//   inv([U11 U12; 0 U22]) = [X11, -X11 U12 X22; 0, X22],  X = inv(U),
+// split at a multiple of 32 near the middle down to leaves of at most 32
+// columns.  Every leaf of every block is independent (one warp each, the
+// column loop of LAPACK dtrti2 in shared memory); then, bottom-up, each split
+// is two GEMMs batched over the blocks on the FP64 DMMA tile engine (the
+// triangular factors are masked operands): T = U12 X22, X12 = -X11 T.
+constexpr int TLEAF = 32;
 
-// Inverts the upper-triangular n x n block at A + blockIdx.x * bstride.
-// Column blocks of width 32, left to right (LAPACK dtrtri 'U' order):
-//   D = U_jj^{-1} (in shared memory),
-//   U(0:j, j) <- -X(0:j,0:j) U(0:j, j) D   with X = U(0:j,0:j)^{-1} already
-//   in place; row chunks are produced top-down so the in-place update only
-//   overwrites rows that later chunks no longer read.
-// An exactly zero diagonal entry leaves the block untouched and records the
-// smallest 1-based global index (block * n + i + 1) in *info.
-__global__ void __launch_bounds__(256) trtri_blocks_kernel(double* A, long long ld, int n,
-                                                           long long bstride, int* info) {
-  __shared__ double sD[TB][TB + 1];
-  __shared__ double sX[TB][TB + 1];
-  __shared__ double sY[TB][TB + 1];
-  __shared__ double sS[TB][TB + 1];
-  __shared__ int sbad;
-  const int tid = threadIdx.x;
-  double* U = A + (long long)blockIdx.x * bstride;
-
-  if (tid == 0) sbad = INT_MAX;
-  __syncthreads();
-  for (int i = tid; i < n; i += blockDim.x)
-    if (U[cm(i, i, ld)] == 0.0) atomicMin(&sbad, i);
-  __syncthreads();
-  if (sbad != INT_MAX) {
-    if (tid == 0) atomicMin(info, blockIdx.x * n + sbad + 1);
+// One warp inverts one leaf (rows/columns [32 l, 32 l + w) of block b).  An
+// exactly zero diagonal entry leaves the leaf as it is and records the
+// smallest 1-based global index (block * n + i + 1) in *info; the block's
+// inverse is then not formed.
+__global__ void __launch_bounds__(128) trtri_leaves_kernel(double* A, long long ld, int n,
+                                                           long long bstride, int nblk, int* info) {
+  __shared__ double sU[4][TLEAF][TLEAF + 1];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nleaf = (n + TLEAF - 1) / TLEAF;
+  const long long gw = (long long)blockIdx.x * 4 + warp;
+  if (gw >= (long long)nblk * nleaf) return;  // whole warps only: no block barrier below
+  const int b = (int)(gw / nleaf), o = (int)(gw % nleaf) * TLEAF;
+  const int w = min(TLEAF, n - o);
+  double* U = A + (long long)b * bstride + cm(o, o, ld);
+  double(*X)[TLEAF + 1] = sU[warp];
+  for (int c = 0; c < TLEAF; c++)
+    X[lane][c] = (lane <= c && c < w) ? U[cm(lane, c, ld)] : 0.0;
+  __syncwarp();
+  const unsigned zero = __ballot_sync(0xffffffffu, lane < w && X[lane][lane] == 0.0);
+  if (zero != 0u) {
+    if (lane == __ffs(zero) - 1) atomicMin(info, b * n + o + lane + 1);
     return;
   }
-
-  const int tr = tid % TB, tc = tid / TB;  // tc in 0..7
-  for (int jb = 0; jb < n; jb += TB) {
-    const int w = min(TB, n - jb);
-    // Diagonal block, upper part.
-    for (int e = tid; e < TB * TB; e += blockDim.x) {
-      int r = e % TB, c = e / TB;
-      sD[r][c] = (r <= c && r < w && c < w) ? U[cm(jb + r, jb + c, ld)] : 0.0;
-    }
-    __syncthreads();
-    // dtrti2 on sD by warp 0: column j: d = 1/D_jj; D(0:j,j) = -d triu(D(0:j,0:j)) D(0:j,j).
-    if (tid < 32) {
-      for (int j = 0; j < w; j++) {
-        double djj = 1.0 / sD[j][j];
-        double s = 0.0;
-        if (tid < j)
-          for (int k = tid; k < j; k++) s = fma(sD[tid][k], sD[k][j], s);
-        __syncwarp();
-        if (tid < j) sD[tid][j] = -djj * s;
-        if (tid == j) sD[j][j] = djj;
-        __syncwarp();
-      }
-    }
-    __syncthreads();
-    // Off-diagonal column block rows 0..jb.
-    for (int r0 = 0; r0 < jb; r0 += TB) {
-      const int h = min(TB, jb - r0);
-      double acc[4] = {0.0, 0.0, 0.0, 0.0};
-      for (int k0 = r0; k0 < jb; k0 += TB) {
-        const int kw = min(TB, jb - k0);
-        __syncthreads();
-        for (int e = tid; e < TB * TB; e += blockDim.x) {
-          int r = e % TB, c = e / TB;
-          // X(r0+r, k0+c), upper triangular.
-          sX[r][c] = (r < h && c < kw && r0 + r <= k0 + c) ? U[cm(r0 + r, k0 + c, ld)] : 0.0;
-          // top(k0+r, c) = U(k0+r, jb+c)
-          sY[r][c] = (r < kw && c < w) ? U[cm(k0 + r, jb + c, ld)] : 0.0;
-        }
-        __syncthreads();
-#pragma unroll 8
-        for (int k = 0; k < TB; k++) {
-          double x = sX[tr][k];
-#pragma unroll
-          for (int q = 0; q < 4; q++) acc[q] = fma(x, sY[k][tc + 8 * q], acc[q]);
-        }
-      }
-      __syncthreads();
-#pragma unroll
-      for (int q = 0; q < 4; q++) sS[tr][tc + 8 * q] = acc[q];
-      __syncthreads();
-      // out = -S D
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const int c = tc + 8 * q;
-        double s = 0.0;
-        for (int k = 0; k <= c; k++) s = fma(sS[tr][k], sD[k][c], s);
-        if (tr < h && c < w) U[cm(r0 + tr, jb + c, ld)] = -s;
-      }
-    }
-    __syncthreads();
-    for (int e = tid; e < TB * TB; e += blockDim.x) {
-      int r = e % TB, c = e / TB;
-      if (r <= c && c < w) U[cm(jb + r, jb + c, ld)] = sD[r][c];
-    }
-    __syncthreads();
+  // dtrti2 ('U'): X(j,j) = 1/U(j,j), X(0:j,j) = -X(j,j) X(0:j,0:j) U(0:j,j).
+  for (int j = 0; j < w; j++) {
+    const double xjj = 1.0 / X[j][j];
+    double s = 0.0;
+    if (lane < j)
+      for (int k = lane; k < j; k++) s = fma(X[lane][k], X[k][j], s);
+    __syncwarp();
+    if (lane < j) X[lane][j] = -xjj * s;
+    if (lane == j) X[j][j] = xjj;
+    __syncwarp();
   }
+  for (int c = 0; c < w; c++)
+    if (lane <= c) U[cm(lane, c, ld)] = X[lane][c];
 }
 
+namespace {
+struct TriNode {
+  int off, size, h;
+};
+
+// Splits of an n-column triangle in post order (children before parents).
+void tri_nodes(int off, int size, std::vector<TriNode>& out) {
+  if (size <= TLEAF) return;
+  const int h = TLEAF * ((size + 2 * TLEAF - 1) / (2 * TLEAF));
+  tri_nodes(off, h, out);
+  tri_nodes(off + h, size - h, out);
+  out.push_back({off, size, h});
+}
+}  // namespace
+
 cudaError_t launch_trtri_blocks(double* A, long long ld, int n, long long bstride, int nblk,
-                                int* info, cudaStream_t st) {
-  if (nblk <= 0) return cudaSuccess;
-  trtri_blocks_kernel<<<nblk, 256, 0, st>>>(A, ld, n, bstride, info);
-  return cudaGetLastError();
+                                int* info, double* tmp, cudaStream_t st) {
+  if (nblk <= 0 || n <= 0) return cudaSuccess;
+  const long long leaves = (long long)nblk * ((n + TLEAF - 1) / TLEAF);
+  trtri_leaves_kernel<<<(int)((leaves + 3) / 4), 128, 0, st>>>(A, ld, n, bstride, nblk, info);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  std::vector<TriNode> nodes;
+  tri_nodes(0, n, nodes);
+  for (const TriNode& q : nodes) {
+    const int h = q.h, r = q.size - q.h;
+    double* U12 = A + cm(q.off, q.off + h, ld);
+    const double* X11 = A + cm(q.off, q.off, ld);
+    const double* X22 = A + cm(q.off + h, q.off + h, ld);
+    // T = U12 X22 (X22 upper triangular), T is h x r with leading dimension h.
+    {
+      GemmDims d = {h, r, r};
+      GemmA a = {};
+      a.p0 = U12;
+      a.ld0 = ld;
+      a.bs0 = bstride;
+      a.ld1 = 2;
+      a.ksplit = r;
+      a.rlim0 = INT_MAX;
+      a.roff0 = kNoMask;
+      a.rlim1 = INT_MAX;
+      a.roff1 = kNoMask;
+      GemmB b = {X22, ld, bstride, 0};
+      GemmC c = {};
+      c.p0 = tmp;
+      c.ld0 = h;
+      c.bs0 = (long long)h * r;
+      c.ld1 = 1;
+      c.nsplit = r;
+      c.alpha = 1.0;
+      if ((e = launch_gemm(d, a, b, c, nblk, 0, st)) != cudaSuccess) return e;
+    }
+    // X12 = -X11 T (X11 upper triangular), written over U12.
+    {
+      GemmDims d = {h, r, h};
+      GemmA a = {};
+      a.p0 = X11;
+      a.ld0 = ld;
+      a.bs0 = bstride;
+      a.ld1 = 2;
+      a.ksplit = h;
+      a.rlim0 = INT_MAX;
+      a.roff0 = 0;
+      a.rlim1 = INT_MAX;
+      a.roff1 = kNoMask;
+      GemmB b = {tmp, h, (long long)h * r, kNoMask};
+      GemmC c = {};
+      c.p0 = U12;
+      c.ld0 = ld;
+      c.bs0 = bstride;
+      c.ld1 = 1;
+      c.nsplit = r;
+      c.alpha = -1.0;
+      if ((e = launch_gemm(d, a, b, c, nblk, 0, st)) != cudaSuccess) return e;
+    }
+  }
+  return cudaSuccess;
 }
 
 // ------------------------------------------------------------------ utilities

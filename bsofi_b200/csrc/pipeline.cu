@@ -235,7 +235,8 @@ int run_bstri(int n, int L, double* dA, int ldd, void* ws, cudaStream_t st) {
   const long long nn = (long long)n * n, diag = (long long)n * (ldd + 1);
   CKM(cudaMemsetAsync(info, 0x7f, sizeof(int), st));
   // X_ii = R_ii^{-1} for every diagonal block.
-  CK(launch_trtri_blocks(dA, ldd, n, diag, L, info, st));
+  // (Y, not yet used, is the scratch of the recursive inversion: n^2/4 per block.)
+  CK(launch_trtri_blocks(dA, ldd, n, diag, L, info, Y, st));
   GemmDims d = {n, n, n};
   // Y_i = R_{i,L-1} X_{L-1,L-1},  i = 0..L-2.
   {
