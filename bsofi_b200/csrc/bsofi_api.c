@@ -914,9 +914,17 @@ unsigned long long bsofi_device_workspace_bytes(int n, int L, int ldda) {
   return (unsigned long long)bsofi_dev_ws_bytes(n, L, ldda);
 }
 
+/* Sizes and pointers every device entry point requires. */
+static int device_args_ok(int n, int L, const double *dA, int ldda, const double *dtau,
+                          const void *dwork) {
+  return n >= 1 && n <= BSOFI_MAX_BLOCK && L >= 2 && ldda >= n * L && dA && dtau && dwork;
+}
+
 int bsofi_device_bsoftri(int n, int L, double *dA, int ldda, double *dtau, void *dwork,
                          void *stream) {
-  int e = bsofi_dev_prepare();
+  int e;
+  if (!device_args_ok(n, L, dA, ldda, dtau, dwork)) return -1;
+  e = bsofi_dev_prepare();
   if (e) return cuda_info((cudaError_t)e);
   e = bsofi_dev_bsoftri(n, L, dA, ldda, dtau, dwork, stream);
   return e ? cuda_info((cudaError_t)e) : 0;
@@ -924,7 +932,9 @@ int bsofi_device_bsoftri(int n, int L, double *dA, int ldda, double *dtau, void 
 
 int bsofi_device_bsoi(int n, int L, double *dA, int ldda, const double *dtau, void *dwork,
                       void *stream) {
-  int e = bsofi_dev_prepare();
+  int e;
+  if (!device_args_ok(n, L, dA, ldda, dtau, dwork)) return -1;
+  e = bsofi_dev_prepare();
   if (e) return cuda_info((cudaError_t)e);
   e = bsofi_dev_bsoi(n, L, dA, ldda, dtau, dwork, stream);
   return e ? cuda_info((cudaError_t)e) : 0;
@@ -932,7 +942,9 @@ int bsofi_device_bsoi(int n, int L, double *dA, int ldda, const double *dtau, vo
 
 int bsofi_device_invert(int n, int L, double *dA, int ldda, double *dtau, void *dwork,
                         void *stream) {
-  int e = bsofi_dev_prepare();
+  int e;
+  if (!device_args_ok(n, L, dA, ldda, dtau, dwork)) return -1;
+  e = bsofi_dev_prepare();
   if (!e) e = bsofi_dev_invert(n, L, dA, ldda, dtau, dwork, stream);
   return e ? cuda_info((cudaError_t)e) : 0;
 }

@@ -147,8 +147,9 @@ unsigned long long bsofi_device_workspace_bytes(int n, int L, int ldda);
 /* BSOF + BSTRI + BSOI on device memory, enqueued on `stream`
  * (cudaStream_t, 0 = legacy default stream); dtau is device memory (N
  * doubles), dwork device memory of bsofi_device_workspace_bytes.  dA must
- * hold the p-cyclic input with every other block zero.  Returns 0 or
- * BSOFI_INFO_CUDA - cudaError_t; the BSTRI info word is at
+ * hold the p-cyclic input (no other block is read).  Returns 0, -1 for an
+ * illegal argument (n outside 1..BSOFI_MAX_BLOCK, L < 2, ldda < n*L, a NULL
+ * pointer) or BSOFI_INFO_CUDA - cudaError_t; the BSTRI info word is at
  * bsofi_device_info(dwork) (device int, values >= 0x7f7f7f7f mean 0; after
  * bsofi_device_invert or bsofi_device_bsoi it is BSOFI_INFO_CUDA -
  * cudaErrorLaunchTimeout if a bounded wait inside a persistent kernel gave

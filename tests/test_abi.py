@@ -93,3 +93,15 @@ def test_timers():
     lib.fgetwalltime_(t0.ctypes.data_as(_dp))
     lib.fgetwalltime_(t1.ctypes.data_as(_dp))
     assert lib.felapsed_(t1.ctypes.data_as(_dp), t0.ctypes.data_as(_dp)) >= 0.0
+
+
+def test_device_api_rejects_bad_arguments():
+    """The device entry points validate sizes and pointers before any CUDA
+    call (n beyond BSOFI_MAX_BLOCK = 768, L < 2, ldda < n L, NULL)."""
+    lib = _lib.load()
+    fake = 0x1000  # never dereferenced: the checks come first
+    for n, L, ld, p in [(769, 2, 1538, fake), (0, 4, 16, fake), (4, 1, 16, fake), (4, 4, 15, fake),
+                        (4, 4, 16, 0)]:
+        assert lib.bsofi_device_invert(n, L, p, ld, fake, fake, None) == -1
+        assert lib.bsofi_device_bsoftri(n, L, p, ld, fake, fake, None) == -1
+        assert lib.bsofi_device_bsoi(n, L, p, ld, fake, fake, None) == -1

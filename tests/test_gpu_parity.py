@@ -197,3 +197,17 @@ def test_handle_api_pinned_host_arrays(cuda_device, n, L):
         assert h.bsoftri(A, tau) == 0
         assert h.bsoi(A, tau) == 0
         assert residual(M, A) < 1e-13
+
+
+@pytest.mark.parametrize("L", [2, 3])
+def test_largest_block_size(cuda_device, L):
+    """n = BSOFI_MAX_BLOCK (768): the tallest panels (2n = 1536 rows, six rows
+    per thread in the BSOF kernel) against the oracle."""
+    n = 768
+    M = random_pcyclic(n, L, seed=768 + L)
+    Ar, taur, Xr = _reference(M, n, L)
+    X, state, tau, info = api.invert(M, n, L)
+    assert info == 0
+    _check_state(M, n, L, state, tau, Ar, taur, Xr)
+    assert rel_fro(X, Xr) < inverse_tolerance(M, Xr)
+    assert residual(M, X) < 1e-13
