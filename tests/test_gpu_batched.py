@@ -13,7 +13,8 @@ def test_batched_matches_single(cuda_device):
     import torch
     from gpu_util import from_device_colmajor, to_device_colmajor
     specs = [(64, 8, "hub", 3), (100, 5, "hub", 4), (36, 12, "rand", 5), (144, 3, "hub", 6),
-             (17, 9, "rand", 7), (256, 4, "hub", 8), (49, 2, "hub", 9)]
+             (17, 9, "rand", 7), (256, 4, "hub", 8), (49, 2, "hub", 9), (289, 3, "hub", 10),
+             (450, 2, "rand", 11)]
     mats = []
     for n, L, kind, seed in specs:
         if kind == "hub":

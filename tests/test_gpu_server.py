@@ -32,7 +32,7 @@ def test_server_results_match_alone(cuda_device):
     from gpu_util import from_device_colmajor, to_device_colmajor
     specs = [(64, 8, "hub", 1), (100, 12, "hub", 2), (36, 20, "rand", 3), (144, 6, "hub", 4),
              (25, 33, "rand", 5), (196, 4, "hub", 6), (64, 16, "hub", 7), (81, 9, "hub", 8),
-             (12, 50, "rand", 9), (256, 3, "hub", 10)]
+             (12, 50, "rand", 9), (256, 3, "hub", 10), (324, 4, "hub", 11), (400, 3, "rand", 12)]
     mats = [hubbard_matrix(int(round(n ** 0.5)), L, 3.0, seed=s) if k == "hub"
             else random_pcyclic(n, L, seed=s) for n, L, k, s in specs]
     sizes = [api.server_request_bytes(n, L, n * L) for n, L, _, _ in specs]
