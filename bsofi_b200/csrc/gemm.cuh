@@ -210,19 +210,27 @@ BSOFI_DEVINL void gemm_tile(const GemmDims& d, const GemmA& a, const GemmB& b,
     const double* tB = sB + (it % Cfg::STAGES) * Cfg::B_STAGE + (wn * Cfg::WTN + g) * Cfg::SB + t;
 #pragma unroll
     for (int k8 = 0; k8 < Cfg::BK / 8; k8++) {
-      // With 32-deep stages the next stage's loads are issued after the first
-      // k8 step's DMMAs, so the tensor pipe has work queued while the warp
-      // computes addresses (measured: -4% on 128x128 K32 tiles; with 16-deep
-      // stages issuing them first is faster).
-      if (k8 == (Cfg::BK >= 32 ? 1 : 0)) {
+      // With 32-deep stages the next stage's B loads are issued after the
+      // first k8 step's DMMAs and its A loads after the second, so the tensor
+      // pipe has work queued while the warp computes addresses (measured: -6%
+      // on 128x128 K32 tiles; with 16-deep stages issuing them first is
+      // faster).
+      {
+        constexpr int KA = Cfg::BK >= 32 ? 2 : 0, KB = Cfg::BK >= 32 ? 1 : 0;
         int nx = it + Cfg::STAGES - 1;
-        if (nx < nkt) {
+        if (k8 == KA && nx < nkt) {
           int s = nx % Cfg::STAGES;
           int k0 = (kt0 + nx) * Cfg::BK;
           load_a_tile<Cfg, ALIGNED>(sA + s * Cfg::A_STAGE, a, pa0, pa1, d.M, d.K, m0, k0);
-          load_b_tile<Cfg, ALIGNED>(sB + s * Cfg::B_STAGE, b, pb, d.N, d.K, k0, n0);
         }
-        cp_async_commit();
+        if (k8 == KB) {
+          if (nx < nkt) {
+            int s = nx % Cfg::STAGES;
+            int k0 = (kt0 + nx) * Cfg::BK;
+            load_b_tile<Cfg, ALIGNED>(sB + s * Cfg::B_STAGE, b, pb, d.N, d.K, k0, n0);
+          }
+          cp_async_commit();
+        }
       }
       double af[Cfg::MT][4], bf[Cfg::NT][2];
 #pragma unroll
