@@ -216,21 +216,22 @@ BSOFI_DEVINL void gemm_tile(const GemmDims& d, const GemmA& a, const GemmB& b,
       // on 128x128 K32 tiles; with 16-deep stages issuing them first is
       // faster).
       {
+        // One commit group per iteration holding both of the stage's loads:
+        // the group is committed after the later of the two.
         constexpr int KA = Cfg::BK >= 32 ? 2 : 0, KB = Cfg::BK >= 32 ? 1 : 0;
+        constexpr int KC = KA > KB ? KA : KB;
         int nx = it + Cfg::STAGES - 1;
         if (k8 == KA && nx < nkt) {
           int s = nx % Cfg::STAGES;
           int k0 = (kt0 + nx) * Cfg::BK;
           load_a_tile<Cfg, ALIGNED>(sA + s * Cfg::A_STAGE, a, pa0, pa1, d.M, d.K, m0, k0);
         }
-        if (k8 == KB) {
-          if (nx < nkt) {
-            int s = nx % Cfg::STAGES;
-            int k0 = (kt0 + nx) * Cfg::BK;
-            load_b_tile<Cfg, ALIGNED>(sB + s * Cfg::B_STAGE, b, pb, d.N, d.K, k0, n0);
-          }
-          cp_async_commit();
+        if (k8 == KB && nx < nkt) {
+          int s = nx % Cfg::STAGES;
+          int k0 = (kt0 + nx) * Cfg::BK;
+          load_b_tile<Cfg, ALIGNED>(sB + s * Cfg::B_STAGE, b, pb, d.N, d.K, k0, n0);
         }
+        if (k8 == KC) cp_async_commit();
       }
       double af[Cfg::MT][4], bf[Cfg::NT][2];
 #pragma unroll
