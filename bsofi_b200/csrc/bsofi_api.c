@@ -168,6 +168,12 @@ typedef struct bsofi_ctx {
   cudaEvent_t *ev;      /* 2 * nev: [0, nev) uploaded, [nev, 2 nev) finished */
   cudaEvent_t ev_refl, ev_start;
   int nev;
+  /* G_k = Q_k^T formed by the last hybridxbsoftrih_ stay in the workspace;
+   * dref holds the reflector rows and tau they were formed from, so that
+   * hybridxbsoih_ skips Q formation when it gets the same state back. */
+  double *dref;
+  int *dflag, *hflag;
+  int g_valid;
 } bsofi_ctx;
 
 /* Layout of the caller's integer handler(10) (40 bytes). */
@@ -189,9 +195,12 @@ static void ctx_free_buffers(bsofi_ctx *c) {
   if (c->dA) cudaFree(c->dA);
   if (c->dtau) cudaFree(c->dtau);
   if (c->dws) cudaFree(c->dws);
+  if (c->dref) cudaFree(c->dref);
   c->dA = NULL;
   c->dtau = NULL;
   c->dws = NULL;
+  c->dref = NULL;
+  c->g_valid = 0;
   c->n = c->L = c->ldd = 0;
 }
 
@@ -208,6 +217,11 @@ static cudaError_t ctx_fit(bsofi_ctx *c, int n, int L) {
   if ((e = cudaMalloc(&c->dws, c->ws_bytes)) != cudaSuccess) goto fail;
   /* info words (BSTRI info, BSOF and BSOI error words) start cleared */
   if ((e = cudaMemset(c->dws, 0, 256)) != cudaSuccess) goto fail;
+  if ((e = cudaMalloc((void **)&c->dref, sizeof(double) * bsofi_dev_state_ref_doubles(n, L))) !=
+      cudaSuccess)
+    goto fail;
+  if (!c->dflag && (e = cudaMalloc((void **)&c->dflag, sizeof(int))) != cudaSuccess) goto fail;
+  if (!c->hflag && (e = cudaMallocHost((void **)&c->hflag, sizeof(int))) != cudaSuccess) goto fail;
   c->n = n;
   c->L = L;
   c->ldd = ldd;
@@ -277,6 +291,8 @@ static void ctx_destroy(bsofi_ctx *c) {
   free(c->ev);
   if (c->ev_refl) cudaEventDestroy(c->ev_refl);
   if (c->ev_start) cudaEventDestroy(c->ev_start);
+  if (c->dflag) cudaFree(c->dflag);
+  if (c->hflag) cudaFreeHost(c->hflag);
   if (c->stream) cudaStreamDestroy(c->stream);
   c->magic = 0;
   free(c);
@@ -490,9 +506,16 @@ static int drive_bsoftri(bsofi_ctx *c, int n, int L, double *A, int lda, double 
   } else {
     if ((e = copy_state(c, A, lda, 0)) != cudaSuccess) return cuda_info(e);
   }
-  if (do_bsof && do_tri)
-    e = (cudaError_t)bsofi_dev_bsoftri(n, L, c->dA, c->ldd, c->dtau, c->dws, c->stream);
-  else if (do_bsof)
+  c->g_valid = 0;
+  if (do_bsof && do_tri) {
+    /* The workers also form every G_k (off the critical chain) for the BSOI
+     * call that usually follows; dref records what they were formed from. */
+    e = (cudaError_t)bsofi_dev_bsoftri_q(n, L, c->dA, c->ldd, c->dtau, c->dws, c->stream);
+    if (e == cudaSuccess)
+      e = (cudaError_t)bsofi_dev_state_ref(n, L, c->dA, c->ldd, c->dtau, c->dref, 0, c->dflag,
+                                           c->stream);
+    if (e == cudaSuccess) c->g_valid = 1;
+  } else if (do_bsof)
     e = (cudaError_t)bsofi_dev_bsof(n, L, c->dA, c->ldd, c->dtau, c->dws, c->stream);
   else
     e = (cudaError_t)bsofi_dev_bstri(n, L, c->dA, c->ldd, c->dws, c->stream);
@@ -509,6 +532,18 @@ static int drive_bsoftri(bsofi_ctx *c, int n, int L, double *A, int lda, double 
   }
   e = cudaStreamSynchronize(c->stream);
   return e == cudaSuccess ? 0 : cuda_info(e);
+}
+
+/* After the reflector rows and tau of a state are on the device (ordered
+ * before `st`): 1 if they are the ones the workspace's G_k were formed from. */
+static int state_matches(bsofi_ctx *c, int n, int L, cudaStream_t st) {
+  if (!c->g_valid) return 0;
+  if (cudaMemsetAsync(c->dflag, 0, sizeof(int), st) != cudaSuccess) return 0;
+  if (bsofi_dev_state_ref(n, L, c->dA, c->ldd, c->dtau, c->dref, 1, c->dflag, st) != 0) return 0;
+  if (cudaMemcpyAsync(c->hflag, c->dflag, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    return 0;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return 0;
+  return *c->hflag == 0;
 }
 
 /* Streams and L events of each kind for the pipelined BSOI. */
@@ -577,9 +612,18 @@ static cudaError_t bsoi_pipelined(bsofi_ctx *c, int n, int L, double *A, int lda
   if (e != cudaSuccess) goto drain;
   /* compute */
   if ((e = cudaStreamWaitEvent(c->stream, c->ev_refl, 0)) != cudaSuccess) goto drain;
-  if ((r = bsofi_dev_bsoi_form_q(n, L, c->dA, c->ldd, c->dtau, c->dws, c->stream)) != 0) {
-    e = (cudaError_t)r;
-    goto drain;
+  if (!state_matches(c, n, L, c->stream)) {
+    if ((r = bsofi_dev_bsoi_form_q(n, L, c->dA, c->ldd, c->dtau, c->dws, c->stream)) != 0) {
+      e = (cudaError_t)r;
+      goto drain;
+    }
+    /* The workspace's G_k now belong to this state. */
+    if ((r = bsofi_dev_state_ref(n, L, c->dA, c->ldd, c->dtau, c->dref, 0, c->dflag,
+                                 c->stream)) != 0) {
+      e = (cudaError_t)r;
+      goto drain;
+    }
+    c->g_valid = 1;
   }
   if ((e = cudaStreamWaitEvent(c->stream, up[L - 1], 0)) != cudaSuccess) goto drain;
   if ((r = bsofi_dev_bsoi_carry(n, L, c->dA, c->ldd, c->dws, c->stream)) != 0) {
@@ -628,7 +672,11 @@ static int drive_bsoi(bsofi_ctx *c, int n, int L, double *A, int lda, const doub
   if ((e = copy_state(c, A, lda, 0)) != cudaSuccess) return cuda_info(e);
   e = cudaMemcpyAsync(c->dtau, tau, sizeof(double) * N, cudaMemcpyHostToDevice, c->stream);
   if (e != cudaSuccess) return cuda_info(e);
-  e = (cudaError_t)bsofi_dev_bsoi(n, L, c->dA, c->ldd, c->dtau, c->dws, c->stream);
+  {
+    const int q_ready = state_matches(c, n, L, c->stream);
+    if (!q_ready) c->g_valid = 0;
+    e = (cudaError_t)bsofi_dev_bsoi_ex(n, L, c->dA, c->ldd, c->dtau, c->dws, c->stream, q_ready);
+  }
   if (e != cudaSuccess) return cuda_info(e);
   e = d2h_cols(c, A, lda, c->dA, c->ldd, N, N);
   if (e != cudaSuccess) return cuda_info(e);

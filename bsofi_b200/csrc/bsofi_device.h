@@ -44,6 +44,21 @@ int bsofi_dev_invert_ex(int n, int L, double *dA, int ldd, double *dtau, void *d
 int bsofi_dev_bsoi(int n, int L, double *dA, int ldd, const double *dtau, void *dws,
                    void *stream);
 
+/* BSOF (also forming every G_k = Q_k^T in the workspace, off the critical
+ * chain) + BSTRI; and BSOI that skips Q formation when q_ready (the
+ * workspace's G_k belong to the state in dA and dtau). */
+int bsofi_dev_bsoftri_q(int n, int L, double *dA, int ldd, double *dtau, void *dws,
+                        void *stream);
+int bsofi_dev_bsoi_ex(int n, int L, double *dA, int ldd, const double *dtau, void *dws,
+                      void *stream, int q_ready);
+
+/* The reflector rows of every block column and tau (what Q formation reads):
+ * mode 0 packs them into ref (bsofi_dev_state_ref_doubles doubles), mode 1
+ * compares them with ref and sets the device int *dflag to 1 on a difference. */
+size_t bsofi_dev_state_ref_doubles(int n, int L);
+int bsofi_dev_state_ref(int n, int L, const double *dA, int ldd, const double *dtau, double *ref,
+                        int mode, int *dflag, void *stream);
+
 /* BSOI in pieces, for callers that overlap it with host copies:
  * form_q builds every G_k = Q_k^T (needs the reflectors and tau);
  * carry seeds the first step (needs column block L-1);

@@ -87,6 +87,10 @@ constexpr int kInfoWaitFailed = -1000 - (int)cudaErrorLaunchTimeout;
 cudaError_t launch_copy_masked(double* dst, long long ldd, const double* src, long long lds,
                                int rows, int cols, int roff, cudaStream_t st,
                                int* fold = nullptr);
+// Pack (mode 0) or compare (mode 1, *mismatch set on a difference) the
+// reflector rows of every block column and tau; ref holds 2 n^2 L + n L doubles.
+cudaError_t launch_state_ref(const double* A, long long ld, int n, int L, const double* tau,
+                             double* ref, int mode, int* mismatch, cudaStream_t st);
 // Zero the n x n blocks of A that BSOF reads as structural zeros:
 // superdiagonal blocks (k,k+1) and last-column blocks (k,L-1), 1 <= k <= L-2.
 cudaError_t launch_zero_structural(double* A, long long ld, int n, int L, cudaStream_t st);

@@ -140,6 +140,47 @@ cudaError_t launch_trtri_blocks(double* A, long long ld, int n, long long bstrid
 }
 
 // ------------------------------------------------------------------ utilities
+// The part of the BSOF/I state that Q formation reads: rows [k n, (k+2) n)
+// of block column k (the reflectors under each panel's diagonal, with the
+// diagonal block), packed block after block with a 2n x n stride, then tau.
+// mode 0 packs it into ref; mode 1 compares it with ref and sets *mismatch on
+// any difference (bitwise: NaN never matches).
+__global__ void state_ref_kernel(const double* A, long long ld, int n, int L, const double* tau,
+                                 double* ref, int mode, int* mismatch) {
+  const int k = blockIdx.y;
+  const long long N = (long long)n * L;
+  if (k < L) {
+    const long long r0 = (long long)k * n;
+    const int rows = (int)min(2ll * n, N - r0);
+    const long long cnt = (long long)rows * n;
+    const double* src = A + r0 + r0 * ld;
+    double* dst = ref + (long long)k * 2 * n * n;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < cnt;
+         e += (long long)gridDim.x * blockDim.x) {
+      const double v = src[(e % rows) + (e / rows) * ld];
+      if (mode == 0) dst[e] = v;
+      else if (!(v == dst[e])) *mismatch = 1;
+    }
+  } else {
+    double* dt = ref + 2ll * n * n * L;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < N;
+         e += (long long)gridDim.x * blockDim.x) {
+      const double v = tau[e];
+      if (mode == 0) dt[e] = v;
+      else if (!(v == dt[e])) *mismatch = 1;
+    }
+  }
+}
+
+cudaError_t launch_state_ref(const double* A, long long ld, int n, int L, const double* tau,
+                             double* ref, int mode, int* mismatch, cudaStream_t st) {
+  const long long per = 2ll * n * n;
+  const int gx = (int)min((per + 255) / 256, 256ll);
+  state_ref_kernel<<<dim3(gx, L + 1), 256, 0, st>>>(A, ld, n, L, tau, ref, mode, mismatch);
+  return cudaGetLastError();
+}
+
+
 __global__ void set_identity_kernel(double* G, long long ld, int m, long long bs) {
   double* g = G + (long long)blockIdx.y * bs;
   long long total = (long long)m * m;

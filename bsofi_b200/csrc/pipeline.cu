@@ -501,6 +501,30 @@ int bsofi_dev_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* 
   return run_bsoi(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, false);
 }
 
+int bsofi_dev_bsoftri_q(int n, int L, double* dA, int ldd, double* dtau, void* dws,
+                        void* stream) {
+  g_launches = 0;
+  int e = run_bsof(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, true, bsof_workers(n, L, 0));
+  if (e) return e;
+  return run_bstri(n, L, dA, ldd, dws, (cudaStream_t)stream);
+}
+
+int bsofi_dev_bsoi_ex(int n, int L, double* dA, int ldd, const double* dtau, void* dws,
+                      void* stream, int q_ready) {
+  g_launches = 0;
+  return run_bsoi(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, q_ready != 0);
+}
+
+size_t bsofi_dev_state_ref_doubles(int n, int L) {
+  return 2ull * n * n * L + (size_t)n * L;
+}
+
+int bsofi_dev_state_ref(int n, int L, const double* dA, int ldd, const double* dtau, double* ref,
+                        int mode, int* dflag, void* stream) {
+  CK(launch_state_ref(dA, ldd, n, L, dtau, ref, mode, dflag, (cudaStream_t)stream));
+  return 0;
+}
+
 int bsofi_dev_bsoi_form_q(int n, int L, double* dA, int ldd, const double* dtau, void* dws,
                           void* stream) {
   return bsoi_form_q(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream);

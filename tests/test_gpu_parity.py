@@ -211,3 +211,47 @@ def test_largest_block_size(cuda_device, L):
     _check_state(M, n, L, state, tau, Ar, taur, Xr)
     assert rel_fro(X, Xr) < inverse_tolerance(M, Xr)
     assert residual(M, X) < 1e-13
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+def test_handle_bsoi_with_another_state_recomputes_q(cuda_device, pinned):
+    """hybridxbsoih_ reuses the Q_k^T its handle formed during hybridxbsoftrih_
+    only for the same state: a handle given another matrix's state (or a
+    changed tau) forms Q again and inverts that matrix."""
+    import torch
+    n, L = 40, 6
+    N = n * L
+    M1 = random_pcyclic(n, L, seed=51)
+    M2 = random_pcyclic(n, L, seed=52)
+
+    def host(a):
+        if not pinned:
+            return np.asfortranarray(a.copy())
+        t = torch.empty(a.shape[::-1], dtype=torch.float64, pin_memory=True).numpy().T
+        t[:] = a
+        return t
+
+    X2, state2, tau2, info = api.invert(M2, n, L)
+    assert info == 0
+    with api.Handle(n, L) as h:
+        A1 = host(M1)
+        tau1 = np.zeros(N)
+        assert h.bsoftri(A1, tau1) == 0
+        # Another matrix's state through the same handle.
+        A = host(state2)
+        assert h.bsoi(A, tau2.copy()) == 0
+        assert rel_fro(A, X2) < inverse_tolerance(M2, X2)
+        assert residual(M2, A) < 1e-13
+        # The first state again, but with one tau changed: Q must be re-formed.
+        A1b = host(M1)
+        tau1b = np.zeros(N)
+        assert h.bsoftri(A1b, tau1b) == 0
+        tau_mod = tau1b.copy()
+        tau_mod[3] = 0.0
+        Am = host(np.array(A1b))
+        assert h.bsoi(Am, tau_mod) == 0
+    # Reference for the modified state: a fresh handle (nothing to reuse).
+    with api.Handle(n, L) as h2:
+        Ar = host(np.array(A1b))
+        assert h2.bsoi(Ar, tau_mod) == 0
+    assert rel_fro(Am, Ar) < 1e-12
