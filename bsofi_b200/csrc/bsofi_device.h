@@ -70,6 +70,14 @@ int bsofi_dev_bsoi_carry(int n, int L, double *dA, int ldd, void *dws, void *str
 int bsofi_dev_bsoi_step(int n, int L, int k, double *dA, int ldd, void *dws, void *stream);
 int bsofi_dev_bsoi_finish(int n, int L, double *dA, int ldd, void *dws, void *stream);
 
+/* FP32 <-> FP64 copies for the single-precision API: region 0 the whole
+ * N x N matrix, 1 the BSOF/BSTRI state (rows [0, min((k+2)n, N)) of block
+ * column k), 2 the p-cyclic input blocks.  to_float 0 widens f (pitch ldf)
+ * into d (pitch ldd), 1 rounds d into f. */
+int bsofi_dev_convert(int n, int L, float *f, int ldf, double *d, int ldd, int region,
+                      int to_float, void *stream);
+int bsofi_dev_convert_vec(float *f, double *d, int len, int to_float, void *stream);
+
 /* Device address of the int info words inside the workspace: [0] BSTRI info
  * (values >= 0x7f7f7f7f mean 0; i > 0: R(i,i) exactly zero, 1-based global
  * index), [1] BSOF, [2] BSOI, [3] BSTRI wait timeout (nonzero = error). */

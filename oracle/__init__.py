@@ -13,6 +13,9 @@ Two checkers, same calling convention (column-major float64, ``lda = n*L``):
   101-157), which without CUDA is lapackXbsof + lapackXbstri +
   lapackXbsoi_ormqr (src/bsofi_cpu.c:86-248).
 * ``port_*`` -- the plain-C restatement in ``oracle/bsofi_oracle.c``.
+* ``ref32_*`` -- the reference's single-precision variant (the same sources
+  with -D__SINGLE_PREC__, scalar_t = float; config.h:132-136), the checker for
+  libbsofi_b200_fp32.so.  Column-major float32.
 """
 import ctypes
 import os
@@ -21,6 +24,7 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _REF_SO = os.path.join(_HERE, "_ref", "libbsofi_ref.so")
+_REF32_SO = os.path.join(_HERE, "_ref", "libbsofi_ref_fp32.so")
 _PORT_SO = os.path.join(_HERE, "liboracle.so")
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -39,18 +43,22 @@ def ref_available():
     return os.path.exists(_REF_SO)
 
 
+def ref32_available():
+    return os.path.exists(_REF32_SO)
+
+
 def _lib(kind):
     if kind not in _libs:
-        path = _REF_SO if kind == "ref" else _PORT_SO
+        path = {"ref": _REF_SO, "ref32": _REF32_SO}.get(kind, _PORT_SO)
         if not os.path.exists(path):
             raise RuntimeError("oracle library missing: %s (run make -C oracle)" % path)
         _libs[kind] = ctypes.CDLL(path)
     return _libs[kind]
 
 
-def set_ref_threads(k):
+def set_ref_threads(k, kind="ref"):
     """Set the OpenBLAS thread count used by the reference library."""
-    lib = _lib("ref")
+    lib = _lib(kind)
     try:
         f = lib.openblas_set_num_threads
     except AttributeError:
@@ -124,6 +132,50 @@ def ref_inverse(M, n, L):
 def ref_lwork(n, L):
     lib = _lib("ref")
     return int(lib.lapackXbsofiLWork(ctypes.c_int(n), ctypes.c_int(L), ctypes.c_int(n * L)))
+
+
+# ------------------------------------------------ reference, single precision
+_fp = ctypes.POINTER(ctypes.c_float)
+
+
+def _check32(A, n, L):
+    N = n * L
+    A = np.asfortranarray(np.array(A, dtype=np.float32, copy=True))
+    if A.shape != (N, N):
+        raise ValueError("A must be %dx%d" % (N, N))
+    return A
+
+
+def _ref32_call(fname, A, tau, n, L):
+    lib = _lib("ref32")
+    N = n * L
+    h = np.zeros(10, dtype=np.int32)
+    hp = h.ctypes.data_as(_ip)
+    lib.hybridxinith_(hp, _i(n), _i(L), _i(N))
+    lw = lib.hybridxbsofilworkh_(hp, _i(n), _i(L), _i(N))
+    work = np.zeros(max(int(lw), 1), dtype=np.float32)
+    info = ctypes.c_int(0)
+    getattr(lib, fname)(hp, _i(n), _i(L), A.ctypes.data_as(_fp), _i(N), tau.ctypes.data_as(_fp),
+                        work.ctypes.data_as(_fp), _i(lw), ctypes.byref(info))
+    lib.hybridxfinalizeh_(hp)
+    return info.value
+
+
+def ref32_bsoftri(A, n, L):
+    """hybridxbsoftrih_ of the single-precision build on a float32 copy of A.
+    Returns (A_out, tau, info)."""
+    A = _check32(A, n, L)
+    tau = np.zeros(n * L, dtype=np.float32)
+    info = _ref32_call("hybridxbsoftrih_", A, tau, n, L)
+    return A, tau, info
+
+
+def ref32_bsoi(A, tau, n, L):
+    """hybridxbsoih_ of the single-precision build.  Returns (A_out, info)."""
+    A = _check32(A, n, L)
+    tau = np.array(tau, dtype=np.float32, copy=True)
+    info = _ref32_call("hybridxbsoih_", A, tau, n, L)
+    return A, info
 
 
 # ---------------------------------------------------------------- C port
