@@ -15,7 +15,8 @@ Printed JSON line (rank 0): value (device-resident inversions/s), tflops
 (flop model of include/bsofi_flops.h), roofline of the dominant kernel (the
 persistent BSOI kernel, FP64 DMMA, against cuBLAS DGEMM measured in the same run),
 e2e (the reference handle API hybridxbsoftrih_ + hybridxbsoih_ on pinned host
-buffers, copies included; e2e_pageable the same on pageable numpy arrays),
+buffers, copies included; e2e_pageable the same on pageable numpy arrays;
+e2e_fp32 the single-precision library's handle API on pinned float arrays),
 cpu_baseline (the reference's CPU path,
 oracle/_ref, on the host cores), clocks sampled during the timed region.
 
@@ -383,11 +384,12 @@ def main():
     if args.serve > 0:
         served = run_serving(api, torch, dev, args.serve, args.serve_rate, 31 + rank)
 
-    e2e = e2e_pageable = None
+    e2e = e2e_pageable = e2e_fp32 = None
     if not args.no_e2e and args.e2e_steps > 0:
         e2e = run_e2e(api, torch, dist, world, side, L, U, rank, args.e2e_steps)
         e2e_pageable = run_e2e(api, torch, dist, world, side, L, U, rank, args.e2e_steps,
                                pinned=False)
+        e2e_fp32 = run_e2e_fp32(torch, dist, world, side, L, U, rank, args.e2e_steps)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu and args.cpu_sample > 0:
@@ -410,6 +412,7 @@ def main():
                 "residual": resid,
                 "roofline": roofline, "roofline_bsof": roofline_bsof,
                 "cpu_baseline": cpu, "e2e": e2e, "e2e_pageable": e2e_pageable,
+                "e2e_fp32": e2e_fp32,
                 "batched": batched, "batched_mixed_sizes": batched_mixed, "served": served,
                 "gpu_launches": launches_per_step * args.steps,
                 "clocks": clk}
@@ -604,6 +607,51 @@ def run_e2e(api, torch, dist, world, side, L, U, rank, steps, pinned=True):
             "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
             "api": "hybridxbsoftrih_ + hybridxbsoih_ (host %s buffers)"
                    % ("pinned" if pinned else "pageable"),
+            "steps": len(times), "residual": resid}
+
+
+def run_e2e_fp32(torch, dist, world, side, L, U, rank, steps):
+    """The single-precision library's handle API (libbsofi_b200_fp32.so) on
+    pinned float32 host buffers, copies included: same workload, half the
+    host <-> device bytes of the FP64 API."""
+    from bsofi_b200 import fp32
+    from bsofi_b200.hubbard import hubbard_matrix, pcyclic_blocks
+    n = side * side
+    N = n * L
+    M32 = hubbard_matrix(side, L, U, seed=777 + rank).astype(np.float32)
+    A = torch.empty((N, N), dtype=torch.float32, pin_memory=True).numpy().T
+    tau = torch.zeros(N, dtype=torch.float32, pin_memory=True).numpy()
+    h = fp32.Handle(n, L)
+    times = []
+    for i in range(steps + 1):
+        np.copyto(A, M32)
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        info = h.bsoftri(A, tau)
+        info2 = h.bsoi(A, tau)
+        dt = time.perf_counter() - t0
+        if info or info2:
+            raise RuntimeError("FP32 handle API info %d %d" % (info, info2))
+        if i > 0:
+            times.append(dt)
+    h.close()
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from gpu_util import block_residual_gpu
+    resid = block_residual_gpu(torch, *pcyclic_blocks(M32.astype(np.float64), n, L),
+                               torch.from_numpy(np.ascontiguousarray(A, dtype=np.float64)).to("cuda"))
+    if not resid < 1e-5:
+        raise RuntimeError("FP32 e2e result check failed: residual %g" % resid)
+    t = torch.tensor([sum(times)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    tot = float(t.item())
+    state_bytes = sum(min(N, (k + 2) * n) * n for k in range(L)) * 4
+    return {"value": world * len(times) / tot, "unit": "inversions/s",
+            "h2d_bytes_per_step": 2 * L * n * n * 4 + state_bytes + N * 4,
+            "d2h_bytes_per_step": state_bytes + N * 4 + N * N * 4,
+            "api": "hybridxbsoftrih_ + hybridxbsoih_ of libbsofi_b200_fp32.so (host pinned "
+                   "float32 buffers; FP64 arithmetic on the GPU, results rounded to float32)",
             "steps": len(times), "residual": resid}
 
 
