@@ -100,16 +100,21 @@ BSOFI_API int bsofi_autotune(int n, int L, int reps, void* stream, int* plan_out
   float best;
   if ((c = time_plan(n, L, ldd, b, st, plan, reps, &best)) != cudaSuccess) goto fail;
   {
-    // Knob 0: BSOI form; knob 1: BSTRI recurrence tiles; knob 2: BSOF workers.
+    // Knob 0: BSOI form; knob 3: BSTRI row group; knob 1: BSTRI one-row
+    // recurrence tiles (only used with row group 0); knob 2: BSOF workers.
     static const int cand0[] = {0, 5, 1, 2, 3, 4};
     static const int cand1[] = {2, 4, 0, 3, 1};
     static const int cand2[] = {32, 48, 16, 64};
-    const int* cands[3] = {cand0, cand1, cand2};
-    const int ncand[3] = {6, 5, 4};
-    for (int knob = 0; knob < 3; knob++) {
+    static const int cand3[] = {0, 4, 2, 6};
+    const int* cands[4] = {cand0, cand1, cand2, cand3};
+    const int ncand[4] = {6, 5, 4, 4};
+    static const int order[4] = {0, 3, 1, 2};
+    for (int o = 0; o < 4; o++) {
+      const int knob = order[o];
+      if (knob == 1 && plan[3] >= 2) continue;
       for (int i = 0; i < ncand[knob]; i++) {
         if (cands[knob][i] == plan[knob]) continue;
-        int trial[4] = {plan[0], plan[1], plan[2], 0};
+        int trial[4] = {plan[0], plan[1], plan[2], plan[3]};
         trial[knob] = cands[knob][i];
         float t;
         if ((c = time_plan(n, L, ldd, b, st, trial, reps, &t)) != cudaSuccess) goto fail;

@@ -87,7 +87,8 @@ int *bsofi_dev_info_ptr(void *dws);
  * tile count, 2/3/4 per-step 64x64 / 128x128 K-stage 32 / 128x128 K-stage 16
  * tiles), plan[1] BSTRI recurrence (launch_gemm cfg per step, or 4 for the
  * persistent recurrence kernel), plan[2]
- * BSOF worker CTAs, plan[3] reserved; plan[0] = 5: persistent BSOI with
+ * BSOF worker CTAs, plan[3] the BSTRI row group (0 one block row per step,
+ * 2..8 block rows per step of the blocked recurrence); plan[0] = 5: persistent BSOI with
  * 64x64 tiles.  get returns 1 for a tuned plan, 0 for
  * the default (plan still filled); set returns -1 for an invalid plan. */
 int bsofi_dev_plan_get(int n, int L, int *plan);

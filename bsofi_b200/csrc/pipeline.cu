@@ -46,13 +46,16 @@ thread_local GemmTimer g_timer;
 // launch of 128x128 / 64x64 tiles; 1: one GEMM launch per step with the tile
 // shape chosen by tile count; 2, 3, 4: per step with 64x64, 128x128 K32,
 // 128x128 K16 tiles), the BSTRI
-// row recurrence (launch_gemm's cfg per step, or 4: one persistent launch)
-// and the number
-// of BSOF worker CTAs of a single inversion.  Tuned plans (bsofi_autotune)
-// live in a process-wide table; other sizes use the default below.
+// row recurrence (launch_gemm's cfg per step, or 4: one persistent launch),
+// the number of BSOF worker CTAs of a single inversion, and the BSTRI row
+// group (0: one recurrence step per block row; 2..8: that many block rows per
+// step of the blocked recurrence, which then replaces bstri_cfg).  Tuned plans
+// (bsofi_autotune) live in a process-wide table; other sizes use the default
+// below.
 struct Plan {
-  int bsoi, bstri_cfg, workers;
+  int bsoi, bstri_cfg, workers, bstri_group;
 };
+constexpr int kMaxBstriGroup = 8;
 std::mutex g_plan_mu;
 std::map<std::pair<int, int>, Plan> g_plans;
 
@@ -62,7 +65,10 @@ Plan default_plan(int n, int L) {
   // 64 x 64 tiles waste less of the 2n columns: one persistent launch for
   // mid-size N (100/64, 196/40, 324/40), per-step launches for N of 20k and
   // more (400/64, 576/80) and for small N (64/16, 144/20).  The persistent
-  // recurrence helped at 64/16 and 400/64 and tied elsewhere.
+  // recurrence helped at 64/16 and 400/64 and tied elsewhere.  The blocked
+  // BSTRI recurrence with 4 rows per step gained 1-7% below N = 20000
+  // (256/32, 196/40, 100/64), 2 rows at 64/16; at 400/64 every group size
+  // lost to the persistent one-row recurrence.
   const int N = n * L;
   const int tiles = ((N + 127) / 128) * ((2 * n + 127) / 128);
   int bsoi;
@@ -71,7 +77,8 @@ Plan default_plan(int n, int L) {
   else if (N >= 4000) bsoi = 5;
   else bsoi = 1;
   const int rec = (N <= 2048 || (N >= 20000 && N < 40000)) ? 4 : 2;
-  return Plan{bsoi, rec, 32};
+  const int group = N >= 20000 ? 0 : (N <= 2048 ? 2 : 4);
+  return Plan{bsoi, rec, 32, group};
 }
 
 Plan plan_for(int n, int L) {
@@ -227,6 +234,117 @@ int run_bsof(int n, int L, double* dA, int ldd, double* dtau, void* ws, cudaStre
   return 0;
 }
 
+// Blocked BSTRI row recurrence.  The block rows i = L-3 .. 0 are taken in
+// groups of grp from the bottom; group g holds rows t..b (b = L-3-g grp).
+// Inside a group, X_{r,c} = W_r W_{r+1} ... W_b X_{b+1,c} for every column c
+// beyond b, so with the stacked products P_r = W_r P_{r+1} (P_b = W_b) one
+// GEMM of (b-t+1) n rows computes the whole group from row b+1:
+//   X_{t:b, b+1:L} = [P_t; ...; P_b] X_{b+1, b+1:L}  (+ Zc on block column L-1),
+// where Zc_r = Z_r + W_r Zc_{r+1} (Zc_b = Z_b) carries the Z terms.  The
+// columns inside the group, X_{r, r+1:b} = W_r X_{r+1, r+1:b}, and P and Zc
+// need only the group's own W_i, Z_i and X_ii, so every group forms them at
+// once, in grp - 1 batched rounds, before the ceil((L-2)/grp) group steps run
+// in order.  Same per-block products as the one-row recurrence, grouped
+// differently; the serial chain is grp times shorter and every step grp times
+// taller.  P (grp n x n per group, leading dimension grp n; a short top group
+// uses the bottom rows of its block) lives in the BSOI carry buffers, which
+// are idle until BSOI.
+int bstri_blocked(int n, int L, double* dA, int ldd, const double* W, double* P, int grp,
+                  cudaStream_t st) {
+  const long long nn = (long long)n * n;
+  const int b0 = L - 3;
+  const int ngr = (L - 2 + grp - 1) / grp;
+  const int mlast = (L - 2) - (ngr - 1) * grp;
+  const long long pld = (long long)grp * n, pbs = pld * n;
+  const long long rstep = -(long long)grp * n;  // row offset from one group to the next
+  const long long dstep = rstep + rstep * (long long)ldd;  // the same along the diagonal
+  // P_b = W_b at the bottom of every group's block.
+  for (int g = 0; g < ngr; g++)
+    CKM(cudaMemcpy2DAsync(P + g * pbs + (long long)(grp - 1) * n, sizeof(double) * pld,
+                          W + (long long)(b0 - g * grp) * nn, sizeof(double) * n,
+                          sizeof(double) * n, n, cudaMemcpyDeviceToDevice, st));
+  for (int q = 1; q < grp; q++) {
+    // Row r = b_g - q of every group that has it.
+    const int batch = mlast > q ? ngr : ngr - 1;
+    if (batch <= 0) break;
+    const int r = b0 - q;  // in group 0
+    GemmDims d1 = {n, n, n};
+    GemmA a = {};
+    a.p0 = W + (long long)r * nn;
+    a.ld0 = n;
+    a.bs0 = -(long long)grp * nn;
+    a.ld1 = 2;
+    a.ksplit = n;
+    a.rlim0 = INT_MAX;
+    a.roff0 = kNoMask;
+    a.rlim1 = INT_MAX;
+    a.roff1 = kNoMask;
+    {  // P_r = W_r P_{r+1}
+      GemmB b = {P + (long long)(grp - q) * n, pld, pbs, kNoMask};
+      GemmC c = {};
+      c.p0 = P + (long long)(grp - 1 - q) * n;
+      c.ld0 = pld;
+      c.bs0 = pbs;
+      c.ld1 = 1;
+      c.nsplit = n;
+      c.alpha = 1.0;
+      CK(launch_gemm(d1, a, b, c, batch, 2, st));
+    }
+    {  // X_{r, r+1:r+q} = W_r X_{r+1, r+1:r+q}; X_{r+1,r+1} is upper triangular
+      GemmDims dq = {n, q * n, n};
+      GemmB b = {dA + cm((long long)(r + 1) * n, (long long)(r + 1) * n, ldd), ldd,
+                 dstep, 0};
+      GemmC c = {};
+      c.p0 = dA + cm((long long)r * n, (long long)(r + 1) * n, ldd);
+      c.ld0 = ldd;
+      c.bs0 = dstep;
+      c.ld1 = 1;
+      c.nsplit = q * n;
+      c.alpha = 1.0;
+      CK(launch_gemm(dq, a, b, c, batch, 2, st));
+    }
+    {  // Zc_r = Z_r + W_r Zc_{r+1}, in place in block column L-1
+      GemmB b = {dA + cm((long long)(r + 1) * n, (long long)(L - 1) * n, ldd), ldd, rstep,
+                 kNoMask};
+      GemmC c = {};
+      c.p0 = dA + cm((long long)r * n, (long long)(L - 1) * n, ldd);
+      c.ld0 = ldd;
+      c.bs0 = rstep;
+      c.ld1 = 1;
+      c.nsplit = n;
+      c.alpha = 1.0;
+      c.beta0 = 1.0;
+      CK(launch_gemm(d1, a, b, c, batch, 2, st));
+    }
+  }
+  // Group steps, bottom to top.
+  for (int g = 0; g < ngr; g++) {
+    const int b = b0 - g * grp, m = b + 1 < grp ? b + 1 : grp, t = b - m + 1;
+    GemmDims d = {m * n, (L - 1 - b) * n, n};
+    GemmA a = {};
+    a.p0 = P + g * pbs + (long long)(grp - m) * n;
+    a.ld0 = pld;
+    a.ld1 = 2;
+    a.ksplit = n;
+    a.rlim0 = INT_MAX;
+    a.roff0 = kNoMask;
+    a.rlim1 = INT_MAX;
+    a.roff1 = kNoMask;
+    GemmB bb = {dA + cm((long long)(b + 1) * n, (long long)(b + 1) * n, ldd), ldd, 0, 0};
+    GemmC c = {};
+    c.p0 = dA + cm((long long)t * n, (long long)(b + 1) * n, ldd);
+    c.ld0 = ldd;
+    c.p1 = dA + cm((long long)t * n, (long long)(L - 1) * n, ldd);
+    c.ld1 = ldd;
+    c.nsplit = (L - 2 - b) * n;
+    c.alpha = 1.0;
+    c.beta0 = 0.0;
+    c.beta1 = 1.0;
+    CK(launch_gemm(d, a, bb, c, 1, 0, st));
+  }
+  return 0;
+}
+
 int run_bstri(int n, int L, double* dA, int ldd, void* ws, cudaStream_t st) {
   Layout ly = layout(n, L, ldd);
   int* info = at<int>(ws, ly.info);
@@ -305,8 +423,13 @@ int run_bstri(int n, int L, double* dA, int ldd, void* ws, cudaStream_t st) {
     CK(launch_gemm(d, a, b, c, L - 2, 0, st));
   }
   // Row recurrence: X_{i, i+1:L} = W_i X_{i+1, i+1:L} (+ Z_i on the last block).
-  const int rec = plan_for(n, L).bstri_cfg;
+  const Plan plan = plan_for(n, L);
+  const int rec = plan.bstri_cfg;
   CKM(cudaMemsetAsync(info + 3, 0, sizeof(int), st));
+  // At most L-2 rows per group: the stacked P then takes at most (2L-5) n^2
+  // doubles, inside the two carry buffers (2 ldd n >= 2 L n^2).
+  const int grp = plan.bstri_group < L - 2 ? plan.bstri_group : L - 2;
+  if (grp >= 2) return bstri_blocked(n, L, dA, ldd, W, at<double>(ws, ly.C0), grp, st);
   if (rec == 4) {
     // One persistent launch, column tiles pipelined across the steps.
     if (L >= 3) {
@@ -573,16 +696,16 @@ int bsofi_dev_plan_get(int n, int L, int* plan) {
   plan[0] = p.bsoi;
   plan[1] = p.bstri_cfg;
   plan[2] = p.workers;
-  plan[3] = 0;
+  plan[3] = p.bstri_group;
   return it == g_plans.end() ? 0 : 1;
 }
 
 int bsofi_dev_plan_set(int n, int L, const int* plan) {
   if (n < 1 || L < 2 || plan[0] < 0 || plan[0] > 5 || plan[1] < 0 || plan[1] > 4 ||
-      plan[2] < 1 || plan[2] > 1024)
+      plan[2] < 1 || plan[2] > 1024 || plan[3] < 0 || plan[3] == 1 || plan[3] > kMaxBstriGroup)
     return -1;
   std::lock_guard<std::mutex> lk(g_plan_mu);
-  g_plans[{n, L}] = Plan{plan[0], plan[1], plan[2]};
+  g_plans[{n, L}] = Plan{plan[0], plan[1], plan[2], plan[3]};
   return 0;
 }
 

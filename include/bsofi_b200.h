@@ -234,7 +234,10 @@ void bsofi_batch_graph_destroy(bsofi_batch_graph *graph);
  * [1] the BSTRI row recurrence (one GEMM launch per step with tiles 0 by
  * tile count, 1 128x128 K16, 2 64x64, 3 128x128 K32; or 4: one persistent
  * launch of 64x64 tiles pipelined across the steps), [2] BSOF worker CTAs of
- * a single inversion, [3] reserved (0).
+ * a single inversion, [3] the BSTRI row group: 0 one recurrence step per
+ * block row, g in 2..8 the blocked recurrence with g block rows per step
+ * (products of g consecutive W_i formed for all groups at once, then one
+ * GEMM of g n rows per group; [1] is then unused).
  * Every inversion of block size n with L blocks uses the tuned plan of (n, L)
  * if there is one, else a default fitted to the sizes tuned on a B200
  * (bsofi_plan_get shows it).  bsofi_autotune times the candidates one knob at a time on a

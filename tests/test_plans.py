@@ -13,12 +13,12 @@ def _clear_plans():
 
 def test_default_plan_follows_the_tuned_sizes():
     # 2n = 512 fills 128-wide tiles and 256 tiles per step: persistent 128x128.
-    assert api.plan_get(256, 32) == (False, [0, 2, 32, 0])
+    assert api.plan_get(256, 32) == (False, [0, 2, 32, 4])
     # Small N: one GEMM launch per step; persistent recurrence for N <= 2048.
-    assert api.plan_get(144, 20) == (False, [1, 2, 32, 0])
-    assert api.plan_get(64, 16) == (False, [1, 4, 32, 0])
+    assert api.plan_get(144, 20) == (False, [1, 2, 32, 4])
+    assert api.plan_get(64, 16) == (False, [1, 4, 32, 2])
     # 2n = 392: 64x64 tiles, persistent for mid-size N, per step for N >= 20k.
-    assert api.plan_get(196, 40) == (False, [5, 2, 32, 0])
+    assert api.plan_get(196, 40) == (False, [5, 2, 32, 4])
     assert api.plan_get(400, 64) == (False, [2, 4, 32, 0])
 
 
@@ -30,7 +30,13 @@ def test_set_get_clear_roundtrip():
     assert api.plan_get(100, 8)[0] is False
 
 
-@pytest.mark.parametrize("plan", [[6, 2, 32, 0], [-1, 2, 32, 0], [0, 5, 32, 0], [0, 2, 0, 0]])
+def test_bstri_group_is_stored():
+    assert api.plan_set(100, 8, [1, 2, 32, 4]) == 0
+    assert api.plan_get(100, 8) == (True, [1, 2, 32, 4])
+
+
+@pytest.mark.parametrize("plan", [[6, 2, 32, 0], [-1, 2, 32, 0], [0, 5, 32, 0], [0, 2, 0, 0],
+                                  [0, 2, 32, 1], [0, 2, 32, 9], [0, 2, 32, -1]])
 def test_invalid_plans_rejected(plan):
     assert api.plan_set(64, 4, plan) == -1
     assert api.plan_get(64, 4)[0] is False
