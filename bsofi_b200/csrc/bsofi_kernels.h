@@ -57,6 +57,11 @@ cudaError_t launch_bsof_persistent(double* A, long long ld, int n, int L, double
 int bstri_recurrence_ctmax(int n, int L);
 cudaError_t launch_bstri_recurrence(double* A, long long ld, const double* W, int n, int L,
                                     int* done, int* next, int* err, cudaStream_t st);
+// The blocked form: grp rows per step, step g's left operand the stacked
+// products at P + g pstep (leading dimension pld), 128x128 tiles.
+cudaError_t launch_bstri_recurrence_blocked(double* A, long long ld, const double* P,
+                                            long long pld, long long pstep, int grp, int n, int L,
+                                            int* done, int* next, int* err, cudaStream_t st);
 
 // Persistent BSOI (kernels_bsoi.cu): all p-1 steps in one launch.
 // done: (L-1) * bsoi_row_bands(N) ints and next: one int, zeroed before;

@@ -4,13 +4,17 @@
 // blocks are inverted and W_i = -X_ii R_{i,i+1}, Z_i = -X_ii R_{i,L-1}
 // X_{L-1,L-1} are formed, row block i of R^{-1} is
 //   X_{i, i+1:L} = W_i X_{i+1, i+1:L}  (+ Z_i on block column L-1),
-// for i = L-3 down to 0.  An output tile of row block i only reads the same
-// columns of row block i+1, so the steps need not wait for each other as a
-// whole: tiles are claimed in (step, column tile, row tile) order from a
-// global counter, and a tile waits (bounded) only for the tiles of the
-// previous step that cover its columns.  Every wait is on a tile claimed
-// earlier, whose CTA is already running, so an ordinary launch cannot
-// deadlock.
+// for i = L-3 down to 0.  The blocked form takes the rows in groups of grp
+// from the bottom (group g: rows t..b, b = L-3-g grp) and computes a whole
+// group from the row below it with the stacked products P of the group:
+//   X_{t:b, b+1:L} = P_g X_{b+1, b+1:L}  (+ Zc on block column L-1);
+// grp = 1 is the one-row recurrence with P_g = W_b.  An output tile of group g
+// only reads the top row block of group g-1 over its own columns, so the steps
+// need not wait for each other as a whole: tiles are claimed in (step, column
+// tile, row tile) order from a global counter, and a tile waits (bounded) only
+// for the top-row tiles of the previous step that cover its columns.  Every
+// wait is on a tile claimed earlier, whose CTA is already running, so an
+// ordinary launch cannot deadlock.
 #include <climits>
 #include "bsofi_common.cuh"
 #include "bsofi_kernels.h"
@@ -20,9 +24,10 @@ namespace bsofi {
 struct RecArgs {
   double* A;
   long long ld;
-  const double* W;  // (L-2) blocks of n x n, leading dimension n
-  int n, L, ctmax;
-  int* done;  // (L-2) x ctmax: finished row tiles per (step, column tile)
+  const double* P;  // step g's left operand: P + g pstep + (grp - m_g) n, leading dimension pld
+  long long pstep, pld;
+  int n, L, grp, ctmax;
+  int* done;  // steps x ctmax: finished top-row tiles per (step, column tile)
   int* next;  // tile counter
   int* err;
   long long spin_limit;
@@ -38,39 +43,52 @@ template <class Cfg, bool ALIGNED>
 __global__ void __launch_bounds__(Cfg::THREADS) bstri_recurrence_kernel(RecArgs s) {
   extern __shared__ __align__(16) double smem_rec[];
   __shared__ int s_tile, s_ok;
-  const int n = s.n, L = s.L;
-  const int RT = (n + Cfg::BM - 1) / Cfg::BM;
-  // Step st (0 .. L-3) computes row block i = L-3-st over (st+2)*n columns.
+  const int n = s.n, L = s.L, grp = s.grp;
+  const int nsteps = (L - 2 + grp - 1) / grp;
+  const int top = (n + Cfg::BM - 1) / Cfg::BM;  // row tiles covering a step's top row block
+  // Step g computes rows t..b (b = L-3-g grp, m = b-t+1 <= grp) over (L-1-b) n columns.
   long long total = 0;
-  for (int st = 0; st < L - 2; st++) total += (long long)RT * (((st + 2) * n + Cfg::BN - 1) / Cfg::BN);
+  for (int g = 0; g < nsteps; g++) {
+    const int b = L - 3 - g * grp, m = b + 1 < grp ? b + 1 : grp;
+    total += (long long)((m * n + Cfg::BM - 1) / Cfg::BM) *
+             (((L - 1 - b) * n + Cfg::BN - 1) / Cfg::BN);
+  }
   for (;;) {
     __syncthreads();  // the previous tile's shared memory is no longer read
     if (threadIdx.x == 0) s_tile = atomicAdd(s.next, 1);
     __syncthreads();
     long long rem = s_tile;
     if (rem >= total) return;
-    int st = 0, ct_n = 0;
-    for (;; st++) {
-      ct_n = ((st + 2) * n + Cfg::BN - 1) / Cfg::BN;
-      if (rem < (long long)RT * ct_n) break;
-      rem -= (long long)RT * ct_n;
+    int g = 0, b = 0, m = 0, rt_n = 0, ct_n = 0;
+    for (;; g++) {
+      b = L - 3 - g * grp;
+      m = b + 1 < grp ? b + 1 : grp;
+      rt_n = (m * n + Cfg::BM - 1) / Cfg::BM;
+      ct_n = ((L - 1 - b) * n + Cfg::BN - 1) / Cfg::BN;
+      if (rem < (long long)rt_n * ct_n) break;
+      rem -= (long long)rt_n * ct_n;
     }
-    const int ct = (int)(rem / RT), rt = (int)(rem % RT);
-    const int i = L - 3 - st, ncol = (st + 2) * n;
-    if (st > 0) {
-      // Columns [ct*BN, ct*BN + BN) of this step are columns shifted by n in
-      // the previous step; those below n lie in the diagonal block X_{i+1,i+1}.
+    const int ct = (int)(rem / rt_n), rt = (int)(rem % rt_n);
+    const int t = b - m + 1, ncol = (L - 1 - b) * n;
+    if (g > 0) {
+      // Columns [ct*BN, ct*BN + BN) of this step are columns shifted by grp n
+      // in the previous step; those below grp n lie in the previous group's
+      // diagonal and in-group blocks, final before this kernel.
       if (threadIdx.x == 0) {
         int ok = 1;
-        const int lo = ct * Cfg::BN - n, hi = ct * Cfg::BN + Cfg::BN - 1 - n;
-        const int prev_cols = (st + 1) * n;
+        const int shift = grp * n;
+        const int lo = ct * Cfg::BN - shift, hi = ct * Cfg::BN + Cfg::BN - 1 - shift;
+        const int prev_cols = ncol - shift;
+        const int pb = b + grp, pm = pb + 1 < grp ? pb + 1 : grp;
+        const int prt = (pm * n + Cfg::BM - 1) / Cfg::BM;
+        const int need = top < prt ? top : prt;
         if (hi >= 0) {
           const int c0 = (lo > 0 ? lo : 0) / Cfg::BN;
           const int c1 = (hi < prev_cols - 1 ? hi : prev_cols - 1) / Cfg::BN;
           for (int c = c0; c <= c1 && ok; c++) {
-            const int* flag = s.done + (long long)(st - 1) * s.ctmax + c;
+            const int* flag = s.done + (long long)(g - 1) * s.ctmax + c;
             long long it = 0;
-            while (rec_ld_acquire(flag) < RT) {
+            while (rec_ld_acquire(flag) < need) {
               if (rec_ld_acquire(s.err) != 0 || ++it > s.spin_limit) {
                 atomicExch(s.err, 1);
                 ok = 0;
@@ -85,11 +103,11 @@ __global__ void __launch_bounds__(Cfg::THREADS) bstri_recurrence_kernel(RecArgs 
       __syncthreads();
       if (!s_ok) return;
     }
-    GemmDims d = {n, ncol, n};
+    GemmDims d = {m * n, ncol, n};
     GemmA a;
-    a.p0 = s.W + (long long)i * n * n;
+    a.p0 = s.P + (long long)g * s.pstep + (long long)(grp - m) * n;
     a.p1 = nullptr;
-    a.ld0 = n;
+    a.ld0 = s.pld;
     a.ld1 = 2;
     a.bs0 = a.bs1 = 0;
     a.ksplit = n;
@@ -97,22 +115,22 @@ __global__ void __launch_bounds__(Cfg::THREADS) bstri_recurrence_kernel(RecArgs 
     a.roff0 = kNoMask;
     a.rlim1 = INT_MAX;
     a.roff1 = kNoMask;
-    // X_{i+1, i+1:L}; its first block is upper triangular (reflectors below).
-    GemmB b = {s.A + cm((long long)(i + 1) * n, (long long)(i + 1) * n, s.ld), s.ld, 0, 0};
+    // X_{b+1, b+1:L}; its first block is upper triangular (reflectors below).
+    GemmB bb = {s.A + cm((long long)(b + 1) * n, (long long)(b + 1) * n, s.ld), s.ld, 0, 0};
     GemmC c;
-    c.p0 = s.A + cm((long long)i * n, (long long)(i + 1) * n, s.ld);
-    c.p1 = s.A + cm((long long)i * n, (long long)(L - 1) * n, s.ld);
+    c.p0 = s.A + cm((long long)t * n, (long long)(b + 1) * n, s.ld);
+    c.p1 = s.A + cm((long long)t * n, (long long)(L - 1) * n, s.ld);
     c.ld0 = c.ld1 = s.ld;
     c.bs0 = c.bs1 = 0;
     c.nsplit = ncol - n;
     c.alpha = 1.0;
     c.beta0 = 0.0;
     c.beta1 = 1.0;
-    gemm_tile<Cfg, ALIGNED>(d, a, b, c, rt * Cfg::BM, ct * Cfg::BN, 0, smem_rec);
+    gemm_tile<Cfg, ALIGNED>(d, a, bb, c, rt * Cfg::BM, ct * Cfg::BN, 0, smem_rec);
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && rt < top) {
       __threadfence();
-      asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(s.done + (long long)st * s.ctmax + ct)
+      asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(s.done + (long long)g * s.ctmax + ct)
                    : "memory");
     }
   }
@@ -120,35 +138,38 @@ __global__ void __launch_bounds__(Cfg::THREADS) bstri_recurrence_kernel(RecArgs 
 
 int bstri_recurrence_ctmax(int n, int L) { return ((L - 1) * n + CfgS::BN - 1) / CfgS::BN; }
 
-template <bool AL>
-static cudaError_t rec_launch(const RecArgs& s, long long tiles, cudaStream_t st) {
+template <class Cfg, bool AL>
+static cudaError_t rec_launch(const RecArgs& s, cudaStream_t st) {
   static PerDevice once;
   const int pend = once.pending();
   if (pend >= 0) {
-    cudaError_t e = cudaFuncSetAttribute(bstri_recurrence_kernel<CfgS, AL>,
+    cudaError_t e = cudaFuncSetAttribute(bstri_recurrence_kernel<Cfg, AL>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)CfgS::SMEM);
+                                         (int)Cfg::SMEM);
     if (e != cudaSuccess) return e;
     once.mark(pend);
+  }
+  long long tiles = 0;
+  for (int g = 0, nsteps = (s.L - 2 + s.grp - 1) / s.grp; g < nsteps; g++) {
+    const int b = s.L - 3 - g * s.grp, m = b + 1 < s.grp ? b + 1 : s.grp;
+    tiles += (long long)((m * s.n + Cfg::BM - 1) / Cfg::BM) *
+             (((s.L - 1 - b) * s.n + Cfg::BN - 1) / Cfg::BN);
   }
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bstri_recurrence_kernel<CfgS, AL>,
-                                                CfgS::THREADS, CfgS::SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bstri_recurrence_kernel<Cfg, AL>,
+                                                Cfg::THREADS, Cfg::SMEM);
   long long grid = (long long)sms * (per > 0 ? per : 1);
   if (tiles < grid) grid = tiles;
-  bstri_recurrence_kernel<CfgS, AL><<<(int)grid, CfgS::THREADS, CfgS::SMEM, st>>>(s);
+  bstri_recurrence_kernel<Cfg, AL><<<(int)grid, Cfg::THREADS, Cfg::SMEM, st>>>(s);
   return cudaGetLastError();
 }
 
-cudaError_t launch_bstri_recurrence(double* A, long long ld, const double* W, int n, int L,
-                                    int* done, int* next, int* err, cudaStream_t st) {
-  if (L < 3) return cudaSuccess;
+static RecArgs rec_args(double* A, long long ld, int n, int L, int* done, int* next, int* err) {
   RecArgs s;
   s.A = A;
   s.ld = ld;
-  s.W = W;
   s.n = n;
   s.L = L;
   s.ctmax = bstri_recurrence_ctmax(n, L);
@@ -156,11 +177,34 @@ cudaError_t launch_bstri_recurrence(double* A, long long ld, const double* W, in
   s.next = next;
   s.err = err;
   s.spin_limit = 1ll << 22;
-  const int RT = (n + CfgS::BM - 1) / CfgS::BM;
-  long long tiles = 0;
-  for (int k = 0; k < L - 2; k++) tiles += (long long)RT * (((k + 2) * n + CfgS::BN - 1) / CfgS::BN);
+  return s;
+}
+
+cudaError_t launch_bstri_recurrence(double* A, long long ld, const double* W, int n, int L,
+                                    int* done, int* next, int* err, cudaStream_t st) {
+  if (L < 3) return cudaSuccess;
+  RecArgs s = rec_args(A, ld, n, L, done, next, err);
+  // One row per step: step g uses W_{L-3-g}.
+  s.grp = 1;
+  s.P = W + (long long)(L - 3) * n * n;
+  s.pstep = -(long long)n * n;
+  s.pld = n;
   const bool al = ((uintptr_t)A % 16 == 0) && ((uintptr_t)W % 16 == 0) && ld % 2 == 0 && n % 2 == 0;
-  return al ? rec_launch<true>(s, tiles, st) : rec_launch<false>(s, tiles, st);
+  return al ? rec_launch<CfgS, true>(s, st) : rec_launch<CfgS, false>(s, st);
+}
+
+cudaError_t launch_bstri_recurrence_blocked(double* A, long long ld, const double* P,
+                                            long long pld, long long pstep, int grp, int n, int L,
+                                            int* done, int* next, int* err, cudaStream_t st) {
+  if (L < 3) return cudaSuccess;
+  RecArgs s = rec_args(A, ld, n, L, done, next, err);
+  s.grp = grp;
+  s.P = P;
+  s.pstep = pstep;
+  s.pld = pld;
+  const bool al = ((uintptr_t)A % 16 == 0) && ((uintptr_t)P % 16 == 0) && ld % 2 == 0 &&
+                  n % 2 == 0 && pld % 2 == 0 && pstep % 2 == 0;
+  return al ? rec_launch<CfgM, true>(s, st) : rec_launch<CfgM, false>(s, st);
 }
 
 }  // namespace bsofi

@@ -49,7 +49,8 @@ thread_local GemmTimer g_timer;
 // row recurrence (launch_gemm's cfg per step, or 4: one persistent launch),
 // the number of BSOF worker CTAs of a single inversion, and the BSTRI row
 // group (0: one recurrence step per block row; 2..8: that many block rows per
-// step of the blocked recurrence, which then replaces bstri_cfg).  Tuned plans
+// step of the blocked recurrence, one persistent launch when bstri_cfg is 4,
+// else one launch per group).  Tuned plans
 // (bsofi_autotune) live in a process-wide table; other sizes use the default
 // below.
 struct Plan {
@@ -66,9 +67,10 @@ Plan default_plan(int n, int L) {
   // mid-size N (100/64, 196/40, 324/40), per-step launches for N of 20k and
   // more (400/64, 576/80) and for small N (64/16, 144/20).  The persistent
   // recurrence helped at 64/16 and 400/64 and tied elsewhere.  The blocked
-  // BSTRI recurrence with 4 rows per step gained 1-7% below N = 20000
-  // (256/32, 196/40, 100/64), 2 rows at 64/16; at 400/64 every group size
-  // lost to the persistent one-row recurrence.
+  // BSTRI recurrence, persistent with 4 rows per step, gained 2-7% for N
+  // between 2048 and 20000 (256/32, 196/40, 100/64, 324/40); at 64/16 one
+  // launch per group of 2 rows was best; at 400/64 no group size beat the
+  // persistent one-row recurrence.
   const int N = n * L;
   const int tiles = ((N + 127) / 128) * ((2 * n + 127) / 128);
   int bsoi;
@@ -76,8 +78,17 @@ Plan default_plan(int n, int L) {
   else if (N >= 20000) bsoi = 2;
   else if (N >= 4000) bsoi = 5;
   else bsoi = 1;
-  const int rec = (N <= 2048 || (N >= 20000 && N < 40000)) ? 4 : 2;
-  const int group = N >= 20000 ? 0 : (N <= 2048 ? 2 : 4);
+  int rec, group;
+  if (N <= 2048) {
+    rec = 2;
+    group = 2;
+  } else if (N < 20000) {
+    rec = 4;
+    group = 4;
+  } else {
+    rec = N < 40000 ? 4 : 2;
+    group = 0;
+  }
   return Plan{bsoi, rec, 32, group};
 }
 
@@ -250,7 +261,7 @@ int run_bsof(int n, int L, double* dA, int ldd, double* dtau, void* ws, cudaStre
 // uses the bottom rows of its block) lives in the BSOI carry buffers, which
 // are idle until BSOI.
 int bstri_blocked(int n, int L, double* dA, int ldd, const double* W, double* P, int grp,
-                  cudaStream_t st) {
+                  bool persistent, int* rsync, int rsync_ints, int* err, cudaStream_t st) {
   const long long nn = (long long)n * n;
   const int b0 = L - 3;
   const int ngr = (L - 2 + grp - 1) / grp;
@@ -316,6 +327,13 @@ int bstri_blocked(int n, int L, double* dA, int ldd, const double* W, double* P,
       c.beta0 = 1.0;
       CK(launch_gemm(d1, a, b, c, batch, 2, st));
     }
+  }
+  if (persistent) {
+    // All group steps in one launch, column tiles pipelined across the steps.
+    CKM(cudaMemsetAsync(rsync, 0, sizeof(int) * rsync_ints, st));
+    CK(launch_bstri_recurrence_blocked(dA, ldd, P, pld, pbs, grp, n, L, rsync,
+                                       rsync + rsync_ints - 2, err, st));
+    return 0;
   }
   // Group steps, bottom to top.
   for (int g = 0; g < ngr; g++) {
@@ -429,7 +447,9 @@ int run_bstri(int n, int L, double* dA, int ldd, void* ws, cudaStream_t st) {
   // At most L-2 rows per group: the stacked P then takes at most (2L-5) n^2
   // doubles, inside the two carry buffers (2 ldd n >= 2 L n^2).
   const int grp = plan.bstri_group < L - 2 ? plan.bstri_group : L - 2;
-  if (grp >= 2) return bstri_blocked(n, L, dA, ldd, W, at<double>(ws, ly.C0), grp, st);
+  if (grp >= 2)
+    return bstri_blocked(n, L, dA, ldd, W, at<double>(ws, ly.C0), grp, rec == 4,
+                         at<int>(ws, ly.rsync), ly.rsync_ints, info + 3, st);
   if (rec == 4) {
     // One persistent launch, column tiles pipelined across the steps.
     if (L >= 3) {

@@ -237,7 +237,8 @@ void bsofi_batch_graph_destroy(bsofi_batch_graph *graph);
  * a single inversion, [3] the BSTRI row group: 0 one recurrence step per
  * block row, g in 2..8 the blocked recurrence with g block rows per step
  * (products of g consecutive W_i formed for all groups at once, then one
- * GEMM of g n rows per group; [1] is then unused).
+ * GEMM of g n rows per group: all groups in one persistent launch of 128x128
+ * tiles when [1] is 4, else one launch per group).
  * Every inversion of block size n with L blocks uses the tuned plan of (n, L)
  * if there is one, else a default fitted to the sizes tuned on a B200
  * (bsofi_plan_get shows it).  bsofi_autotune times the candidates one knob at a time on a

@@ -22,14 +22,18 @@ def _clear_plans():
     api.plan_clear()
 
 
+@pytest.mark.parametrize("persistent", [False, True], ids=["per_group", "persistent"])
 @pytest.mark.parametrize("n,L,grp", [(5, 4, 2), (7, 9, 3), (16, 10, 4), (33, 7, 8), (31, 3, 4),
-                                     (64, 16, 4), (100, 12, 6), (65, 13, 5), (256, 8, 4)])
-def test_blocked_recurrence_matches_oracle(cuda_device, n, L, grp):
+                                     (64, 16, 4), (100, 12, 6), (65, 13, 5), (256, 8, 4),
+                                     (130, 20, 3)])
+def test_blocked_recurrence_matches_oracle(cuda_device, n, L, grp, persistent):
+    """persistent: all group steps in one launch (plan [1] = 4), tiles
+    waiting on the previous group's top row tiles; else one launch per group."""
     M = random_pcyclic(n, L, seed=9000 + 13 * n + L)
     X0, S0, T0, info0 = api.invert(M, n, L)  # default plan
     assert info0 == 0
     _, plan = api.plan_get(n, L)
-    assert api.plan_set(n, L, plan[:3] + [grp]) == 0
+    assert api.plan_set(n, L, [plan[0], 4 if persistent else 2, plan[2], grp]) == 0
     X, S, T, info = api.invert(M, n, L)
     assert info == 0
     np.testing.assert_array_equal(T, T0)

@@ -13,12 +13,12 @@ def _clear_plans():
 
 def test_default_plan_follows_the_tuned_sizes():
     # 2n = 512 fills 128-wide tiles and 256 tiles per step: persistent 128x128.
-    assert api.plan_get(256, 32) == (False, [0, 2, 32, 4])
-    # Small N: one GEMM launch per step; persistent recurrence for N <= 2048.
-    assert api.plan_get(144, 20) == (False, [1, 2, 32, 4])
-    assert api.plan_get(64, 16) == (False, [1, 4, 32, 2])
+    assert api.plan_get(256, 32) == (False, [0, 4, 32, 4])
+    # Small N: one GEMM launch per BSOI step; BSTRI in groups of 2 rows.
+    assert api.plan_get(144, 20) == (False, [1, 4, 32, 4])
+    assert api.plan_get(64, 16) == (False, [1, 2, 32, 2])
     # 2n = 392: 64x64 tiles, persistent for mid-size N, per step for N >= 20k.
-    assert api.plan_get(196, 40) == (False, [5, 2, 32, 4])
+    assert api.plan_get(196, 40) == (False, [5, 4, 32, 4])
     assert api.plan_get(400, 64) == (False, [2, 4, 32, 0])
 
 
