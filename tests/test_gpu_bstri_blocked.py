@@ -47,3 +47,33 @@ def test_blocked_recurrence_matches_oracle(cuda_device, n, L, grp, persistent):
     assert rel_fro(up, rup) < tol
     assert rel_fro(X, Xr) < tol
     assert residual(M, X) < 1e-13
+
+
+@pytest.mark.parametrize("n,L", [(324, 20), (400, 12), (196, 40)])
+def test_default_blocked_plan_vs_reference(cuda_device, n, L):
+    """Sizes whose default plan runs the persistent blocked recurrence with
+    block rows that 128-row tiles straddle (n = 324, 400, 196), against the
+    compiled reference CPU path."""
+    _, plan = api.plan_get(n, L)
+    assert plan[1] == 4 and plan[3] == 4
+    M = random_pcyclic(n, L, seed=4400 + n + L)
+    if oracle.ref_available():
+        oracle.set_ref_threads(8)
+        Ar, taur, _ = oracle.ref_bsoftri(M, n, L)
+        Xr, _ = oracle.ref_bsoi(Ar, taur, n, L)
+    else:
+        Ar, taur, _ = oracle.port_bsoftri(M, n, L)
+        Xr, _ = oracle.port_bsoi(Ar, taur, n, L)
+    X, S, T, info = api.invert(M, n, L)
+    assert info == 0
+    np.testing.assert_allclose(T, taur, rtol=0, atol=1e-12)
+    up, _ = split_state(S, n, L)
+    rup, _ = split_state(Ar, n, L)
+    tol = inverse_tolerance(M, Xr)
+    assert rel_fro(up, rup) < tol
+    assert rel_fro(X, Xr) < tol
+    import torch
+    from bsofi_b200.hubbard import pcyclic_blocks
+    from gpu_util import block_residual_gpu
+    Xd = torch.from_numpy(np.ascontiguousarray(X)).to(cuda_device)
+    assert block_residual_gpu(torch, *pcyclic_blocks(M, n, L), Xd) < 1e-13

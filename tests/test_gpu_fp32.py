@@ -173,3 +173,19 @@ def test_hubbard_n256_p32_vs_fp32_reference(cuda_device):
     X, state, tau, info = fp32.invert(M32, n, L)
     assert info == 0
     _check_vs_fp32_reference(M32, n, L, X, state, tau, Ar, taur, Xr)
+
+
+@pytest.mark.parametrize("L", [2, 3])
+def test_largest_block_size_fp32(cuda_device, L):
+    """n = BSOFI_MAX_BLOCK (768) through the single-precision library against
+    the reference's single-precision build."""
+    if not oracle.ref32_available():
+        pytest.skip("FP32 reference library not built")
+    n = 768
+    M32 = random_pcyclic(n, L, seed=7680 + L).astype(np.float32)
+    oracle.set_ref_threads(8, kind="ref32")
+    Ar, taur, _ = oracle.ref32_bsoftri(M32, n, L)
+    Xr, _ = oracle.ref32_bsoi(Ar, taur, n, L)
+    X, state, tau, info = fp32.invert(M32, n, L)
+    assert info == 0
+    _check_vs_fp32_reference(M32, n, L, X, state, tau, Ar, taur, Xr)
