@@ -86,6 +86,7 @@ _SIGS = {
     "bsofi_device_bsof_timeline": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
                                                   _vp, ctypes.c_int]),
     "bsofi_device_set_bsof_workers": (None, [ctypes.c_int]),
+    "bsofi_device_set_bstri_overlap": (None, [ctypes.c_int]),
     "bsofi_device_timing": (None, [ctypes.c_int]),
     "bsofi_device_timing_read": (ctypes.c_int, [_c_dbl_p, ctypes.POINTER(ctypes.c_longlong)]),
     "bsofi_selftest_gemm": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,

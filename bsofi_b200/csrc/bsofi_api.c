@@ -1029,3 +1029,5 @@ int bsofi_device_bsof_timeline(int n, int L, int ldda, void *dwork, unsigned lon
 }
 
 void bsofi_device_set_bsof_workers(int workers) { bsofi_dev_set_bsof_workers(workers); }
+
+void bsofi_device_set_bstri_overlap(int on) { bsofi_dev_set_bstri_overlap(on); }

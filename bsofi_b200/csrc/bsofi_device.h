@@ -110,6 +110,9 @@ int bsofi_dev_timing_read(double *ms, long long *launches);
  * number of leaves. */
 int bsofi_dev_bsof_timeline(int n, int L, int ldd, void *dws, unsigned long long **ptr);
 void bsofi_dev_set_bsof_workers(int w);
+/* Overlap of BSTRI's leading rows with the end of BSOF in single inversions
+ * (1, the default) or the two phases in order (0); process-wide. */
+void bsofi_dev_set_bstri_overlap(int on);
 
 /* One call of the FP64 tile engine (diagnostics). */
 int bsofi_dev_selftest_gemm(int M, int N, int K, double alpha, const double *dA, int lda,

@@ -44,13 +44,16 @@ cudaError_t launch_wy_apply(const WyArgs& a, int batch, cudaStream_t st);
 // Persistent BSOF (kernels_bsof.cu).  cnt: (L + 2(L-1))*tiles ints,
 // factored: leaves ints, next_task and err: one int each, all zeroed before
 // the launch.  G (optional): (L-1) x (2n)^2 identity matrices that become
-// Q_k^T.
+// Q_k^T.  [s_begin, s_end): the leaves this launch factors (-1: to the end);
+// a later launch continues with the counters the earlier one left, after
+// next_task is zeroed again.
 int bsof_leaf_width(int n);
 int bsof_tiles(int n);
 cudaError_t launch_bsof_persistent(double* A, long long ld, int n, int L, double* tau, double* T,
                                    double* G, int maxleaves, int* cnt, int* factored,
                                    int* next_task, int* err, unsigned long long* timeline,
-                                   int workers, cudaStream_t st);
+                                   int workers, cudaStream_t st, int s_begin = 0,
+                                   int s_end = -1);
 
 // Persistent BSTRI row recurrence (kernels_bstri.cu): done is (L-2) x
 // bstri_recurrence_ctmax(n, L) ints and next one int, zeroed before.
@@ -58,10 +61,12 @@ int bstri_recurrence_ctmax(int n, int L);
 cudaError_t launch_bstri_recurrence(double* A, long long ld, const double* W, int n, int L,
                                     int* done, int* next, int* err, cudaStream_t st);
 // The blocked form: grp rows per step, step g's left operand the stacked
-// products at P + g pstep (leading dimension pld), 128x128 tiles.
+// products at P + g pstep (leading dimension pld), 128x128 tiles; block
+// columns left of hfloor are not computed (already final).
 cudaError_t launch_bstri_recurrence_blocked(double* A, long long ld, const double* P,
                                             long long pld, long long pstep, int grp, int n, int L,
-                                            int* done, int* next, int* err, cudaStream_t st);
+                                            int* done, int* next, int* err, cudaStream_t st,
+                                            int hfloor = 0);
 
 // Persistent BSOI (kernels_bsoi.cu): all p-1 steps in one launch.
 // done: (L-1) * bsoi_row_bands(N) ints and next: one int, zeroed before;
@@ -72,9 +77,10 @@ cudaError_t launch_bsoi_persistent(double* A, long long ld, double* carry0, doub
                                    int* next, int* err, bool small, cudaStream_t st);
 
 // In-place inversion of the upper triangles of nblk n x n blocks (block b at
-// A + b * bstride); tmp: device scratch of nblk * n * n / 4 doubles.
+// A + b * bstride); tmp: device scratch of nblk * n * n / 4 doubles.  A zero
+// diagonal is reported as the global index of diagonal block boff + b.
 cudaError_t launch_trtri_blocks(double* A, long long ld, int n, long long bstride,
-                                int nblk, int* info, double* tmp, cudaStream_t st);
+                                int nblk, int* info, double* tmp, cudaStream_t st, int boff = 0);
 
 // cfg: 0 = choose by tile count, 1 = 128x128 (K stage 16), 2 = 64x64, 3 = 128x128 (K stage 32).
 cudaError_t launch_gemm(const GemmDims& d, const GemmA& a, const GemmB& b,

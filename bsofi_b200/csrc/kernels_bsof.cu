@@ -171,6 +171,10 @@ struct BsofState {
   int* err;       // 0 ok; 1 timeout
   long long spin_limit;
   unsigned long long* timeline;  // 4 stamps per leaf from the panel CTA (diagnostics)
+  // This launch factors leaves [s_begin, s_end) and runs their worker tasks;
+  // the per-tile and per-leaf counters carry over from an earlier launch of
+  // the leaves before s_begin, whose updates are then all done.
+  int s_begin, s_end;
 };
 
 BSOFI_DEVINL unsigned long long gtimer() {
@@ -656,7 +660,8 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
   __shared__ Smem<NB> sm;
   extern __shared__ __align__(16) double sC[];  // NB x (R*BT) staged tile
   const int tid = threadIdx.x;
-  const long long total_tasks = tasks_before(g, g.S);
+  const long long first_task = tasks_before(g, st.s_begin);
+  const long long total_tasks = tasks_before(g, st.s_end);
 
   if (blockIdx.x == 0) {
     // ---------------------------------------------------------- panel chain
@@ -670,9 +675,12 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
     constexpr bool PREFETCH = NB == 16 && FW < BW && Pass<R>::NP == 1;
     const int warp = tid >> 5;
     // own: this CTA applied the last update to the current leaf's tile, so it
-    // needs no wait (shared barriers order its own global writes).
-    bool own = false;
-    for (int s = 0; s < g.S; s++) {
+    // needs no wait (shared barriers order its own global writes).  A launch
+    // that continues at s_begin > 0 starts owning its first tile: the earlier
+    // launch, complete before this one starts, applied that tile's last
+    // update from its panel CTA, which is never counted.
+    bool own = st.s_begin > 0;
+    for (int s = st.s_begin; s < st.s_end; s++) {
       const Leaf f = leaf_of(g, s);
       int lo, hi;
       tile_range(g, f.m, f.t, lo, hi);
@@ -787,7 +795,7 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
 
   // ------------------------------------------------------------ workers
   for (;;) {
-    if (tid == 0) sm.task = atomicAdd(st.next_task, 1);
+    if (tid == 0) sm.task = first_task + atomicAdd(st.next_task, 1);
     __syncthreads();
     const long long task = sm.task;
     __syncthreads();
@@ -870,7 +878,7 @@ static int max_grid() {
 cudaError_t launch_bsof_persistent(double* A, long long ld, int n, int L, double* tau, double* T,
                                    double* G, int maxleaves, int* cnt, int* factored,
                                    int* next_task, int* err, unsigned long long* timeline,
-                                   int workers, cudaStream_t st) {
+                                   int workers, cudaStream_t st, int s_begin, int s_end) {
   BsofGeom g;
   g.form_g = G != nullptr;
   g.n = n;
@@ -891,6 +899,9 @@ cudaError_t launch_bsof_persistent(double* A, long long ld, int n, int L, double
   s.err = err;
   s.timeline = timeline;
   s.spin_limit = 1ll << 22;  // polls of ~0.5 us each: a few seconds at most
+  s.s_begin = s_begin > 0 ? s_begin : 0;
+  s.s_end = (s_end < 0 || s_end > g.S) ? g.S : s_end;
+  if (s.s_begin >= s.s_end) return cudaSuccess;
   const int R = (2 * n + BT - 1) / BT;
   int grid = 1 + workers;
   if (g.NB == 16) {

@@ -8,7 +8,10 @@
 // from the bottom (group g: rows t..b, b = L-3-g grp) and computes a whole
 // group from the row below it with the stacked products P of the group:
 //   X_{t:b, b+1:L} = P_g X_{b+1, b+1:L}  (+ Zc on block column L-1);
-// grp = 1 is the one-row recurrence with P_g = W_b.  An output tile of group g
+// grp = 1 is the one-row recurrence with P_g = W_b.  With a column floor h
+// > 0 a step only computes block columns from max(b+1, h) on (the columns
+// left of h were formed earlier, overlapped with the factorization).  An
+// output tile of group g
 // only reads the top row block of group g-1 over its own columns, so the steps
 // need not wait for each other as a whole: tiles are claimed in (step, column
 // tile, row tile) order from a global counter, and a tile waits (bounded) only
@@ -27,6 +30,7 @@ struct RecArgs {
   const double* P;  // step g's left operand: P + g pstep + (grp - m_g) n, leading dimension pld
   long long pstep, pld;
   int n, L, grp, ctmax;
+  int hfloor;  // first block column computed (0: every column beyond the step's rows)
   int* done;  // steps x ctmax: finished top-row tiles per (step, column tile)
   int* next;  // tile counter
   int* err;
@@ -46,12 +50,13 @@ __global__ void __launch_bounds__(Cfg::THREADS) bstri_recurrence_kernel(RecArgs 
   const int n = s.n, L = s.L, grp = s.grp;
   const int nsteps = (L - 2 + grp - 1) / grp;
   const int top = (n + Cfg::BM - 1) / Cfg::BM;  // row tiles covering a step's top row block
-  // Step g computes rows t..b (b = L-3-g grp, m = b-t+1 <= grp) over (L-1-b) n columns.
+  // Step g computes rows t..b (b = L-3-g grp, m = b-t+1 <= grp) over block
+  // columns cs..L-1, cs = max(b+1, hfloor).
   long long total = 0;
   for (int g = 0; g < nsteps; g++) {
     const int b = L - 3 - g * grp, m = b + 1 < grp ? b + 1 : grp;
-    total += (long long)((m * n + Cfg::BM - 1) / Cfg::BM) *
-             (((L - 1 - b) * n + Cfg::BN - 1) / Cfg::BN);
+    const int cs = b + 1 > s.hfloor ? b + 1 : s.hfloor;
+    total += (long long)((m * n + Cfg::BM - 1) / Cfg::BM) * (((L - cs) * n + Cfg::BN - 1) / Cfg::BN);
   }
   for (;;) {
     __syncthreads();  // the previous tile's shared memory is no longer read
@@ -59,27 +64,30 @@ __global__ void __launch_bounds__(Cfg::THREADS) bstri_recurrence_kernel(RecArgs 
     __syncthreads();
     long long rem = s_tile;
     if (rem >= total) return;
-    int g = 0, b = 0, m = 0, rt_n = 0, ct_n = 0;
+    int g = 0, b = 0, m = 0, cs = 0, rt_n = 0, ct_n = 0;
     for (;; g++) {
       b = L - 3 - g * grp;
       m = b + 1 < grp ? b + 1 : grp;
+      cs = b + 1 > s.hfloor ? b + 1 : s.hfloor;
       rt_n = (m * n + Cfg::BM - 1) / Cfg::BM;
-      ct_n = ((L - 1 - b) * n + Cfg::BN - 1) / Cfg::BN;
+      ct_n = ((L - cs) * n + Cfg::BN - 1) / Cfg::BN;
       if (rem < (long long)rt_n * ct_n) break;
       rem -= (long long)rt_n * ct_n;
     }
     const int ct = (int)(rem / rt_n), rt = (int)(rem % rt_n);
-    const int t = b - m + 1, ncol = (L - 1 - b) * n;
+    const int t = b - m + 1, ncol = (L - cs) * n;
     if (g > 0) {
-      // Columns [ct*BN, ct*BN + BN) of this step are columns shifted by grp n
-      // in the previous step; those below grp n lie in the previous group's
-      // diagonal and in-group blocks, final before this kernel.
+      // Columns [ct*BN, ct*BN + BN) of this step are columns shifted by
+      // (cs_prev - cs) n in the previous step; those left of the previous
+      // step's first column lie in the previous group's diagonal and in-group
+      // blocks (or left of the floor), final before this kernel.
       if (threadIdx.x == 0) {
         int ok = 1;
-        const int shift = grp * n;
-        const int lo = ct * Cfg::BN - shift, hi = ct * Cfg::BN + Cfg::BN - 1 - shift;
-        const int prev_cols = ncol - shift;
         const int pb = b + grp, pm = pb + 1 < grp ? pb + 1 : grp;
+        const int pcs = pb + 1 > s.hfloor ? pb + 1 : s.hfloor;
+        const int shift = (pcs - cs) * n;
+        const int lo = ct * Cfg::BN - shift, hi = ct * Cfg::BN + Cfg::BN - 1 - shift;
+        const int prev_cols = (L - pcs) * n;
         const int prt = (pm * n + Cfg::BM - 1) / Cfg::BM;
         const int need = top < prt ? top : prt;
         if (hi >= 0) {
@@ -115,10 +123,12 @@ __global__ void __launch_bounds__(Cfg::THREADS) bstri_recurrence_kernel(RecArgs 
     a.roff0 = kNoMask;
     a.rlim1 = INT_MAX;
     a.roff1 = kNoMask;
-    // X_{b+1, b+1:L}; its first block is upper triangular (reflectors below).
-    GemmB bb = {s.A + cm((long long)(b + 1) * n, (long long)(b + 1) * n, s.ld), s.ld, 0, 0};
+    // X_{b+1, cs:L}; when cs = b+1 its first block is upper triangular
+    // (reflectors below).
+    GemmB bb = {s.A + cm((long long)(b + 1) * n, (long long)cs * n, s.ld), s.ld, 0,
+                cs == b + 1 ? 0 : kNoMask};
     GemmC c;
-    c.p0 = s.A + cm((long long)t * n, (long long)(b + 1) * n, s.ld);
+    c.p0 = s.A + cm((long long)t * n, (long long)cs * n, s.ld);
     c.p1 = s.A + cm((long long)t * n, (long long)(L - 1) * n, s.ld);
     c.ld0 = c.ld1 = s.ld;
     c.bs0 = c.bs1 = 0;
@@ -152,8 +162,9 @@ static cudaError_t rec_launch(const RecArgs& s, cudaStream_t st) {
   long long tiles = 0;
   for (int g = 0, nsteps = (s.L - 2 + s.grp - 1) / s.grp; g < nsteps; g++) {
     const int b = s.L - 3 - g * s.grp, m = b + 1 < s.grp ? b + 1 : s.grp;
+    const int cs = b + 1 > s.hfloor ? b + 1 : s.hfloor;
     tiles += (long long)((m * s.n + Cfg::BM - 1) / Cfg::BM) *
-             (((s.L - 1 - b) * s.n + Cfg::BN - 1) / Cfg::BN);
+             (((s.L - cs) * s.n + Cfg::BN - 1) / Cfg::BN);
   }
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
@@ -177,6 +188,7 @@ static RecArgs rec_args(double* A, long long ld, int n, int L, int* done, int* n
   s.next = next;
   s.err = err;
   s.spin_limit = 1ll << 22;
+  s.hfloor = 0;
   return s;
 }
 
@@ -195,10 +207,12 @@ cudaError_t launch_bstri_recurrence(double* A, long long ld, const double* W, in
 
 cudaError_t launch_bstri_recurrence_blocked(double* A, long long ld, const double* P,
                                             long long pld, long long pstep, int grp, int n, int L,
-                                            int* done, int* next, int* err, cudaStream_t st) {
+                                            int* done, int* next, int* err, cudaStream_t st,
+                                            int hfloor) {
   if (L < 3) return cudaSuccess;
   RecArgs s = rec_args(A, ld, n, L, done, next, err);
   s.grp = grp;
+  s.hfloor = hfloor;
   s.P = P;
   s.pstep = pstep;
   s.pld = pld;

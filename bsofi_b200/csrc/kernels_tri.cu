@@ -24,10 +24,11 @@ constexpr int TLEAF = 32;
 
 // One warp inverts one leaf (rows/columns [32 l, 32 l + w) of block b).  An
 // exactly zero diagonal entry leaves the leaf as it is and records the
-// smallest 1-based global index (block * n + i + 1) in *info; the block's
+// smallest 1-based global index ((boff + block) * n + i + 1) in *info; the block's
 // inverse is then not formed.
 __global__ void __launch_bounds__(128) trtri_leaves_kernel(double* A, long long ld, int n,
-                                                           long long bstride, int nblk, int* info) {
+                                                           long long bstride, int nblk, int* info,
+                                                           int boff) {
   __shared__ double sU[4][TLEAF][TLEAF + 1];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nleaf = (n + TLEAF - 1) / TLEAF;
@@ -42,7 +43,7 @@ __global__ void __launch_bounds__(128) trtri_leaves_kernel(double* A, long long 
   __syncwarp();
   const unsigned zero = __ballot_sync(0xffffffffu, lane < w && X[lane][lane] == 0.0);
   if (zero != 0u) {
-    if (lane == __ffs(zero) - 1) atomicMin(info, b * n + o + lane + 1);
+    if (lane == __ffs(zero) - 1) atomicMin(info, (boff + b) * n + o + lane + 1);
     return;
   }
   // dtrti2 ('U'): X(j,j) = 1/U(j,j), X(0:j,j) = -X(j,j) X(0:j,0:j) U(0:j,j).
@@ -76,10 +77,10 @@ void tri_nodes(int off, int size, std::vector<TriNode>& out) {
 }  // namespace
 
 cudaError_t launch_trtri_blocks(double* A, long long ld, int n, long long bstride, int nblk,
-                                int* info, double* tmp, cudaStream_t st) {
+                                int* info, double* tmp, cudaStream_t st, int boff) {
   if (nblk <= 0 || n <= 0) return cudaSuccess;
   const long long leaves = (long long)nblk * ((n + TLEAF - 1) / TLEAF);
-  trtri_leaves_kernel<<<(int)((leaves + 3) / 4), 128, 0, st>>>(A, ld, n, bstride, nblk, info);
+  trtri_leaves_kernel<<<(int)((leaves + 3) / 4), 128, 0, st>>>(A, ld, n, bstride, nblk, info, boff);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   std::vector<TriNode> nodes;

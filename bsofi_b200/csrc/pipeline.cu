@@ -11,6 +11,7 @@
 //   Y      (L-1) x (n x n)          BSTRI scratch  R_{i,L-1} R_{L-1,L-1}^{-1}
 //   carry  2 x (ldd x n)            BSOI ping-pong block column
 #include <climits>
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <utility>
@@ -260,51 +261,76 @@ int run_bsof(int n, int L, double* dA, int ldd, double* dtau, void* ws, cudaStre
 // taller.  P (grp n x n per group, leading dimension grp n; a short top group
 // uses the bottom rows of its block) lives in the BSOI carry buffers, which
 // are idle until BSOI.
-int bstri_blocked(int n, int L, double* dA, int ldd, const double* W, double* P, int grp,
-                  bool persistent, int* rsync, int rsync_ints, int* err, cudaStream_t st) {
-  const long long nn = (long long)n * n;
-  const int b0 = L - 3;
-  const int ngr = (L - 2 + grp - 1) / grp;
-  const int mlast = (L - 2) - (ngr - 1) * grp;
-  const long long pld = (long long)grp * n, pbs = pld * n;
-  const long long rstep = -(long long)grp * n;  // row offset from one group to the next
+struct RowGroups {
+  int n, L, grp, ngr, mlast, b0;
+  long long nn, pld, pbs;
+  RowGroups(int n_, int L_, int grp_) : n(n_), L(L_), grp(grp_) {
+    b0 = L - 3;
+    ngr = (L - 2 + grp - 1) / grp;
+    mlast = (L - 2) - (ngr - 1) * grp;
+    nn = (long long)n * n;
+    pld = (long long)grp * n;
+    pbs = pld * n;
+  }
+  int b(int g) const { return b0 - g * grp; }
+  int m(int g) const { return b(g) + 1 < grp ? b(g) + 1 : grp; }
+  int t(int g) const { return b(g) - m(g) + 1; }
+};
+
+GemmA plain_a(const double* p, long long ld, long long bs) {
+  GemmA a = {};
+  a.p0 = p;
+  a.ld0 = ld;
+  a.bs0 = bs;
+  a.ld1 = 2;
+  a.rlim0 = INT_MAX;
+  a.roff0 = kNoMask;
+  a.rlim1 = INT_MAX;
+  a.roff1 = kNoMask;
+  return a;
+}
+
+// P_b = W_b at the bottom of the blocks of groups [g0, g1).
+int groups_seed(const RowGroups& G, const double* W, double* P, int g0, int g1, cudaStream_t st) {
+  for (int g = g0; g < g1; g++)
+    CKM(cudaMemcpy2DAsync(P + g * G.pbs + (long long)(G.grp - 1) * G.n, sizeof(double) * G.pld,
+                          W + (long long)G.b(g) * G.nn, sizeof(double) * G.n,
+                          sizeof(double) * G.n, G.n, cudaMemcpyDeviceToDevice, st));
+  return 0;
+}
+
+enum { kRoundP = 1, kRoundIntra = 2, kRoundZc = 4 };
+
+// The in-group rounds of groups [g0, g1): round q forms, for row r = b_g - q
+// of every group that has it, P_r (kRoundP), X_{r, r+1:r+q} (kRoundIntra) and
+// Zc_r in place in block column L-1 (kRoundZc), batched over the groups.
+int groups_rounds(const RowGroups& G, double* dA, int ldd, const double* W, double* P, int g0,
+                  int g1, int what, cudaStream_t st) {
+  const int n = G.n, grp = G.grp, L = G.L;
+  const long long rstep = -(long long)grp * n;             // row offset from one group to the next
   const long long dstep = rstep + rstep * (long long)ldd;  // the same along the diagonal
-  // P_b = W_b at the bottom of every group's block.
-  for (int g = 0; g < ngr; g++)
-    CKM(cudaMemcpy2DAsync(P + g * pbs + (long long)(grp - 1) * n, sizeof(double) * pld,
-                          W + (long long)(b0 - g * grp) * nn, sizeof(double) * n,
-                          sizeof(double) * n, n, cudaMemcpyDeviceToDevice, st));
   for (int q = 1; q < grp; q++) {
-    // Row r = b_g - q of every group that has it.
-    const int batch = mlast > q ? ngr : ngr - 1;
+    // Only the top group (ngr - 1) can be short.
+    const int batch = (g1 - g0) - ((g1 == G.ngr && G.mlast <= q) ? 1 : 0);
     if (batch <= 0) break;
-    const int r = b0 - q;  // in group 0
+    const int r = G.b(g0) - q;  // in group g0
     GemmDims d1 = {n, n, n};
-    GemmA a = {};
-    a.p0 = W + (long long)r * nn;
-    a.ld0 = n;
-    a.bs0 = -(long long)grp * nn;
-    a.ld1 = 2;
+    GemmA a = plain_a(W + (long long)r * G.nn, n, -(long long)grp * G.nn);
     a.ksplit = n;
-    a.rlim0 = INT_MAX;
-    a.roff0 = kNoMask;
-    a.rlim1 = INT_MAX;
-    a.roff1 = kNoMask;
-    {  // P_r = W_r P_{r+1}
-      GemmB b = {P + (long long)(grp - q) * n, pld, pbs, kNoMask};
+    if (what & kRoundP) {  // P_r = W_r P_{r+1}
+      GemmB b = {P + g0 * G.pbs + (long long)(grp - q) * n, G.pld, G.pbs, kNoMask};
       GemmC c = {};
-      c.p0 = P + (long long)(grp - 1 - q) * n;
-      c.ld0 = pld;
-      c.bs0 = pbs;
+      c.p0 = P + g0 * G.pbs + (long long)(grp - 1 - q) * n;
+      c.ld0 = G.pld;
+      c.bs0 = G.pbs;
       c.ld1 = 1;
       c.nsplit = n;
       c.alpha = 1.0;
       CK(launch_gemm(d1, a, b, c, batch, 2, st));
     }
-    {  // X_{r, r+1:r+q} = W_r X_{r+1, r+1:r+q}; X_{r+1,r+1} is upper triangular
+    if (what & kRoundIntra) {  // X_{r, r+1:r+q} = W_r X_{r+1, r+1:r+q}; X_{r+1,r+1} is upper triangular
       GemmDims dq = {n, q * n, n};
-      GemmB b = {dA + cm((long long)(r + 1) * n, (long long)(r + 1) * n, ldd), ldd,
-                 dstep, 0};
+      GemmB b = {dA + cm((long long)(r + 1) * n, (long long)(r + 1) * n, ldd), ldd, dstep, 0};
       GemmC c = {};
       c.p0 = dA + cm((long long)r * n, (long long)(r + 1) * n, ldd);
       c.ld0 = ldd;
@@ -314,9 +340,8 @@ int bstri_blocked(int n, int L, double* dA, int ldd, const double* W, double* P,
       c.alpha = 1.0;
       CK(launch_gemm(dq, a, b, c, batch, 2, st));
     }
-    {  // Zc_r = Z_r + W_r Zc_{r+1}, in place in block column L-1
-      GemmB b = {dA + cm((long long)(r + 1) * n, (long long)(L - 1) * n, ldd), ldd, rstep,
-                 kNoMask};
+    if (what & kRoundZc) {  // Zc_r = Z_r + W_r Zc_{r+1}, in place in block column L-1
+      GemmB b = {dA + cm((long long)(r + 1) * n, (long long)(L - 1) * n, ldd), ldd, rstep, kNoMask};
       GemmC c = {};
       c.p0 = dA + cm((long long)r * n, (long long)(L - 1) * n, ldd);
       c.ld0 = ldd;
@@ -328,64 +353,96 @@ int bstri_blocked(int n, int L, double* dA, int ldd, const double* W, double* P,
       CK(launch_gemm(d1, a, b, c, batch, 2, st));
     }
   }
-  if (persistent) {
-    // All group steps in one launch, column tiles pipelined across the steps.
-    CKM(cudaMemsetAsync(rsync, 0, sizeof(int) * rsync_ints, st));
-    CK(launch_bstri_recurrence_blocked(dA, ldd, P, pld, pbs, grp, n, L, rsync,
-                                       rsync + rsync_ints - 2, err, st));
-    return 0;
-  }
-  // Group steps, bottom to top.
-  for (int g = 0; g < ngr; g++) {
-    const int b = b0 - g * grp, m = b + 1 < grp ? b + 1 : grp, t = b - m + 1;
-    GemmDims d = {m * n, (L - 1 - b) * n, n};
-    GemmA a = {};
-    a.p0 = P + g * pbs + (long long)(grp - m) * n;
-    a.ld0 = pld;
-    a.ld1 = 2;
+  return 0;
+}
+
+// Group steps g0 .. g1-1 in order, one launch each, over block columns
+// [max(b+1, cfrom), cto); cto = L includes block column L-1 with its Zc.
+int groups_steps(const RowGroups& G, double* dA, int ldd, const double* P, int g0, int g1,
+                 int cfrom, int cto, int cfg, cudaStream_t st) {
+  const int n = G.n, L = G.L;
+  for (int g = g0; g < g1; g++) {
+    const int b = G.b(g), m = G.m(g), t = G.t(g);
+    const int cs = b + 1 > cfrom ? b + 1 : cfrom;
+    if (cto <= cs) continue;
+    const int ncol = (cto - cs) * n;
+    GemmDims d = {m * n, ncol, n};
+    GemmA a = plain_a(P + g * G.pbs + (long long)(G.grp - m) * n, G.pld, 0);
     a.ksplit = n;
-    a.rlim0 = INT_MAX;
-    a.roff0 = kNoMask;
-    a.rlim1 = INT_MAX;
-    a.roff1 = kNoMask;
-    GemmB bb = {dA + cm((long long)(b + 1) * n, (long long)(b + 1) * n, ldd), ldd, 0, 0};
+    GemmB bb = {dA + cm((long long)(b + 1) * n, (long long)cs * n, ldd), ldd, 0,
+                cs == b + 1 ? 0 : kNoMask};
     GemmC c = {};
-    c.p0 = dA + cm((long long)t * n, (long long)(b + 1) * n, ldd);
+    c.p0 = dA + cm((long long)t * n, (long long)cs * n, ldd);
     c.ld0 = ldd;
-    c.p1 = dA + cm((long long)t * n, (long long)(L - 1) * n, ldd);
-    c.ld1 = ldd;
-    c.nsplit = (L - 2 - b) * n;
     c.alpha = 1.0;
     c.beta0 = 0.0;
-    c.beta1 = 1.0;
-    CK(launch_gemm(d, a, bb, c, 1, 0, st));
+    if (cto == L) {
+      c.p1 = dA + cm((long long)t * n, (long long)(L - 1) * n, ldd);
+      c.ld1 = ldd;
+      c.nsplit = ncol - n;
+      c.beta1 = 1.0;
+    } else {
+      c.ld1 = 1;
+      c.nsplit = ncol;
+    }
+    CK(launch_gemm(d, a, bb, c, 1, cfg, st));
   }
   return 0;
 }
 
-int run_bstri(int n, int L, double* dA, int ldd, void* ws, cudaStream_t st) {
-  Layout ly = layout(n, L, ldd);
-  int* info = at<int>(ws, ly.info);
-  double* W = at<double>(ws, ly.W);
-  double* Y = at<double>(ws, ly.Y);
+int bstri_blocked(int n, int L, double* dA, int ldd, const double* W, double* P, int grp,
+                  bool persistent, int* rsync, int rsync_ints, int* err, cudaStream_t st) {
+  const RowGroups G(n, L, grp);
+  if (int e = groups_seed(G, W, P, 0, G.ngr, st)) return e;
+  if (int e = groups_rounds(G, dA, ldd, W, P, 0, G.ngr, kRoundP | kRoundIntra | kRoundZc, st))
+    return e;
+  if (persistent) {
+    // All group steps in one launch, column tiles pipelined across the steps.
+    CKM(cudaMemsetAsync(rsync, 0, sizeof(int) * rsync_ints, st));
+    CK(launch_bstri_recurrence_blocked(dA, ldd, P, G.pld, G.pbs, grp, n, L, rsync,
+                                       rsync + rsync_ints - 2, err, st));
+    return 0;
+  }
+  return groups_steps(G, dA, ldd, P, 0, G.ngr, 0, L, 0, st);
+}
+
+// X_ii = R_ii^{-1} for the diagonal blocks [i0, i1) (tmp: the recursive
+// inversion's scratch, n^2/4 doubles per block).
+int diag_inverse(int n, double* dA, int ldd, int* info, double* tmp, int i0, int i1,
+                 cudaStream_t st) {
+  if (i1 <= i0) return 0;
+  const long long diag = (long long)n * (ldd + 1);
+  CK(launch_trtri_blocks(dA + i0 * diag, ldd, n, diag, i1 - i0, info, tmp, st, i0));
+  return 0;
+}
+
+// W_i = -X_ii R_{i,i+1} for i in [i0, i1).
+int w_products(int n, double* dA, int ldd, double* W, int i0, int i1, cudaStream_t st) {
+  if (i1 <= i0) return 0;
   const long long nn = (long long)n * n, diag = (long long)n * (ldd + 1);
-  CKM(cudaMemsetAsync(info, 0x7f, sizeof(int), st));
-  // X_ii = R_ii^{-1} for every diagonal block.
-  // (Y, not yet used, is the scratch of the recursive inversion: n^2/4 per block.)
-  CK(launch_trtri_blocks(dA, ldd, n, diag, L, info, Y, st));
   GemmDims d = {n, n, n};
-  // Y_i = R_{i,L-1} X_{L-1,L-1},  i = 0..L-2.
+  GemmA a = plain_a(dA + i0 * diag, ldd, diag);
+  a.ksplit = n;
+  a.roff0 = 0;
+  GemmB b = {dA + i0 * diag + cm(0, n, ldd), ldd, diag, kNoMask};
+  GemmC c = {};
+  c.p0 = W + i0 * nn;
+  c.ld0 = n;
+  c.bs0 = nn;
+  c.ld1 = 1;
+  c.nsplit = n;
+  c.alpha = -1.0;
+  CK(launch_gemm(d, a, b, c, i1 - i0, 0, st));
+  return 0;
+}
+
+// Y_i = R_{i,L-1} X_{L-1,L-1} and Z_i = -X_ii Y_i -> A(i, L-1), i = 0..L-2.
+int yz_products(int n, int L, double* dA, int ldd, double* Y, cudaStream_t st) {
+  const long long nn = (long long)n * n, diag = (long long)n * (ldd + 1);
+  GemmDims d = {n, n, n};
   {
-    GemmA a = {};
-    a.p0 = dA + cm(0, (long long)(L - 1) * n, ldd);
-    a.ld0 = ldd;
-    a.bs0 = n;
-    a.ld1 = 2;
+    GemmA a = plain_a(dA + cm(0, (long long)(L - 1) * n, ldd), ldd, n);
     a.ksplit = n;
-    a.rlim0 = INT_MAX;
-    a.roff0 = kNoMask;
-    a.rlim1 = INT_MAX;
-    a.roff1 = kNoMask;
     GemmB b = {dA + cm((long long)(L - 1) * n, (long long)(L - 1) * n, ldd), ldd, 0, 0};
     GemmC c = {};
     c.p0 = Y;
@@ -396,18 +453,10 @@ int run_bstri(int n, int L, double* dA, int ldd, void* ws, cudaStream_t st) {
     c.alpha = 1.0;
     CK(launch_gemm(d, a, b, c, L - 1, 0, st));
   }
-  // Z_i = -X_ii Y_i  -> A(i, L-1).
   {
-    GemmA a = {};
-    a.p0 = dA;
-    a.ld0 = ldd;
-    a.bs0 = diag;
-    a.ld1 = 2;
+    GemmA a = plain_a(dA, ldd, diag);
     a.ksplit = n;
-    a.rlim0 = INT_MAX;
     a.roff0 = 0;
-    a.rlim1 = INT_MAX;
-    a.roff1 = kNoMask;
     GemmB b = {Y, n, nn, kNoMask};
     GemmC c = {};
     c.p0 = dA + cm(0, (long long)(L - 1) * n, ldd);
@@ -418,28 +467,21 @@ int run_bstri(int n, int L, double* dA, int ldd, void* ws, cudaStream_t st) {
     c.alpha = -1.0;
     CK(launch_gemm(d, a, b, c, L - 1, 0, st));
   }
-  if (L >= 3) {
-    // W_i = -X_ii R_{i,i+1},  i = 0..L-3.
-    GemmA a = {};
-    a.p0 = dA;
-    a.ld0 = ldd;
-    a.bs0 = diag;
-    a.ld1 = 2;
-    a.ksplit = n;
-    a.rlim0 = INT_MAX;
-    a.roff0 = 0;
-    a.rlim1 = INT_MAX;
-    a.roff1 = kNoMask;
-    GemmB b = {dA + cm(0, n, ldd), ldd, diag, kNoMask};
-    GemmC c = {};
-    c.p0 = W;
-    c.ld0 = n;
-    c.bs0 = nn;
-    c.ld1 = 1;
-    c.nsplit = n;
-    c.alpha = -1.0;
-    CK(launch_gemm(d, a, b, c, L - 2, 0, st));
-  }
+  return 0;
+}
+
+int run_bstri(int n, int L, double* dA, int ldd, void* ws, cudaStream_t st) {
+  Layout ly = layout(n, L, ldd);
+  int* info = at<int>(ws, ly.info);
+  double* W = at<double>(ws, ly.W);
+  double* Y = at<double>(ws, ly.Y);
+  const long long nn = (long long)n * n;
+  CKM(cudaMemsetAsync(info, 0x7f, sizeof(int), st));
+  // X_ii = R_ii^{-1} for every diagonal block (Y, not yet used, is the
+  // scratch of the recursive inversion).
+  if (int e = diag_inverse(n, dA, ldd, info, Y, 0, L, st)) return e;
+  if (int e = yz_products(n, L, dA, ldd, Y, st)) return e;
+  if (int e = w_products(n, dA, ldd, W, 0, L - 2, st)) return e;
   // Row recurrence: X_{i, i+1:L} = W_i X_{i+1, i+1:L} (+ Z_i on the last block).
   const Plan plan = plan_for(n, L);
   const int rec = plan.bstri_cfg;
@@ -462,15 +504,8 @@ int run_bstri(int n, int L, double* dA, int ldd, void* ws, cudaStream_t st) {
   for (int i = L - 3; i >= 0; i--) {
     const int ncol = (L - 1 - i) * n;
     GemmDims dr = {n, ncol, n};
-    GemmA a = {};
-    a.p0 = W + (size_t)i * nn;
-    a.ld0 = n;
-    a.ld1 = 2;
+    GemmA a = plain_a(W + (size_t)i * nn, n, 0);
     a.ksplit = n;
-    a.rlim0 = INT_MAX;
-    a.roff0 = kNoMask;
-    a.rlim1 = INT_MAX;
-    a.roff1 = kNoMask;
     GemmB b = {dA + cm((long long)(i + 1) * n, (long long)(i + 1) * n, ldd), ldd, 0, 0};
     GemmC c = {};
     c.p0 = dA + cm((long long)i * n, (long long)(i + 1) * n, ldd);
@@ -484,6 +519,155 @@ int run_bstri(int n, int L, double* dA, int ldd, void* ws, cudaStream_t st) {
     CK(launch_gemm(dr, a, b, c, 1, rec, st));
   }
   return 0;
+}
+
+// BSOF + BSTRI with BSTRI's leading rows overlapped with the end of the
+// factorization.  Block row i of R (R_ii, R_{i,i+1}, R_{i,L-1}) is final once
+// panel i is factored, and the leading block of X = R^{-1} above row h, the
+// columns left of h, depends only on R's rows above h.  So the factorization
+// runs as two launches split at panel h; after the first, a low-priority side
+// stream inverts the diagonal blocks above h, forms their W_i, the row-group
+// products P and in-group columns of the groups above h, and those groups'
+// steps over the columns left of h, on the SMs the factorization leaves idle,
+// while the second launch (on a high-priority side stream, so its
+// cooperative CTAs are placed first) factors the remaining panels.  The two
+// touch disjoint data: the second launch reads and writes rows from h n down.
+// Once both are done the rest of BSTRI runs: the remaining diagonal blocks,
+// Y and Z, the other groups' rounds, every group's Zc, and one persistent
+// launch of all group steps over the columns from h on.  Every product is the
+// one the unsplit path computes, so the results are the same.  Used for
+// 16-wide leaves (n <= 256: the factorization occupies under half the SMs)
+// with the persistent blocked recurrence; h is the top row of the fourth of
+// the row groups nearest the bottom (at least two groups).
+struct SideStreams {
+  cudaStream_t hi = nullptr, lo = nullptr;
+  cudaEvent_t e1 = nullptr, e2 = nullptr, e3 = nullptr;
+};
+thread_local std::map<int, SideStreams> g_side;
+std::atomic<int> g_overlap_enabled{1};
+
+// This thread's side streams on the current device, created on first use
+// (never while `st` is being captured into a graph: then nullptr and the
+// unsplit path runs).
+SideStreams* side_streams(cudaStream_t st) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  auto it = g_side.find(dev);
+  if (it != g_side.end()) return &it->second;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  SideStreams x;
+  int least = 0, greatest = 0;
+  bool ok = cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess &&
+            cudaStreamCreateWithPriority(&x.hi, cudaStreamNonBlocking, greatest) == cudaSuccess &&
+            cudaStreamCreateWithPriority(&x.lo, cudaStreamNonBlocking, least) == cudaSuccess &&
+            cudaEventCreateWithFlags(&x.e1, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&x.e2, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&x.e3, cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    if (x.hi) cudaStreamDestroy(x.hi);
+    if (x.lo) cudaStreamDestroy(x.lo);
+    if (x.e1) cudaEventDestroy(x.e1);
+    if (x.e2) cudaEventDestroy(x.e2);
+    cudaGetLastError();
+    return nullptr;
+  }
+  return &(g_side[dev] = x);
+}
+
+// Row groups and split row h of the overlapped path, or false when it does
+// not apply to (n, L).
+bool overlap_split(int n, int L, int* grp_out, int* tailg_out, int* h_out) {
+  if (!g_overlap_enabled.load() || bsof_leaf_width(n) != 16 || L < 4) return false;
+  const Plan plan = plan_for(n, L);
+  const int grp = plan.bstri_group < L - 2 ? plan.bstri_group : L - 2;
+  if (plan.bstri_cfg != 4 || grp < 2) return false;
+  const int ngr = (L - 2 + grp - 1) / grp;
+  const int tailg = (ngr + 3) / 4 > 2 ? (ngr + 3) / 4 : 2;
+  if (ngr <= tailg) return false;
+  *grp_out = grp;
+  *tailg_out = tailg;
+  *h_out = L - 2 - tailg * grp;
+  return true;
+}
+
+int run_bsoftri_overlap(int n, int L, double* dA, int ldd, double* dtau, void* ws, cudaStream_t st,
+                        bool form_q, int base_workers, int grp, int tailg, int h,
+                        SideStreams* ss) {
+  Layout ly = layout(n, L, ldd);
+  const RowGroups G(n, L, grp);
+  int* info = at<int>(ws, ly.info);
+  double* W = at<double>(ws, ly.W);
+  double* Y = at<double>(ws, ly.Y);
+  double* P = at<double>(ws, ly.C0);
+  double* Tb = at<double>(ws, ly.T);
+  double* Gq = at<double>(ws, ly.G);
+  int* sync = at<int>(ws, ly.sync);
+  const int ntiles = (L + 2 * (L - 1)) * ly.tiles;
+  int* next_task = sync + ntiles + ly.leaves;
+  // Counters and info words before either side stream starts.
+  CKM(cudaMemsetAsync(sync, 0, sizeof(int) * ly.sync_ints, st));
+  CKM(cudaMemsetAsync(info + 1, 0, sizeof(int), st));
+  CKM(cudaMemsetAsync(info, 0x7f, sizeof(int), st));
+  CKM(cudaMemsetAsync(info + 3, 0, sizeof(int), st));
+  if (form_q) CK(launch_set_identity(Gq, 2 * n, 2 * n, 4ll * n * n, L - 1, st));
+  int workers = base_workers;
+  if (form_q) workers *= 2;
+  const int sh = h * ly.tiles;  // first leaf of panel h
+  CK(launch_bsof_persistent(dA, ldd, n, L, dtau, Tb, form_q ? Gq : nullptr, ly.maxleaves, sync,
+                            sync + ntiles, next_task, info + 1, at<unsigned long long>(ws, ly.tl),
+                            workers, st, 0, sh));
+  CKM(cudaEventRecord(ss->e1, st));
+  // Panels h .. L-2.
+  CKM(cudaStreamWaitEvent(ss->hi, ss->e1, 0));
+  CKM(cudaMemsetAsync(next_task, 0, sizeof(int), ss->hi));
+  CK(launch_bsof_persistent(dA, ldd, n, L, dtau, Tb, form_q ? Gq : nullptr, ly.maxleaves, sync,
+                            sync + ntiles, next_task, info + 1, at<unsigned long long>(ws, ly.tl),
+                            workers, ss->hi, sh, -1));
+  CKM(cudaEventRecord(ss->e3, ss->hi));
+  // BSTRI of the rows above h (W_{h-1} uses R_{h-1,h}, final after panel h-1).
+  CKM(cudaStreamWaitEvent(ss->lo, ss->e1, 0));
+  if (int e = diag_inverse(n, dA, ldd, info, Y, 0, h, ss->lo)) return e;
+  if (int e = w_products(n, dA, ldd, W, 0, h, ss->lo)) return e;
+  if (int e = groups_seed(G, W, P, tailg, G.ngr, ss->lo)) return e;
+  if (int e = groups_rounds(G, dA, ldd, W, P, tailg, G.ngr, kRoundP | kRoundIntra, ss->lo)) return e;
+  if (int e = groups_steps(G, dA, ldd, P, tailg + 1, G.ngr, 0, h, 3, ss->lo)) return e;
+  CKM(cudaEventRecord(ss->e2, ss->lo));
+  // The rest of BSTRI.
+  CKM(cudaStreamWaitEvent(st, ss->e3, 0));
+  CKM(cudaStreamWaitEvent(st, ss->e2, 0));
+  if (int e = diag_inverse(n, dA, ldd, info, Y, h, L, st)) return e;
+  if (int e = yz_products(n, L, dA, ldd, Y, st)) return e;
+  if (int e = w_products(n, dA, ldd, W, h, L - 2, st)) return e;
+  if (int e = groups_seed(G, W, P, 0, tailg, st)) return e;
+  if (int e = groups_rounds(G, dA, ldd, W, P, 0, tailg, kRoundP | kRoundIntra, st)) return e;
+  if (int e = groups_rounds(G, dA, ldd, W, P, 0, G.ngr, kRoundZc, st)) return e;
+  int* rs = at<int>(ws, ly.rsync);
+  CKM(cudaMemsetAsync(rs, 0, sizeof(int) * ly.rsync_ints, st));
+  CK(launch_bstri_recurrence_blocked(dA, ldd, P, G.pld, G.pbs, grp, n, L, rs,
+                                     rs + ly.rsync_ints - 2, info + 3, st, h));
+  return 0;
+}
+
+// BSOF + BSTRI of one inversion: overlapped where it applies, else in order.
+int run_bsoftri(int n, int L, double* dA, int ldd, double* dtau, void* ws, cudaStream_t st,
+                bool form_q, int base_workers, bool allow_overlap) {
+  int grp = 0, tailg = 0, h = 0;
+  if (allow_overlap && overlap_split(n, L, &grp, &tailg, &h)) {
+    SideStreams* ss = side_streams(st);
+    if (ss)
+      return run_bsoftri_overlap(n, L, dA, ldd, dtau, ws, st, form_q, base_workers, grp, tailg,
+                                 h, ss);
+  }
+  int e = run_bsof(n, L, dA, ldd, dtau, ws, st, form_q, base_workers);
+  if (e) return e;
+  return run_bstri(n, L, dA, ldd, ws, st);
 }
 
 // G_k = Q_k^T of every panel from the stored reflectors and tau: compact-WY
@@ -647,9 +831,8 @@ int bsofi_dev_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* 
 int bsofi_dev_bsoftri_q(int n, int L, double* dA, int ldd, double* dtau, void* dws,
                         void* stream) {
   g_launches = 0;
-  int e = run_bsof(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, true, bsof_workers(n, L, 0));
-  if (e) return e;
-  return run_bstri(n, L, dA, ldd, dws, (cudaStream_t)stream);
+  return run_bsoftri(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, true, bsof_workers(n, L, 0),
+                     true);
 }
 
 int bsofi_dev_bsoi_ex(int n, int L, double* dA, int ldd, const double* dtau, void* dws,
@@ -692,9 +875,10 @@ int bsofi_dev_invert(int n, int L, double* dA, int ldd, double* dtau, void* dws,
 int bsofi_dev_invert_ex(int n, int L, double* dA, int ldd, double* dtau, void* dws, void* stream,
                         int workers) {
   g_launches = 0;
-  int e = run_bsof(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, true,
-                   bsof_workers(n, L, workers));
-  if (!e) e = run_bstri(n, L, dA, ldd, dws, (cudaStream_t)stream);
+  // The overlapped BSTRI uses this thread's side streams: only for a single
+  // inversion (workers == 0), not for the pooled ones of batches and servers.
+  int e = run_bsoftri(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, true,
+                      bsof_workers(n, L, workers), workers == 0);
   if (!e) e = run_bsoi(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, true);
   return e;
 }
@@ -708,6 +892,8 @@ int bsofi_dev_bsof_timeline(int n, int L, int ldd, void* dws, unsigned long long
 }
 
 void bsofi_dev_set_bsof_workers(int w) { g_workers_override = w > 0 ? w : 0; }
+
+void bsofi_dev_set_bstri_overlap(int on) { g_overlap_enabled.store(on ? 1 : 0); }
 
 int bsofi_dev_plan_get(int n, int L, int* plan) {
   std::lock_guard<std::mutex> lk(g_plan_mu);

@@ -315,6 +315,13 @@ int bsofi_device_timing_read(double *ms, long long *launches);
 int bsofi_device_bsof_timeline(int n, int L, int ldda, void *dwork, unsigned long long *host,
                                int max_leaves);
 void bsofi_device_set_bsof_workers(int workers);
+/* Single inversions with n <= 256 whose plan runs the persistent blocked BSTRI
+ * recurrence split the factorization at a panel and overlap BSTRI's leading
+ * rows with the rest of it on two side streams of the calling thread (created
+ * on first use, never during a graph capture of the caller's stream; the
+ * results are the same as without the split).  on = 0 turns this off for the
+ * process, 1 (the default) on. */
+void bsofi_device_set_bstri_overlap(int on);
 
 /* Diagnostic entry point (no reference counterpart): one call of the FP64
  * DMMA tile engine, C = alpha*A*B + beta*C on device memory (column-major),

@@ -77,3 +77,49 @@ def test_default_blocked_plan_vs_reference(cuda_device, n, L):
     from gpu_util import block_residual_gpu
     Xd = torch.from_numpy(np.ascontiguousarray(X)).to(cuda_device)
     assert block_residual_gpu(torch, *pcyclic_blocks(M, n, L), Xd) < 1e-13
+
+
+def _device_invert(torch, M, n, L):
+    from gpu_util import from_device_colmajor, to_device_colmajor
+    N = n * L
+    dA = to_device_colmajor(torch, M)
+    dtau = torch.zeros(N, dtype=torch.float64, device="cuda")
+    ws = torch.zeros(api.workspace_bytes(n, L, N) // 8 + 1, dtype=torch.float64, device="cuda")
+    assert api.device_invert(n, L, dA.data_ptr(), N, dtau.data_ptr(), ws.data_ptr(), 0) == 0
+    torch.cuda.synchronize()
+    return from_device_colmajor(dA, N), dtau.cpu().numpy()
+
+
+@pytest.mark.parametrize("n,L,grp", [(256, 32, None), (64, 40, None), (100, 64, None),
+                                     (33, 14, 3), (16, 20, 4), (100, 12, 2), (255, 16, 4),
+                                     (128, 30, 8), (7, 23, 5)])
+def test_overlapped_bstri_is_bitwise_the_ordered_one(cuda_device, n, L, grp):
+    """Single inversions (device API and handle API) whose plan uses the
+    persistent blocked recurrence split the factorization and overlap BSTRI's
+    leading rows with its end; the results are bitwise those of the phases run
+    in order (the same products), and agree with the oracle."""
+    import torch
+    lib = api.load()
+    if grp is not None:
+        _, plan = api.plan_get(n, L)
+        assert api.plan_set(n, L, [plan[0], 4, plan[2], grp]) == 0
+    M = random_pcyclic(n, L, seed=5100 + n + L)
+    try:
+        lib.bsofi_device_set_bstri_overlap(0)
+        X0, tau0 = _device_invert(torch, M, n, L)
+        _, S0, T0, info0 = api.invert(M, n, L)
+        lib.bsofi_device_set_bstri_overlap(1)
+        X1, tau1 = _device_invert(torch, M, n, L)
+        _, S1, T1, info1 = api.invert(M, n, L)
+    finally:
+        lib.bsofi_device_set_bstri_overlap(1)
+    assert info0 == info1 == 0
+    np.testing.assert_array_equal(tau1, tau0)
+    np.testing.assert_array_equal(X1, X0)
+    np.testing.assert_array_equal(T1, T0)
+    np.testing.assert_array_equal(S1, S0)
+    if n * L <= 3000:
+        Ar, taur, _ = oracle.port_bsoftri(M, n, L)
+        Xr, _ = oracle.port_bsoi(Ar, taur, n, L)
+        assert rel_fro(X1, Xr) < inverse_tolerance(M, Xr)
+        assert residual(M, X1) < 1e-13
