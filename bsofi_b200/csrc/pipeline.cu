@@ -624,24 +624,34 @@ int run_bsoftri_overlap(int n, int L, double* dA, int ldd, double* dtau, void* w
                             sync + ntiles, next_task, info + 1, at<unsigned long long>(ws, ly.tl),
                             workers, st, 0, sh));
   CKM(cudaEventRecord(ss->e1, st));
+  // From here on both side streams are always joined back into st, so that
+  // nothing of this call is still queued on them when it returns, error or not.
+  int err = 0;
   // Panels h .. L-2.
-  CKM(cudaStreamWaitEvent(ss->hi, ss->e1, 0));
-  CKM(cudaMemsetAsync(next_task, 0, sizeof(int), ss->hi));
-  CK(launch_bsof_persistent(dA, ldd, n, L, dtau, Tb, form_q ? Gq : nullptr, ly.maxleaves, sync,
-                            sync + ntiles, next_task, info + 1, at<unsigned long long>(ws, ly.tl),
-                            workers, ss->hi, sh, -1));
-  CKM(cudaEventRecord(ss->e3, ss->hi));
+  err = (int)cudaStreamWaitEvent(ss->hi, ss->e1, 0);
+  if (!err) err = (int)cudaMemsetAsync(next_task, 0, sizeof(int), ss->hi);
+  if (!err) {
+    err = (int)launch_bsof_persistent(dA, ldd, n, L, dtau, Tb, form_q ? Gq : nullptr, ly.maxleaves,
+                                      sync, sync + ntiles, next_task, info + 1,
+                                      at<unsigned long long>(ws, ly.tl), workers, ss->hi, sh, -1);
+    if (!err) g_launches++;
+  }
   // BSTRI of the rows above h (W_{h-1} uses R_{h-1,h}, final after panel h-1).
-  CKM(cudaStreamWaitEvent(ss->lo, ss->e1, 0));
-  if (int e = diag_inverse(n, dA, ldd, info, Y, 0, h, ss->lo)) return e;
-  if (int e = w_products(n, dA, ldd, W, 0, h, ss->lo)) return e;
-  if (int e = groups_seed(G, W, P, tailg, G.ngr, ss->lo)) return e;
-  if (int e = groups_rounds(G, dA, ldd, W, P, tailg, G.ngr, kRoundP | kRoundIntra, ss->lo)) return e;
-  if (int e = groups_steps(G, dA, ldd, P, tailg + 1, G.ngr, 0, h, 3, ss->lo)) return e;
-  CKM(cudaEventRecord(ss->e2, ss->lo));
+  if (!err) err = (int)cudaStreamWaitEvent(ss->lo, ss->e1, 0);
+  if (!err) err = diag_inverse(n, dA, ldd, info, Y, 0, h, ss->lo);
+  if (!err) err = w_products(n, dA, ldd, W, 0, h, ss->lo);
+  if (!err) err = groups_seed(G, W, P, tailg, G.ngr, ss->lo);
+  if (!err) err = groups_rounds(G, dA, ldd, W, P, tailg, G.ngr, kRoundP | kRoundIntra, ss->lo);
+  if (!err) err = groups_steps(G, dA, ldd, P, tailg + 1, G.ngr, 0, h, 3, ss->lo);
+  // Join (the events are recorded even after an error).
+  const int j1 = (int)cudaEventRecord(ss->e3, ss->hi);
+  const int j2 = (int)cudaEventRecord(ss->e2, ss->lo);
+  const int j3 = j1 ? j1 : (int)cudaStreamWaitEvent(st, ss->e3, 0);
+  const int j4 = j2 ? j2 : (int)cudaStreamWaitEvent(st, ss->e2, 0);
+  if (err) return err;
+  if (j3) return j3;
+  if (j4) return j4;
   // The rest of BSTRI.
-  CKM(cudaStreamWaitEvent(st, ss->e3, 0));
-  CKM(cudaStreamWaitEvent(st, ss->e2, 0));
   if (int e = diag_inverse(n, dA, ldd, info, Y, h, L, st)) return e;
   if (int e = yz_products(n, L, dA, ldd, Y, st)) return e;
   if (int e = w_products(n, dA, ldd, W, h, L - 2, st)) return e;
