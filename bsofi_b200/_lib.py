@@ -55,6 +55,8 @@ _SIGS = {
                                             _vp, _vp]),
     "bsofi_device_bsoi": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp,
                                          _vp, _vp]),
+    "bsofi_device_bsoi_rows": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp,
+                                              _vp, ctypes.c_int, ctypes.c_int, _vp]),
     "bsofi_device_info": (_vp, [_vp]),
     "bsofi_device_last_launches": (ctypes.c_longlong, []),
     "bsofi_batch_workspace_bytes": (ctypes.c_ulonglong, [ctypes.c_int, _vp, _vp, _vp]),

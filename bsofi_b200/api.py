@@ -120,6 +120,11 @@ def device_bsoi(n, L, dA, ldda, dtau, dwork, stream=0):
     return load().bsofi_device_bsoi(n, L, dA, ldda, dtau, dwork, stream)
 
 
+def device_bsoi_rows(n, L, dA, ldda, dtau, dwork, row0, row1, stream=0):
+    """BSOI of rows [row0, row1) of M^{-1} (bsofi_device_bsoi_rows)."""
+    return load().bsofi_device_bsoi_rows(n, L, dA, ldda, dtau, dwork, row0, row1, stream)
+
+
 def device_assemble(n, L, dD, dS, dA, ldda, stream=0):
     """bsofi_device_assemble: p-cyclic input from packed blocks (dD may be 0 = identity)."""
     return load().bsofi_device_assemble(n, L, dD or None, dS, dA, ldda, stream)

@@ -988,6 +988,17 @@ int bsofi_device_bsoi(int n, int L, double *dA, int ldda, const double *dtau, vo
   return e ? cuda_info((cudaError_t)e) : 0;
 }
 
+int bsofi_device_bsoi_rows(int n, int L, double *dA, int ldda, const double *dtau, void *dwork,
+                           int row0, int row1, void *stream) {
+  int e, N = n * L;
+  if (!device_args_ok(n, L, dA, ldda, dtau, dwork)) return -1;
+  if (row0 < 0 || row1 > N || row0 >= row1 || row0 % 128 != 0 || (row1 % 128 != 0 && row1 != N))
+    return -1;
+  e = bsofi_dev_prepare();
+  if (!e) e = bsofi_dev_bsoi_rows(n, L, dA, ldda, dtau, dwork, stream, row0, row1);
+  return e ? cuda_info((cudaError_t)e) : 0;
+}
+
 int bsofi_device_invert(int n, int L, double *dA, int ldda, double *dtau, void *dwork,
                         void *stream) {
   int e;

@@ -52,6 +52,11 @@ int bsofi_dev_bsoftri_q(int n, int L, double *dA, int ldd, double *dtau, void *d
 int bsofi_dev_bsoi_ex(int n, int L, double *dA, int ldd, const double *dtau, void *dws,
                       void *stream, int q_ready);
 
+/* BSOI of the rows [row0, row1) of M^{-1} only (row0 a multiple of 128, row1
+ * too unless it is N): the other rows of A are left as they were. */
+int bsofi_dev_bsoi_rows(int n, int L, double *dA, int ldd, const double *dtau, void *dws,
+                        void *stream, int row0, int row1);
+
 /* The reflector rows of every block column and tau (what Q formation reads):
  * mode 0 packs them into ref (bsofi_dev_state_ref_doubles doubles), mode 1
  * compares them with ref and sets the device int *dflag to 1 on a difference. */

@@ -72,9 +72,12 @@ cudaError_t launch_bstri_recurrence_blocked(double* A, long long ld, const doubl
 // done: (L-1) * bsoi_row_bands(N) ints and next: one int, zeroed before;
 // small: 64 x 64 tiles instead of 128 x 128.
 int bsoi_row_bands(int N);
+// [row0, row1): the rows computed (row1 = -1: to N); row0 a multiple of the
+// tile height (128, or 64 when small), row1 too unless it is N.
 cudaError_t launch_bsoi_persistent(double* A, long long ld, double* carry0, double* carry1,
                                    long long ldc, const double* G, int n, int L, int* done,
-                                   int* next, int* err, bool small, cudaStream_t st);
+                                   int* next, int* err, bool small, cudaStream_t st,
+                                   int row0 = 0, int row1 = -1);
 
 // In-place inversion of the upper triangles of nblk n x n blocks (block b at
 // A + b * bstride); tmp: device scratch of nblk * n * n / 4 doubles.  A zero

@@ -11,7 +11,10 @@
 // on a tile claimed earlier, whose CTA is already running: progress needs no
 // co-residency, so the launch is an ordinary one (a cooperative launch would
 // wait for the whole GPU and serialise batched inversions on other streams).
-// Every spin is bounded and reports through an error word.
+// Every spin is bounded and reports through an error word.  A launch may be
+// restricted to the row bands [rb0, rb1): each of its tiles is then the tile a
+// launch over all rows computes (rows of X are independent in BSOI), which is
+// how one inversion's BSOI is split across GPUs by rows.
 #include <climits>
 #include "bsofi_common.cuh"
 #include "bsofi_kernels.h"
@@ -29,6 +32,7 @@ struct BsoiArgs {
   int* next;         // tile counter
   int* err;
   long long spin_limit;
+  int rb0, rb1;      // row bands computed (of the tile height)
 };
 
 BSOFI_DEVINL int ld_acq(const int* p) {
@@ -43,16 +47,17 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) bsoi_persistent_kernel(BsoiAr
   __shared__ int s_tile, s_ok;
   const int n2 = 2 * s.n;
   const int RT = (s.N + Cfg::BM - 1) / Cfg::BM, CT = (n2 + Cfg::BN - 1) / Cfg::BN;
-  const long long total = (long long)(s.L - 1) * RT * CT;
+  const int RS = s.rb1 - s.rb0;  // row bands of this launch
+  const long long total = (long long)(s.L - 1) * RS * CT;
   for (;;) {
     __syncthreads();  // the previous tile's shared memory is no longer read
     if (threadIdx.x == 0) s_tile = atomicAdd(s.next, 1);
     __syncthreads();
     const long long tile = s_tile;
     if (tile >= total) return;
-    const int step = (int)(tile / ((long long)RT * CT));  // 0 = k = L-2
-    const int rem = (int)(tile % ((long long)RT * CT));
-    const int rb = rem / CT, cb = rem % CT;
+    const int step = (int)(tile / ((long long)RS * CT));  // 0 = k = L-2
+    const int rem = (int)(tile % ((long long)RS * CT));
+    const int rb = s.rb0 + rem / CT, cb = rem % CT;
     const int k = s.L - 2 - step;
     if (step > 0) {
       if (threadIdx.x == 0) {
@@ -124,17 +129,26 @@ static cudaError_t launch_al(const BsoiArgs& s, cudaStream_t st) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bsoi_persistent_kernel<Cfg, AL>,
                                                 Cfg::THREADS, Cfg::SMEM);
+  BsoiArgs a = s;
   const int RT = (s.N + Cfg::BM - 1) / Cfg::BM, CT = (2 * s.n + Cfg::BN - 1) / Cfg::BN;
-  long long tiles = (long long)(s.L - 1) * RT * CT;
+  // Rows [row0, row1) in bands of the tile height; row0 must start a band and
+  // row1 end one (or be N).
+  if (s.rb0 % Cfg::BM != 0 || (s.rb1 % Cfg::BM != 0 && s.rb1 != s.N) || s.rb0 >= s.rb1)
+    return cudaErrorInvalidValue;
+  a.rb0 = s.rb0 / Cfg::BM;
+  a.rb1 = (s.rb1 + Cfg::BM - 1) / Cfg::BM;
+  if (a.rb1 > RT) return cudaErrorInvalidValue;
+  long long tiles = (long long)(s.L - 1) * (a.rb1 - a.rb0) * CT;
   int grid = sms * (per > 0 ? per : 1);
   if (tiles < grid) grid = (int)tiles;
-  bsoi_persistent_kernel<Cfg, AL><<<grid, Cfg::THREADS, Cfg::SMEM, st>>>(s);
+  bsoi_persistent_kernel<Cfg, AL><<<grid, Cfg::THREADS, Cfg::SMEM, st>>>(a);
   return cudaGetLastError();
 }
 
 cudaError_t launch_bsoi_persistent(double* A, long long ld, double* carry0, double* carry1,
                                    long long ldc, const double* G, int n, int L, int* done,
-                                   int* next, int* err, bool small, cudaStream_t st) {
+                                   int* next, int* err, bool small, cudaStream_t st, int row0,
+                                   int row1) {
   BsoiArgs s;
   s.A = A;
   s.ld = ld;
@@ -149,6 +163,9 @@ cudaError_t launch_bsoi_persistent(double* A, long long ld, double* carry0, doub
   s.next = next;
   s.err = err;
   s.spin_limit = 1ll << 22;
+  // Row range in rows here; launch_al turns it into row bands of its tiles.
+  s.rb0 = row0;
+  s.rb1 = row1 < 0 ? s.N : row1;
   const bool al = ((uintptr_t)A % 16 == 0) && ((uintptr_t)carry0 % 16 == 0) &&
                   ((uintptr_t)carry1 % 16 == 0) && ((uintptr_t)G % 16 == 0) && ld % 2 == 0 &&
                   ldc % 2 == 0 && n % 2 == 0;

@@ -769,6 +769,36 @@ int bsoi_finish(int n, int L, double* dA, int ldd, void* ws, cudaStream_t st) {
   return 0;
 }
 
+// BSOI of the rows [row0, row1) only (every column): the share of one GPU
+// when an inversion's BSOI is split by rows.  Q formation is repeated in
+// full; the carry seed, the persistent launch and the final copy cover only
+// those rows.  Each computed tile is the one the full launch of the same tile
+// shape computes.  row0 a multiple of 128, row1 too unless it is N.
+int run_bsoi_rows(int n, int L, double* dA, int ldd, const double* dtau, void* ws, cudaStream_t st,
+                  int row0, int row1) {
+  Layout ly = layout(n, L, ldd);
+  const int N = n * L;
+  if (row0 < 0 || row1 > N || row0 >= row1 || row0 % 128 != 0 || (row1 % 128 != 0 && row1 != N))
+    return (int)cudaErrorInvalidValue;
+  double* G = at<double>(ws, ly.G);
+  double* C[2] = {at<double>(ws, ly.C0), at<double>(ws, ly.C1)};
+  if (int e = bsoi_form_q(n, L, dA, ldd, dtau, ws, st)) return e;
+  const int rows = row1 - row0;
+  CK(launch_copy_masked(C[0] + row0, ldd, dA + cm(row0, (long long)(L - 1) * n, ldd), ldd, rows, n,
+                        (L - 1) * n - row0, st));
+  CKM(cudaMemsetAsync(at<int>(ws, ly.info) + 2, 0, sizeof(int), st));
+  // Persistent with the plan's tile shape when it has one, else 64 x 64.
+  const Plan plan = plan_for(n, L);
+  int* bs = at<int>(ws, ly.bsync);
+  CKM(cudaMemsetAsync(bs, 0, sizeof(int) * ly.bsync_ints, st));
+  CK(launch_bsoi_persistent(dA, ldd, C[0], C[1], ldd, G, n, L, bs, bs + ly.bsync_ints - 2,
+                            at<int>(ws, ly.info) + 2, plan.bsoi != 0, st, row0, row1));
+  const int cur = (L - 1) & 1;  // carry buffer written by step 0
+  CK(launch_copy_masked(dA + row0, ldd, C[cur] + row0, ldd, rows, n, kNoMask, st,
+                        at<int>(ws, ly.info)));
+  return 0;
+}
+
 int run_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* ws, cudaStream_t st,
              bool q_ready) {
   Layout ly = layout(n, L, ldd);
@@ -843,6 +873,12 @@ int bsofi_dev_bsoftri_q(int n, int L, double* dA, int ldd, double* dtau, void* d
   g_launches = 0;
   return run_bsoftri(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, true, bsof_workers(n, L, 0),
                      true);
+}
+
+int bsofi_dev_bsoi_rows(int n, int L, double* dA, int ldd, const double* dtau, void* dws,
+                        void* stream, int row0, int row1) {
+  g_launches = 0;
+  return run_bsoi_rows(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, row0, row1);
 }
 
 int bsofi_dev_bsoi_ex(int n, int L, double* dA, int ldd, const double* dtau, void* dws,

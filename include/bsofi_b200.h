@@ -160,6 +160,18 @@ int bsofi_device_bsoftri(int n, int L, double *dA, int ldda, double *dtau, void 
                          void *stream);
 int bsofi_device_bsoi(int n, int L, double *dA, int ldda, const double *dtau, void *dwork,
                       void *stream);
+
+/* BSOI of the rows [row0, row1) of M^{-1} only, every column (no reference
+ * counterpart; the split that the survey of the reference sketches for one
+ * inversion over several GPUs: the factorization on every GPU, BSOI by rows,
+ * since rows of X are independent in X(:,k:k+1) Q_k^T).  dA holds the BSOF +
+ * BSTRI state as for bsofi_device_bsoi; rows outside the range are left as
+ * they were.  row0 must be a multiple of 128 and row1 too unless it is n*L.
+ * Returns 0, -1 for an illegal argument or range, or BSOFI_INFO_CUDA -
+ * cudaError_t.  bsofi_b200/shard.py runs it on every rank of a
+ * torch.distributed group and all-gathers the rows. */
+int bsofi_device_bsoi_rows(int n, int L, double *dA, int ldda, const double *dtau, void *dwork,
+                           int row0, int row1, void *stream);
 int *bsofi_device_info(void *dwork);
 /* Kernels launched by the last bsofi_device_* call on this thread. */
 long long bsofi_device_last_launches(void);
