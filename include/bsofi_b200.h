@@ -162,9 +162,9 @@ int bsofi_device_bsoi(int n, int L, double *dA, int ldda, const double *dtau, vo
                       void *stream);
 
 /* BSOI of the rows [row0, row1) of M^{-1} only, every column (no reference
- * counterpart; the split that the survey of the reference sketches for one
- * inversion over several GPUs: the factorization on every GPU, BSOI by rows,
- * since rows of X are independent in X(:,k:k+1) Q_k^T).  dA holds the BSOF +
+ * counterpart; one inversion over several GPUs: the factorization on every
+ * GPU, BSOI by rows, since rows of X are independent in X(:,k:k+1) Q_k^T,
+ * src/bsofi_cpu.c:211-248).  dA holds the BSOF +
  * BSTRI state as for bsofi_device_bsoi; rows outside the range are left as
  * they were.  row0 must be a multiple of 128 and row1 too unless it is n*L.
  * Returns 0, -1 for an illegal argument or range, or BSOFI_INFO_CUDA -
