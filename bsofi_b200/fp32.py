@@ -39,9 +39,17 @@ _SIGS = {
     "hybridXbsofiLWork": (_i, [_i] * 4),
     "hybridXbsoftri": (_i, [_i, _i, _i, _fp, _i, _fp, _fp, _i, _fp, _i, _ip]),
     "hybridXbsoi": (_i, [_i, _i, _i, _fp, _i, _fp, _fp, _i, _fp, _i, _ip]),
+    "lapackxbsofilwork_": (_i, [_ip] * 3),
+    "lapackxbsof_": (_i, [_ip, _ip, _fp, _ip, _fp, _fp, _ip, _ip]),
+    "lapackxbstri_": (_i, [_ip, _ip, _fp, _ip, _ip]),
+    "lapackxbsoi_ormqr_": (_i, [_ip, _ip, _fp, _ip, _fp, _fp, _ip, _ip]),
+    "lapackxbsoi_orgqr_": (_i, [_ip, _ip, _fp, _ip, _fp, _fp, _ip, _ip]),
     "gpuXbsof": (_i, [_i, _i, _vp, _i, _fp, _fp, _i, _vp, _ip]),
     "gpuXbstri_rseq": (_i, [_i, _i, _vp, _i, _vp, _i, _ip]),
+    "gpuXbstri_rbatched": (_i, [_i, _i, _vp, _i, _vp, _i, _ip]),
     "gpuXbsoi_ormqr": (_i, [_i, _i, _vp, _i, _fp, _fp, _i, _vp, _vp, _i, _ip]),
+    "gpuXbsoi_orgqr": (_i, [_i, _i, _vp, _i, _fp, _fp, _i, _vp, _vp, _i, _ip]),
+    "gpuXbsoi_batched": (_i, [_i, _i, _vp, _i, _fp, _fp, _i, _vp, _vp, _i, _ip]),
     "bsofi_fp32_last_launches": (ctypes.c_longlong, []),
 }
 

@@ -55,6 +55,24 @@ def test_library_loads_and_exports_exactly_the_header():
         assert name in exported
 
 
+def test_binding_declares_every_export():
+    """Every name of the header has a ctypes signature (no default int
+    conversions of pointers)."""
+    assert set(fp32._SIGS) == set(fp32.declared())
+
+
+def test_fortran_twins_validate():
+    lib = fp32.load()
+    A = np.zeros((8, 8), dtype=np.float32, order="F")
+    tau = np.zeros(8, dtype=np.float32)
+    w = np.zeros(1, dtype=np.float32)
+    info = ctypes.c_int(0)
+    lib.lapackxbsof_(_i(0), _i(2), A.ctypes.data_as(_fp), _i(8), tau.ctypes.data_as(_fp),
+                     w.ctypes.data_as(_fp), _i(1), ctypes.byref(info))
+    assert info.value == -1
+    assert lib.lapackxbsofilwork_(_i(4), _i(2), _i(8)) >= 1
+
+
 def test_no_oracle_linkage():
     out = subprocess.run(["ldd", fp32.LIB_PATH], capture_output=True, text=True).stdout
     assert "oracle" not in out and "openblas" not in out.lower()
