@@ -45,6 +45,20 @@ _SIGS = {
                                 _c_dbl_p, ctypes.c_int, _vp, _c_int_p]),
     "gpuXbstri_rseq": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp,
                                       ctypes.c_int, _c_int_p]),
+    "gpuXbstri_rbatched": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp,
+                                          ctypes.c_int, _c_int_p]),
+    "gpuXbsoi_ormqr": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _c_dbl_p,
+                                      _c_dbl_p, ctypes.c_int, _vp, _vp, ctypes.c_int, _c_int_p]),
+    "gpuXbsoi_orgqr": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _c_dbl_p,
+                                      _c_dbl_p, ctypes.c_int, _vp, _vp, ctypes.c_int, _c_int_p]),
+    "lapackxbsofilwork_": (ctypes.c_int, [_c_int_p] * 3),
+    "lapackxbsof_": (ctypes.c_int, [_c_int_p, _c_int_p, _c_dbl_p, _c_int_p, _c_dbl_p, _c_dbl_p,
+                                    _c_int_p, _c_int_p]),
+    "lapackxbstri_": (ctypes.c_int, [_c_int_p, _c_int_p, _c_dbl_p, _c_int_p, _c_int_p]),
+    "lapackxbsoi_ormqr_": (ctypes.c_int, [_c_int_p, _c_int_p, _c_dbl_p, _c_int_p, _c_dbl_p,
+                                          _c_dbl_p, _c_int_p, _c_int_p]),
+    "lapackxbsoi_orgqr_": (ctypes.c_int, [_c_int_p, _c_int_p, _c_dbl_p, _c_int_p, _c_dbl_p,
+                                          _c_dbl_p, _c_int_p, _c_int_p]),
     "gpuXbsoi_batched": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _c_dbl_p,
                                         _c_dbl_p, ctypes.c_int, _vp, _vp, ctypes.c_int,
                                         _c_int_p]),
@@ -104,7 +118,7 @@ def declared_symbols(header=HEADER):
     """Function names declared in include/bsofi_b200.h."""
     text = open(header).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"^\s*(?:unsigned\s+long\s+long|long\s+long|int\s*\*?|double|void)\s+\*?\s*(\w+)\s*\(",
+    return sorted(set(re.findall(r"^\s*(?:unsigned\s+long\s+long|long\s+long|int\s*\*?|double|void|bsofi_\w+)\s*\*?\s*(\w+)\s*\(",
                                  text, flags=re.M)))
 
 

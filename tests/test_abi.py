@@ -32,6 +32,11 @@ def test_exports_match_header():
         assert name in exported
 
 
+def test_binding_declares_every_export():
+    """Every function of the header has a ctypes signature in the binding."""
+    assert set(_lib.declared_symbols()) <= set(_lib._SIGS)
+
+
 def test_no_oracle_linkage():
     out = subprocess.run(["ldd", _lib.LIB_PATH], capture_output=True, text=True).stdout
     assert "oracle" not in out and "openblas" not in out.lower()
