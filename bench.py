@@ -61,6 +61,8 @@ def parse():
     p.add_argument("--batch-mixed", type=int, default=64,
                    help="instances in the mixed-size batched sample (0 = skip)")
     p.add_argument("--batch-steps", type=int, default=3)
+    p.add_argument("--c4-steps", type=int, default=4,
+                   help="timed inversions at n=400, p=64, U=6 for the c4 key (0 = skip)")
     p.add_argument("--serve", type=int, default=60,
                    help="requests in the served Poisson stream (0 = skip)")
     p.add_argument("--serve-rate", type=float, default=12.0, help="mean arrivals per second")
@@ -220,9 +222,13 @@ def cpu_reference(side, L, U, steps, threads=None):
     M = hubbard_matrix(side, L, U, seed=12345)
     times = []
     for _ in range(steps):
+        # The reference overwrites its input in place: a fresh copy of M and a
+        # tau array are made before the clock starts, as a caller holds them.
+        A = np.asfortranarray(M)
+        tau = np.zeros(n * L)
         t0 = time.perf_counter()
-        A, tau, info = oracle.ref_bsoftri(M, n, L)
-        oracle.ref_bsoi(A, tau, n, L)
+        _, _, info = oracle.ref_bsoftri(A, n, L, inplace=True)
+        oracle.ref_bsoi(A, tau, n, L, inplace=True)
         times.append(time.perf_counter() - t0)
     return {"times": times, "cores": cores}
 
@@ -338,8 +344,8 @@ def main():
 
     peak = measure_dgemm_peak(torch, dev)
     achieved = flops_bsoi(n, L) * args.steps / (gemm_ms * 1e-3) / 1e12 if gemm_ms > 0 else None
-    roofline = {"kernel": "bsoi_persistent_kernel (all p-1 BSOI steps in one cooperative "
-                          "launch, FP64 DMMA m16n8k8); dominant by algorithmic work "
+    roofline = {"kernel": "bsoi_persistent_kernel (all p-1 BSOI steps in one ordinary "
+                          "persistent launch, FP64 DMMA m16n8k8); dominant by algorithmic work "
                           "(79% of the flop model)",
                 "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if achieved else None,
@@ -361,6 +367,10 @@ def main():
                      "peak_gbs": hbm_peak(),
                      "algorithmic_bytes": bsof_bytes,
                      "achieved_tflops": flops_bsof(n, L) / (bsof_ms * 1e-3) / 1e12 if bsof_ms else None}
+
+    c4 = None
+    if args.c4_steps > 0:
+        c4 = run_c4(api, torch, dev, stream, args.c4_steps, max(args.warmup, 3), peak, rank)
 
     batched = None
     if args.batch > 0:
@@ -410,7 +420,7 @@ def main():
                 "config": config(args, n, N),
                 "tflops": bsofi_flops(n, L) * value / world / 1e12,
                 "residual": resid,
-                "roofline": roofline, "roofline_bsof": roofline_bsof,
+                "roofline": roofline, "roofline_bsof": roofline_bsof, "c4": c4,
                 "cpu_baseline": cpu, "e2e": e2e, "e2e_pageable": e2e_pageable,
                 "e2e_fp32": e2e_fp32,
                 "batched": batched, "batched_mixed_sizes": batched_mixed, "served": served,
@@ -419,6 +429,55 @@ def main():
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
+
+
+def run_c4(api, torch, dev, stream, steps, warmup, peak, rank):
+    """The plain FP64 path at n = 400, p = 64, U = 6 (N = 25600, 5.2 GB per
+    matrix, larger than L2): device-resident single inversions with the
+    default launch plan, each timed with CUDA events on its stream from a
+    fresh copy of the input made outside the timed window.  TFLOP/s uses the
+    reference's flop model; frac is against the DGEMM peak measured in this
+    run."""
+    from bsofi_b200 import replicas
+    side, L, U = 20, 64, 6.0
+    n = side * side
+    N = n * L
+    blocks = hubbard_pcyclic(side, L, U, 7000 + rank)
+    pristine = pcyclic_device(torch, *blocks, N, dev)
+    work = torch.empty_like(pristine)
+    dtau = torch.zeros(N, dtype=torch.float64, device=dev)
+    ws = torch.zeros(api.workspace_bytes(n, L, N) // 8 + 1, dtype=torch.float64, device=dev)
+    sp = stream.cuda_stream
+    total = 0.0
+    for it in range(warmup + steps):
+        work.copy_(pristine)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            rc = api.device_invert(n, L, work.data_ptr(), N, dtau.data_ptr(), ws.data_ptr(), sp)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        if rc != 0:
+            raise RuntimeError("bsofi_device_invert (n=400, p=64) failed: %d" % rc)
+        if it >= warmup:
+            total += e0.elapsed_time(e1)
+    ms = replicas.max_over_ranks(total, dev) / steps
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from gpu_util import block_residual_colmajor
+    resid = block_residual_colmajor(torch, *blocks, work, N)
+    _, plan = api.plan_get(n, L)
+    tf = bsofi_flops(n, L) / (ms * 1e-3) / 1e12
+    del pristine, work, ws
+    torch.cuda.empty_cache()
+    return {"workload": "single FP64 inversion, 20x20 lattice, n=400, p=64, N=25600, U=6 "
+                        "(inputs larger than L2)",
+            "steps": steps, "warmup": warmup, "ms_per_inversion": ms,
+            "value": 1e3 / ms, "unit": "inversions/s", "tflops": tf,
+            "frac": tf / peak if peak else None,
+            "peak": peak, "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+            "residual": resid, "plan": plan}
 
 
 def run_batched(api, torch, dev, specs, steps, stream):

@@ -35,6 +35,11 @@ _SIGS = {
     "lapackXbsoi_orgqr": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _c_dbl_p, ctypes.c_int,
                                          _c_dbl_p, _c_dbl_p, ctypes.c_int, _c_int_p]),
     "hybridXbsofiLWork": (ctypes.c_int, [ctypes.c_int] * 4),
+    "hybridxbsofilwork_": (ctypes.c_int, [_c_int_p] * 4),
+    "hybridxbsoftri_": (ctypes.c_int, [_c_int_p, _c_int_p, _c_dbl_p, _c_int_p, _c_dbl_p, _c_dbl_p,
+                                       _c_int_p, _c_dbl_p, _c_int_p, _c_int_p]),
+    "hybridxbsoi_": (ctypes.c_int, [_c_int_p, _c_int_p, _c_dbl_p, _c_int_p, _c_dbl_p, _c_dbl_p,
+                                    _c_int_p, _c_dbl_p, _c_int_p, _c_int_p]),
     "hybridXbsoftri": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _c_dbl_p,
                                       ctypes.c_int, _c_dbl_p, _c_dbl_p, ctypes.c_int, _c_dbl_p,
                                       ctypes.c_int, _c_int_p]),
@@ -97,11 +102,13 @@ _SIGS = {
     "bsofi_device_logdet": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp,
                                            ctypes.c_int, _vp, _vp]),
     "bsofi_noalloc_scratch_bytes": (ctypes.c_ulonglong, []),
+    "bsofi_noalloc_prepare": (ctypes.c_int, []),
     "bsofi_device_invert_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int,
                                                    _vp, _vp, _vp]),
     "bsofi_device_bsof_timeline": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
                                                   _vp, ctypes.c_int]),
     "bsofi_device_set_bsof_workers": (None, [ctypes.c_int]),
+    "bsofi_device_set_wait_test": (None, [ctypes.c_int]),
     "bsofi_device_set_bstri_overlap": (None, [ctypes.c_int]),
     "bsofi_device_timing": (None, [ctypes.c_int]),
     "bsofi_device_timing_read": (ctypes.c_int, [_c_dbl_p, ctypes.POINTER(ctypes.c_longlong)]),

@@ -13,6 +13,7 @@
  */
 #include <pthread.h>
 #include <stdint.h>
+#include <limits.h>
 #include <stdlib.h>
 #include <string.h>
 #include <sys/time.h>
@@ -190,6 +191,15 @@ typedef char handle_fits_in_40_bytes[(sizeof(bsofi_handle) <= 40) ? 1 : -1];
 static int cuda_info(cudaError_t e) { return BSOFI_INFO_CUDA - (int)e; }
 
 static int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+/* Device workspace of the lwork = -2 query in doubles: the N x N matrix (leading
+ * dimension rounded up to 32), tau and the pipeline workspace.  As a double it
+ * is exact at every supported size (2.1e9 doubles at n = 576, L = 80 is past
+ * INT_MAX, so the int-returning query saturates). */
+static double device_lwork(int n, int L) {
+  int ldd = round_up(n * L, 32), N = n * L;
+  return (double)((size_t)ldd * N + N + bsofi_dev_ws_bytes(n, L, ldd) / sizeof(double));
+}
 
 static void ctx_free_buffers(bsofi_ctx *c) {
   if (c->dA) cudaFree(c->dA);
@@ -730,8 +740,7 @@ int hybridxbsoftrih_(int *handle, int *n, int *L, double *A, int *lda, double *t
     return *info = 0;
   }
   if (*lwork == -2) {
-    int ldd = round_up((*n) * (*L), 32), N = (*n) * (*L);
-    work[0] = (double)((size_t)ldd * N + N + bsofi_dev_ws_bytes(*n, *L, ldd) / sizeof(double));
+    work[0] = device_lwork(*n, *L);
     return *info = 0;
   }
   return *info = drive_bsoftri(c, *n, *L, A, *lda, tau, 1, 1);
@@ -753,8 +762,7 @@ int hybridxbsoih_(int *handle, int *n, int *L, double *A, int *lda, double *tau,
     return *info = 0;
   }
   if (*lwork == -2) {
-    int ldd = round_up((*n) * (*L), 32), N = (*n) * (*L);
-    work[0] = (double)((size_t)ldd * N + N + bsofi_dev_ws_bytes(*n, *L, ldd) / sizeof(double));
+    work[0] = device_lwork(*n, *L);
     return *info = 0;
   }
   return *info = drive_bsoi(c, *n, *L, A, *lda, tau);
@@ -804,8 +812,8 @@ int lapackXbsofiLWork(int n, int L, int lda) {
 int hybridXbsofiLWork(int n, int L, int lda, int lworkHostDevice) {
   (void)lda;
   if (lworkHostDevice == -2) {
-    int ldd = round_up(n * L, 32), N = n * L;
-    return (int)((size_t)ldd * N + N + bsofi_dev_ws_bytes(n, L, ldd) / sizeof(double));
+    const double w = device_lwork(n, L);
+    return w > (double)INT_MAX ? INT_MAX : (int)w;
   }
   return 1;
 }
@@ -818,7 +826,7 @@ static int c_phase(int n, int L, double *A, int lda, double *tau, double *work, 
   r = check_args(NULL, n, L, A, lda, phase == 1 ? A : tau, work, lwork, 1);
   if (r) return *info = r;
   if (lwork == -1 || lwork == -2) {
-    work[0] = lwork == -1 ? 1.0 : (double)hybridXbsofiLWork(n, L, lda, -2);
+    work[0] = lwork == -1 ? 1.0 : device_lwork(n, L);
     return *info = 0;
   }
   c = thread_ctx(n, L, info);
@@ -880,6 +888,32 @@ int hybridXbsoi(int handle, int n, int L, double A[], int lda, double tau[], dou
   (void)dwork;
   (void)ldwork;
   return c_phase(n, L, A, lda, tau, work, lwork, info, 3);
+}
+
+/* Fortran twins of the hybridX names (the reference's cb_hybridXbsofiLWork,
+ * cb_hybridXbsoftri, cb_hybridXbsoi, src/bsofi_callback.c:62-87): every
+ * argument by pointer; the cuBLAS handle is not passed. */
+int hybridxbsofilwork_(int *n, int *L, int *lda, int *lworkHostDevice) {
+  if (!n || !L || !lda || !lworkHostDevice) return 1;
+  return hybridXbsofiLWork(*n, *L, *lda, *lworkHostDevice);
+}
+int hybridxbsoftri_(int *n, int *L, double A[], int *lda, double tau[], double work[], int *lwork,
+                    double dwork[], int *ldwork, int *info) {
+  if (!info) return -10;
+  if (!n || !L || !lda || !lwork || !ldwork) {
+    *info = !n ? -1 : !L ? -2 : !lda ? -4 : !lwork ? -7 : -9;
+    return *info;
+  }
+  return hybridXbsoftri(0, *n, *L, A, *lda, tau, work, *lwork, dwork, *ldwork, info);
+}
+int hybridxbsoi_(int *n, int *L, double A[], int *lda, double tau[], double work[], int *lwork,
+                 double dwork[], int *ldwork, int *info) {
+  if (!info) return -10;
+  if (!n || !L || !lda || !lwork || !ldwork) {
+    *info = !n ? -1 : !L ? -2 : !lda ? -4 : !lwork ? -7 : -9;
+    return *info;
+  }
+  return hybridXbsoi(0, *n, *L, A, *lda, tau, work, *lwork, dwork, *ldwork, info);
 }
 
 /* ------------------------------------------------------ device-pointer API */
@@ -1042,3 +1076,5 @@ int bsofi_device_bsof_timeline(int n, int L, int ldda, void *dwork, unsigned lon
 void bsofi_device_set_bsof_workers(int workers) { bsofi_dev_set_bsof_workers(workers); }
 
 void bsofi_device_set_bstri_overlap(int on) { bsofi_dev_set_bstri_overlap(on); }
+
+void bsofi_device_set_wait_test(int on) { bsofi_dev_set_wait_test(on); }

@@ -447,6 +447,32 @@ int hybridXbsoi(int handle, int n, int L, float A[], int lda, float tau[], float
   return c_phase(n, L, A, lda, tau, work, lwork, info, PH_BSOI);
 }
 
+/* Fortran twins of the hybridX names (the reference's cb_hybridXbsofiLWork,
+ * cb_hybridXbsoftri, cb_hybridXbsoi, src/bsofi_callback.c:62-87): every
+ * argument by pointer; the cuBLAS handle is not passed. */
+int hybridxbsofilwork_(int *n, int *L, int *lda, int *lworkHostDevice) {
+  if (!n || !L || !lda || !lworkHostDevice) return 1;
+  return hybridXbsofiLWork(*n, *L, *lda, *lworkHostDevice);
+}
+int hybridxbsoftri_(int *n, int *L, float A[], int *lda, float tau[], float work[], int *lwork,
+                    float dwork[], int *ldwork, int *info) {
+  if (!info) return -10;
+  if (!n || !L || !lda || !lwork || !ldwork) {
+    *info = !n ? -1 : !L ? -2 : !lda ? -4 : !lwork ? -7 : -9;
+    return *info;
+  }
+  return hybridXbsoftri(0, *n, *L, A, *lda, tau, work, *lwork, dwork, *ldwork, info);
+}
+int hybridxbsoi_(int *n, int *L, float A[], int *lda, float tau[], float work[], int *lwork,
+                 float dwork[], int *ldwork, int *info) {
+  if (!info) return -10;
+  if (!n || !L || !lda || !lwork || !ldwork) {
+    *info = !n ? -1 : !L ? -2 : !lda ? -4 : !lwork ? -7 : -9;
+    return *info;
+  }
+  return hybridXbsoi(0, *n, *L, A, *lda, tau, work, *lwork, dwork, *ldwork, info);
+}
+
 /* ------------------------------------------------------ device-pointer API */
 /* A phase on the caller's float device matrix dA (pitch ldda), in place;
  * tau is host memory as in the reference. */

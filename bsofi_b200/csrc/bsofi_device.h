@@ -20,6 +20,11 @@ size_t bsofi_dev_ws_bytes(int n, int L, int ldd);
 /* One-time per-process set-up (kernel attributes).  Call before capturing
  * the pipeline into a CUDA graph. */
 int bsofi_dev_prepare(void);
+/* bsofi_dev_prepare plus loading every kernel of the pipeline onto the
+ * current device now (under lazy module loading each kernel is otherwise
+ * loaded, and device memory taken, at its first launch) and reserving the
+ * largest per-thread local memory any of them needs. */
+int bsofi_dev_preload(void);
 
 /* Zero the blocks of A that the factorization reads as structural zeros
  * (superdiagonal blocks and the last block column except its first and last
@@ -115,6 +120,9 @@ int bsofi_dev_timing_read(double *ms, long long *launches);
  * number of leaves. */
 int bsofi_dev_bsof_timeline(int n, int L, int ldd, void *dws, unsigned long long **ptr);
 void bsofi_dev_set_bsof_workers(int w);
+/* Diagnostics: persistent BSOI launches of this thread poll a word that
+ * nothing writes in every step wait (short limit), so the waits give up. */
+void bsofi_dev_set_wait_test(int on);
 /* Overlap of BSTRI's leading rows with the end of BSOF in single inversions
  * (1, the default) or the two phases in order (0); process-wide. */
 void bsofi_dev_set_bstri_overlap(int on);

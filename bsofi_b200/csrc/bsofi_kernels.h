@@ -70,14 +70,16 @@ cudaError_t launch_bstri_recurrence_blocked(double* A, long long ld, const doubl
 
 // Persistent BSOI (kernels_bsoi.cu): all p-1 steps in one launch.
 // done: (L-1) * bsoi_row_bands(N) ints and next: one int, zeroed before;
-// small: 64 x 64 tiles instead of 128 x 128.
+// small: 64 x 64 tiles instead of 128 x 128.  never (diagnostics): a zeroed
+// word that nothing writes; when given, every step wait polls it under a short
+// limit, so the waits give up and report through err.
 int bsoi_row_bands(int N);
 // [row0, row1): the rows computed (row1 = -1: to N); row0 a multiple of the
 // tile height (128, or 64 when small), row1 too unless it is N.
 cudaError_t launch_bsoi_persistent(double* A, long long ld, double* carry0, double* carry1,
                                    long long ldc, const double* G, int n, int L, int* done,
                                    int* next, int* err, bool small, cudaStream_t st,
-                                   int row0 = 0, int row1 = -1);
+                                   int row0 = 0, int row1 = -1, const int* never = nullptr);
 
 // In-place inversion of the upper triangles of nblk n x n blocks (block b at
 // A + b * bstride); tmp: device scratch of nblk * n * n / 4 doubles.  A zero
@@ -108,5 +110,24 @@ cudaError_t launch_state_ref(const double* A, long long ld, int n, int L, const 
 // Zero the n x n blocks of A that BSOF reads as structural zeros:
 // superdiagonal blocks (k,k+1) and last-column blocks (k,L-1), 1 <= k <= L-2.
 cudaError_t launch_zero_structural(double* A, long long ld, int n, int L, cudaStream_t st);
+
+// Loading every kernel onto the current device ahead of use.  Under lazy
+// module loading (the CUDA 12 default) a kernel's code is loaded, and device
+// memory taken for it, at its first launch; cudaFuncGetAttributes loads it
+// now.  *local is raised to the kernel's per-thread local memory.
+template <class F>
+cudaError_t preload_one(F* f, size_t* local) {
+  cudaFuncAttributes at;
+  cudaError_t e = cudaFuncGetAttributes(&at, (const void*)f);
+  if (e == cudaSuccess && at.localSizeBytes > *local) *local = at.localSizeBytes;
+  return e;
+}
+// One per kernel file: every kernel (each template instance) it launches.
+cudaError_t preload_bsof(size_t* local);
+cudaError_t preload_bsoi(size_t* local);
+cudaError_t preload_bstri(size_t* local);
+cudaError_t preload_gemm(size_t* local);
+cudaError_t preload_panel(size_t* local);
+cudaError_t preload_tri(size_t* local);
 
 }  // namespace bsofi

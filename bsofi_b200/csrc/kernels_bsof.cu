@@ -920,4 +920,14 @@ cudaError_t launch_bsof_persistent(double* A, long long ld, int n, int L, double
   }
 }
 
+cudaError_t preload_bsof(size_t* local) {
+  cudaError_t e;
+  if ((e = preload_one(bsof_persistent_kernel<1, 16>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(bsof_persistent_kernel<2, 16>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(bsof_persistent_kernel<3, 8>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(bsof_persistent_kernel<4, 8>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(bsof_persistent_kernel<5, 8>, local)) != cudaSuccess) return e;
+  return preload_one(bsof_persistent_kernel<6, 8>, local);
+}
+
 }  // namespace bsofi

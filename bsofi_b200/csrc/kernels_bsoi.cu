@@ -33,6 +33,7 @@ struct BsoiArgs {
   int* err;
   long long spin_limit;
   int rb0, rb1;      // row bands computed (of the tile height)
+  const int* never;  // diagnostics: when set, every step wait polls this word instead
 };
 
 BSOFI_DEVINL int ld_acq(const int* p) {
@@ -61,7 +62,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) bsoi_persistent_kernel(BsoiAr
     const int k = s.L - 2 - step;
     if (step > 0) {
       if (threadIdx.x == 0) {
-        const int* flag = s.done + (long long)(step - 1) * RT + rb;
+        const int* flag = s.never ? s.never : s.done + (long long)(step - 1) * RT + rb;
         long long it = 0;
         int ok = 1;
         while (ld_acq(flag) < CT) {
@@ -148,7 +149,7 @@ static cudaError_t launch_al(const BsoiArgs& s, cudaStream_t st) {
 cudaError_t launch_bsoi_persistent(double* A, long long ld, double* carry0, double* carry1,
                                    long long ldc, const double* G, int n, int L, int* done,
                                    int* next, int* err, bool small, cudaStream_t st, int row0,
-                                   int row1) {
+                                   int row1, const int* never) {
   BsoiArgs s;
   s.A = A;
   s.ld = ld;
@@ -162,7 +163,8 @@ cudaError_t launch_bsoi_persistent(double* A, long long ld, double* carry0, doub
   s.done = done;
   s.next = next;
   s.err = err;
-  s.spin_limit = 1ll << 22;
+  s.spin_limit = never ? 1ll << 12 : 1ll << 22;
+  s.never = never;
   // Row range in rows here; launch_al turns it into row bands of its tiles.
   s.rb0 = row0;
   s.rb1 = row1 < 0 ? s.N : row1;
@@ -171,6 +173,14 @@ cudaError_t launch_bsoi_persistent(double* A, long long ld, double* carry0, doub
                   ldc % 2 == 0 && n % 2 == 0;
   if (small) return al ? launch_al<CfgS, true>(s, st) : launch_al<CfgS, false>(s, st);
   return al ? launch_al<CfgM, true>(s, st) : launch_al<CfgM, false>(s, st);
+}
+
+cudaError_t preload_bsoi(size_t* local) {
+  cudaError_t e;
+  if ((e = preload_one(bsoi_persistent_kernel<CfgM, true>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(bsoi_persistent_kernel<CfgM, false>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(bsoi_persistent_kernel<CfgS, true>, local)) != cudaSuccess) return e;
+  return preload_one(bsoi_persistent_kernel<CfgS, false>, local);
 }
 
 }  // namespace bsofi

@@ -221,4 +221,12 @@ cudaError_t launch_bstri_recurrence_blocked(double* A, long long ld, const doubl
   return al ? rec_launch<CfgM, true>(s, st) : rec_launch<CfgM, false>(s, st);
 }
 
+cudaError_t preload_bstri(size_t* local) {
+  cudaError_t e;
+  if ((e = preload_one(bstri_recurrence_kernel<CfgM, true>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(bstri_recurrence_kernel<CfgM, false>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(bstri_recurrence_kernel<CfgS, true>, local)) != cudaSuccess) return e;
+  return preload_one(bstri_recurrence_kernel<CfgS, false>, local);
+}
+
 }  // namespace bsofi

@@ -63,4 +63,14 @@ cudaError_t launch_gemm(const GemmDims& d, const GemmA& a, const GemmB& b, const
   return run<CfgS>(d, a, b, c, batch, st);
 }
 
+cudaError_t preload_gemm(size_t* local) {
+  cudaError_t e;
+  if ((e = preload_one(gemm_kernel<CfgL, true>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(gemm_kernel<CfgL, false>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(gemm_kernel<CfgM, true>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(gemm_kernel<CfgM, false>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(gemm_kernel<CfgS, true>, local)) != cudaSuccess) return e;
+  return preload_one(gemm_kernel<CfgS, false>, local);
+}
+
 }  // namespace bsofi

@@ -127,4 +127,6 @@ cudaError_t launch_wy_apply(const WyArgs& a, int batch, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+cudaError_t preload_panel(size_t* local) { return preload_one(wy_apply_kernel, local); }
+
 }  // namespace bsofi

@@ -252,4 +252,13 @@ cudaError_t launch_zero_structural(double* A, long long ld, int n, int L, cudaSt
   return cudaGetLastError();
 }
 
+cudaError_t preload_tri(size_t* local) {
+  cudaError_t e;
+  if ((e = preload_one(trtri_leaves_kernel, local)) != cudaSuccess) return e;
+  if ((e = preload_one(state_ref_kernel, local)) != cudaSuccess) return e;
+  if ((e = preload_one(set_identity_kernel, local)) != cudaSuccess) return e;
+  if ((e = preload_one(copy_masked_kernel, local)) != cudaSuccess) return e;
+  return preload_one(zero_structural_kernel, local);
+}
+
 }  // namespace bsofi

@@ -9,19 +9,22 @@
 // file-scope array below instead of a caller buffer, and it calls no
 // cudaMalloc, cudaFree or allocating library routine.
 //
-// The array is BSOFI_NOALLOC_SCRATCH_BYTES (32 MiB) and every GPU that loads
-// this library holds it until the process exits.  All calls share it and it
-// keeps the previous call's contents: the pipeline writes every scratch
-// region before reading it (the BSTRI info word is reset at the start of each
-// call), so nothing needs clearing between calls, but calls that overlap on
-// the GPU (different streams or threads on the same device) race on it.
+// The array is BSOFI_NOALLOC_SCRATCH_BYTES (32 MiB).  The driver reserves it
+// when it loads this file's module on a device, which under lazy module
+// loading (the CUDA 12 default) is the first time the module is used there;
+// kernel code and local memory are likewise taken at first use.
+// bsofi_noalloc_prepare does all of that up front, so that a caller can run it
+// before its own pool takes the rest of HBM.  After that the device holds the
+// array until the process exits.  All calls share it and it keeps the previous
+// call's contents: the pipeline writes every scratch region before reading it
+// (the BSTRI info word is reset at the start of each call), so nothing needs
+// clearing between calls, but calls that overlap on the GPU (different streams
+// or threads on the same device) race on it.
 #include <cuda_runtime.h>
-#include <pthread.h>
 
 #include "bsofi_device.h"
 
 #define BSOFI_NOALLOC_SCRATCH_BYTES (32ull << 20)
-#define BSOFI_NOALLOC_MAX_DEVICES 64
 #define BSOFI_INFO_CUDA (-1000)
 #define BSOFI_NOALLOC_TOO_LARGE (-2000)
 
@@ -29,26 +32,13 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[BSOFI_NOALLOC_S
 
 namespace {
 
-pthread_mutex_t g_mu = PTHREAD_MUTEX_INITIALIZER;
-void* g_scratch_addr[BSOFI_NOALLOC_MAX_DEVICES];
-
 // Device address of the scratch array on the current device.  In host code
-// the array's name is only a host-side stand-in, so the address is looked up
-// once per device (with that device current) and cached.
+// the array's name is only a host-side stand-in; the address is looked up on
+// every call (cheap once the module is loaded), so a context that was reset
+// and reloaded the module at another address is never handed a stale one.
 cudaError_t scratch_address(void** out) {
-  int dev = -1;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= BSOFI_NOALLOC_MAX_DEVICES) return cudaErrorInvalidDevice;
-  pthread_mutex_lock(&g_mu);
-  if (g_scratch_addr[dev] == nullptr) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e == cudaSuccess) g_scratch_addr[dev] = p;
-  }
-  *out = g_scratch_addr[dev];
-  pthread_mutex_unlock(&g_mu);
-  return e;
+  *out = nullptr;
+  return cudaGetSymbolAddress(out, g_noalloc_scratch);
 }
 
 }  // namespace
@@ -56,6 +46,14 @@ cudaError_t scratch_address(void** out) {
 extern "C" __attribute__((visibility("default"))) unsigned long long
 bsofi_noalloc_scratch_bytes(void) {
   return BSOFI_NOALLOC_SCRATCH_BYTES;
+}
+
+extern "C" __attribute__((visibility("default"))) int bsofi_noalloc_prepare(void) {
+  void* ws = nullptr;
+  cudaError_t e = scratch_address(&ws);
+  if (e != cudaSuccess) return BSOFI_INFO_CUDA - (int)e;
+  const int r = bsofi_dev_preload();
+  return r ? BSOFI_INFO_CUDA - r : 0;
 }
 
 extern "C" __attribute__((visibility("default"))) int bsofi_device_invert_noalloc(
@@ -72,9 +70,19 @@ extern "C" __attribute__((visibility("default"))) int bsofi_device_invert_noallo
     r = bsofi_dev_bsoi(n, L, dA, ldda, dtau, ws, stream);
     bsofi_dev_add_launches(c);
   }
-  // The info word after BSOI also carries the BSOF/BSOI wait error.
-  if (r == 0 && dinfo != nullptr)
+  if (r) return BSOFI_INFO_CUDA - r;
+  // The info word after BSOI also carries the BSOF/BSOI wait errors.
+  if (dinfo != nullptr)
     r = (int)cudaMemcpyAsync(dinfo, bsofi_dev_info_ptr(ws), sizeof(int), cudaMemcpyDeviceToDevice,
                              (cudaStream_t)stream);
-  return r ? BSOFI_INFO_CUDA - r : 0;
+  if (r) return BSOFI_INFO_CUDA - r;
+  if (dinfo != nullptr) return 0;
+  // No device word to receive it: wait for the stream and return the info
+  // word itself (0, i > 0 for an exactly zero R(i,i), or the wait-failure code).
+  int info = 0;
+  r = (int)cudaMemcpyAsync(&info, bsofi_dev_info_ptr(ws), sizeof(int), cudaMemcpyDeviceToHost,
+                           (cudaStream_t)stream);
+  if (r == 0) r = (int)cudaStreamSynchronize((cudaStream_t)stream);
+  if (r) return BSOFI_INFO_CUDA - r;
+  return info >= 0x7f7f7f7f ? 0 : info;
 }

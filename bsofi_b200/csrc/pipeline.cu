@@ -101,6 +101,10 @@ Plan plan_for(int n, int L) {
 
 // Diagnostics override of the BSOF worker count (0 = the plan's).
 thread_local int g_workers_override = 0;
+// Diagnostics: persistent BSOI launches of this thread wait on a word that
+// nothing writes (the spare int after the BSOI tile counter), so their
+// bounded waits give up.
+thread_local bool g_wait_test = false;
 
 // Worker CTAs of one BSOF launch: the caller's count, else the override, else
 // the plan's.
@@ -818,7 +822,8 @@ int run_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* ws, cu
     CKM(cudaMemsetAsync(bs, 0, sizeof(int) * ly.bsync_ints, st));
     if (g_timer.on) CKM(g_timer.mark(st));
     CK(launch_bsoi_persistent(dA, ldd, C[0], C[1], ldd, G, n, L, bs, bs + ly.bsync_ints - 2,
-                              at<int>(ws, ly.info) + 2, plan.bsoi == 5, st));
+                              at<int>(ws, ly.info) + 2, plan.bsoi == 5, st, 0, -1,
+                              g_wait_test ? bs + ly.bsync_ints - 1 : nullptr));
     if (g_timer.on) CKM(g_timer.mark(st));
   } else {
     // One launch per step (small problems: more, smaller tiles per step).
@@ -837,6 +842,27 @@ extern "C" {
 size_t bsofi_dev_ws_bytes(int n, int L, int ldd) { return layout(n, L, ldd).total; }
 
 int bsofi_dev_prepare(void) { return (int)gemm_init_attributes(); }
+
+int bsofi_dev_preload(void) {
+  size_t local = 0;
+  cudaError_t e;
+  if ((e = gemm_init_attributes()) != cudaSuccess) return (int)e;
+  if ((e = preload_bsof(&local)) != cudaSuccess) return (int)e;
+  if ((e = preload_bsoi(&local)) != cudaSuccess) return (int)e;
+  if ((e = preload_bstri(&local)) != cudaSuccess) return (int)e;
+  if ((e = preload_gemm(&local)) != cudaSuccess) return (int)e;
+  if ((e = preload_panel(&local)) != cudaSuccess) return (int)e;
+  if ((e = preload_tri(&local)) != cudaSuccess) return (int)e;
+  if ((e = preload_one(build_leaf_t_kernel, &local)) != cudaSuccess) return (int)e;
+  // The context's local-memory reservation grows at the launch of a kernel
+  // that needs more than it holds; growing it here keeps later launches from
+  // allocating.
+  size_t stack = 0;
+  if ((e = cudaDeviceGetLimit(&stack, cudaLimitStackSize)) != cudaSuccess) return (int)e;
+  if (local > stack && (e = cudaDeviceSetLimit(cudaLimitStackSize, local)) != cudaSuccess)
+    return (int)e;
+  return 0;
+}
 
 int bsofi_dev_zero_structural(int n, int L, double* dA, int ldd, void* stream) {
   g_launches = 0;
@@ -938,6 +964,8 @@ int bsofi_dev_bsof_timeline(int n, int L, int ldd, void* dws, unsigned long long
 }
 
 void bsofi_dev_set_bsof_workers(int w) { g_workers_override = w > 0 ? w : 0; }
+
+void bsofi_dev_set_wait_test(int on) { g_wait_test = on != 0; }
 
 void bsofi_dev_set_bstri_overlap(int on) { g_overlap_enabled.store(on ? 1 : 0); }
 

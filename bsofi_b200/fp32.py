@@ -39,6 +39,9 @@ _SIGS = {
     "hybridXbsofiLWork": (_i, [_i] * 4),
     "hybridXbsoftri": (_i, [_i, _i, _i, _fp, _i, _fp, _fp, _i, _fp, _i, _ip]),
     "hybridXbsoi": (_i, [_i, _i, _i, _fp, _i, _fp, _fp, _i, _fp, _i, _ip]),
+    "hybridxbsofilwork_": (_i, [_ip] * 4),
+    "hybridxbsoftri_": (_i, [_ip, _ip, _fp, _ip, _fp, _fp, _ip, _fp, _ip, _ip]),
+    "hybridxbsoi_": (_i, [_ip, _ip, _fp, _ip, _fp, _fp, _ip, _fp, _ip, _ip]),
     "lapackxbsofilwork_": (_i, [_ip] * 3),
     "lapackxbsof_": (_i, [_ip, _ip, _fp, _ip, _fp, _fp, _ip, _ip]),
     "lapackxbstri_": (_i, [_ip, _ip, _fp, _ip, _ip]),

@@ -1,10 +1,11 @@
-"""Multi-GPU execution of BSOF/I: replicas only.
+"""Multi-GPU execution of independent BSOF/I inversions: replicas.
 
 Independent inversions (Monte Carlo walkers, serving requests) shard by
 instance across ranks, one process per GPU, with no collective on the data
 path; the only collectives are a barrier around timed regions and a MAX
 reduction of the elapsed device time, so throughput is "all instances /
-slowest rank".  A single inversion is not split across GPUs.
+slowest rank".  (Splitting one inversion across the GPUs of a group is a
+separate path, bsofi_b200.shard.)
 """
 import os
 

@@ -118,6 +118,15 @@ int hybridXbsoftri(int handle, int n, int L, double A[], int lda, double tau[], 
                    int lwork, double dwork[], int ldwork, int *info);
 int hybridXbsoi(int handle, int n, int L, double A[], int lda, double tau[], double work[],
                 int lwork, double dwork[], int ldwork, int *info);
+/* Fortran twins of the three names above: cb_hybridXbsofiLWork,
+ * cb_hybridXbsoftri, cb_hybridXbsoi, src/bsofi_callback.c:62-87
+ * (include/bsofi_hybrid.h:57-69).  Every argument by pointer, no cuBLAS
+ * handle; a NULL argument gives info = -(its position). */
+int hybridxbsofilwork_(int *n, int *L, int *lda, int *lworkHostDevice);
+int hybridxbsoftri_(int *n, int *L, double A[], int *lda, double tau[], double work[], int *lwork,
+                    double dwork[], int *ldwork, int *info);
+int hybridxbsoi_(int *n, int *L, double A[], int *lda, double tau[], double work[], int *lwork,
+                 double dwork[], int *ldwork, int *info);
 
 /* Device-pointer API, include/bsofi_gpu.h:34-62 (src/bsofi_gpu.c:74-414).
  * dA is device memory (ldda >= n*L), tau is HOST memory as in the reference
@@ -293,20 +302,39 @@ void bsofi_server_destroy(bsofi_server *server);
  * pool already holds nearly all of HBM (cudaMalloc would fail), or one that
  * cannot let cudaMalloc/cudaFree synchronize the device mid-sweep.  Same
  * kernels and result as bsofi_device_invert, but the workspace is a static
- * device array of bsofi_noalloc_scratch_bytes() (32 MiB) that every GPU
- * loading this library keeps until exit; the call makes no cudaMalloc,
- * cudaFree or other allocating call.  Problems whose workspace
- * (bsofi_device_workspace_bytes) exceeds it are rejected with
- * BSOFI_NOALLOC_TOO_LARGE (for example n=64 up to L=64, n=128 up to L=16).
- * The first call on a device looks up the array's device address (with that
- * device current) and should come before any stream capture.  All calls share
- * the array: calls that overlap on the GPU race.  dinfo (device int, may be
- * NULL) receives the info word as bsofi_device_info describes it (values
- * >= 0x7f7f7f7f mean 0).
- * Returns 0, -1 for an illegal argument, BSOFI_NOALLOC_TOO_LARGE, or
- * BSOFI_INFO_CUDA - cudaError_t. */
+ * device array of bsofi_noalloc_scratch_bytes() (32 MiB) instead of a caller
+ * buffer, and the call makes no cudaMalloc, cudaFree or other allocating call.
+ *
+ * bsofi_noalloc_prepare: call it once per device, with that device current,
+ * before the caller's pool reserves HBM and before any stream capture.  Under
+ * lazy module loading (the CUDA 12 default) the driver reserves the static
+ * array, loads kernel code and grows the local-memory reservation the first
+ * time each is used; prepare does all of it now (it looks up the array's
+ * device address and loads every kernel of the pipeline).  Without it the
+ * first inversion on a device does that work and can fail for lack of memory
+ * (BSOFI_INFO_CUDA - cudaErrorMemoryAllocation).  From then on the device holds
+ * the array until the process exits.  Returns 0 or BSOFI_INFO_CUDA -
+ * cudaError_t.
+ *
+ * Size limit: the workspace grows with n, L and ldda; problems with
+ * bsofi_device_workspace_bytes(n, L, ldda) > bsofi_noalloc_scratch_bytes()
+ * are rejected with BSOFI_NOALLOC_TOO_LARGE before any device work.  With
+ * ldda = n*L that allows L up to 120 at n = 64, 50 at n = 100, 31 at n = 128,
+ * 14 at n = 196 and 8 at n = 256; compare the two functions for other sizes.
+ *
+ * All calls share the array and it keeps the last call's contents (the
+ * pipeline writes every region before reading it): calls that overlap on the
+ * GPU (other streams or threads on the same device) race.  dinfo (device int)
+ * receives the info word as bsofi_device_info describes it (values >=
+ * 0x7f7f7f7f mean 0), enqueued on `stream`, and the call returns without
+ * waiting.  With dinfo = NULL the call waits for `stream` and returns the info
+ * word itself: 0, i > 0 for an exactly zero R(i,i), or BSOFI_INFO_CUDA -
+ * cudaErrorLaunchTimeout when a bounded wait inside a kernel gave up.
+ * Returns 0 (or that info word), -1 for an illegal argument,
+ * BSOFI_NOALLOC_TOO_LARGE, or BSOFI_INFO_CUDA - cudaError_t. */
 #define BSOFI_NOALLOC_TOO_LARGE (-2000)
 unsigned long long bsofi_noalloc_scratch_bytes(void);
+int bsofi_noalloc_prepare(void);
 int bsofi_device_invert_noalloc(int n, int L, double *dA, int ldda, double *dtau, int *dinfo,
                                 void *stream);
 
@@ -334,6 +362,14 @@ void bsofi_device_set_bsof_workers(int workers);
  * results are the same as without the split).  on = 0 turns this off for the
  * process, 1 (the default) on. */
 void bsofi_device_set_bstri_overlap(int on);
+/* Diagnostics (no reference counterpart): with on = 1, the persistent BSOI
+ * launches made by this thread wait, in every step after the first, on a
+ * zeroed workspace word that nothing writes, under a short poll limit (about
+ * a millisecond).  The waits give up, the kernel returns, and the inversion's
+ * info word reads BSOFI_INFO_CUDA - cudaErrorLaunchTimeout, exactly as when a
+ * real wait runs out; the device and the workspace stay usable.  Lets a test
+ * check that path without any fault.  on = 0 (the default) turns it off. */
+void bsofi_device_set_wait_test(int on);
 
 /* Diagnostic entry point (no reference counterpart): one call of the FP64
  * DMMA tile engine, C = alpha*A*B + beta*C on device memory (column-major),

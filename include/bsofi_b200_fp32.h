@@ -80,6 +80,15 @@ int hybridXbsoftri(int handle, int n, int L, float A[], int lda, float tau[], fl
                    int lwork, float dwork[], int ldwork, int *info);
 int hybridXbsoi(int handle, int n, int L, float A[], int lda, float tau[], float work[],
                 int lwork, float dwork[], int ldwork, int *info);
+/* Fortran twins of the three names above: cb_hybridXbsofiLWork,
+ * cb_hybridXbsoftri, cb_hybridXbsoi, src/bsofi_callback.c:62-87
+ * (include/bsofi_hybrid.h:57-69).  Every argument by pointer, no cuBLAS
+ * handle; a NULL argument gives info = -(its position). */
+int hybridxbsofilwork_(int *n, int *L, int *lda, int *lworkHostDevice);
+int hybridxbsoftri_(int *n, int *L, float A[], int *lda, float tau[], float work[], int *lwork,
+                    float dwork[], int *ldwork, int *info);
+int hybridxbsoi_(int *n, int *L, float A[], int *lda, float tau[], float work[], int *lwork,
+                 float dwork[], int *ldwork, int *info);
 
 /* Device-pointer names, include/bsofi_gpu.h:34-62 (src/bsofi_gpu.c:74-414):
  * dA is device memory (float, ldda >= n*L), tau HOST memory.  Synchronous. */

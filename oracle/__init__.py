@@ -32,11 +32,22 @@ _ip = ctypes.POINTER(ctypes.c_int)
 _libs = {}
 
 
+def reference_tree():
+    """The reference source tree: $BSOFI_REFERENCE, else the read-only mount
+    /root/reference of the build container; None where neither exists (the
+    GPU box uses the prebuilt _ref/ libraries)."""
+    for d in (os.environ.get("BSOFI_REFERENCE"), "/root/reference"):
+        if d and os.path.exists(os.path.join(d, "src", "bsofi_cpu.c")):
+            return d
+    return None
+
+
 def build():
     """Compile the checkers (make -C oracle).  The reference library is only
     rebuilt where the reference tree is present."""
     import subprocess
-    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    ref = reference_tree()
+    subprocess.run(["make", "-s", "-C", _HERE] + (["REF=" + ref] if ref else []), check=True)
 
 
 def ref_available():
@@ -84,11 +95,20 @@ def _check(A, n, L):
     return A
 
 
+def _inplace(A, n, L):
+    N = n * L
+    if A.shape != (N, N) or A.dtype != np.float64 or not A.flags.f_contiguous:
+        raise ValueError("A must be a Fortran-ordered float64 %dx%d array" % (N, N))
+    return A
+
+
 # ---------------------------------------------------------------- reference
-def ref_bsoftri(A, n, L):
-    """hybridxbsoftrih_ on a copy of A.  Returns (A_out, tau, info)."""
+def ref_bsoftri(A, n, L, inplace=False):
+    """hybridxbsoftrih_ on a copy of A (on A itself with inplace=True: A must
+    then be a Fortran-ordered float64 N x N array, as the reference's callers
+    pass it).  Returns (A_out, tau, info)."""
     lib = _lib("ref")
-    A = _check(A, n, L)
+    A = _inplace(A, n, L) if inplace else _check(A, n, L)
     N = n * L
     h = np.zeros(10, dtype=np.int32)
     hp = h.ctypes.data_as(_ip)
@@ -103,12 +123,16 @@ def ref_bsoftri(A, n, L):
     return A, tau, info.value
 
 
-def ref_bsoi(A, tau, n, L):
-    """hybridxbsoih_ on a copy of the BSOFTRI state.  Returns (A_out, info)."""
+def ref_bsoi(A, tau, n, L, inplace=False):
+    """hybridxbsoih_ on a copy of the BSOFTRI state (on A and tau themselves
+    with inplace=True).  Returns (A_out, info)."""
     lib = _lib("ref")
-    A = _check(A, n, L)
+    A = _inplace(A, n, L) if inplace else _check(A, n, L)
     N = n * L
-    tau = np.ascontiguousarray(tau, dtype=np.float64).copy()
+    if not inplace:
+        tau = np.ascontiguousarray(tau, dtype=np.float64).copy()
+    elif not (tau.dtype == np.float64 and tau.flags.c_contiguous):
+        raise ValueError("tau must be a contiguous float64 array")
     h = np.zeros(10, dtype=np.int32)
     hp = h.ctypes.data_as(_ip)
     lib.hybridxinith_(hp, _i(n), _i(L), _i(N))

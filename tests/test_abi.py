@@ -110,3 +110,55 @@ def test_device_api_rejects_bad_arguments():
         assert lib.bsofi_device_invert(n, L, p, ld, fake, fake, None) == -1
         assert lib.bsofi_device_bsoftri(n, L, p, ld, fake, fake, None) == -1
         assert lib.bsofi_device_bsoi(n, L, p, ld, fake, fake, None) == -1
+
+
+def test_device_lwork_query_at_largest_serving_size():
+    """n = 576, L = 80 (N = 46080): the device length is past INT_MAX doubles.
+    The int-returning query saturates; the lwork = -2 queries that write
+    work[0] (a double) give the exact length."""
+    lib = _lib.load()
+    n, L = 576, 80
+    N = n * L
+    exact = ((N + 31) // 32 * 32) * N + N + lib.bsofi_device_workspace_bytes(n, L, N) // 8
+    assert exact > 2**31 - 1
+    assert lib.hybridXbsofiLWork(n, L, N, -2) == 2**31 - 1
+    n_, L_, N_, m2 = ctypes.c_int(n), ctypes.c_int(L), ctypes.c_int(N), ctypes.c_int(-2)
+    assert lib.hybridxbsofilwork_(ctypes.byref(n_), ctypes.byref(L_), ctypes.byref(N_),
+                                  ctypes.byref(m2)) == 2**31 - 1
+    w = np.zeros(1)
+    info = ctypes.c_int(7)
+    A = np.zeros(1)
+    tau = np.zeros(1)
+    lib.hybridXbsoftri(0, n, L, A.ctypes.data_as(_dp), N, tau.ctypes.data_as(_dp),
+                       w.ctypes.data_as(_dp), -2, None, 0, ctypes.byref(info))
+    assert info.value == 0 and w[0] == float(exact)
+
+
+def test_hybrid_fortran_twins_validate_and_query():
+    """hybridxbsofilwork_ / hybridxbsoftri_ / hybridxbsoi_ (the reference's
+    cb_hybridX* callbacks, src/bsofi_callback.c:62-87) take every argument by
+    pointer and answer the lwork queries without a GPU."""
+    lib = _lib.load()
+    A = np.zeros((8, 8), order="F")
+    tau = np.zeros(8)
+    w = np.zeros(1)
+    info = ctypes.c_int(5)
+    n, L, lda, ldw = ctypes.c_int(4), ctypes.c_int(2), ctypes.c_int(8), ctypes.c_int(0)
+    for f in (lib.hybridxbsoftri_, lib.hybridxbsoi_):
+        lw = ctypes.c_int(-1)
+        f(ctypes.byref(n), ctypes.byref(L), A.ctypes.data_as(_dp), ctypes.byref(lda),
+          tau.ctypes.data_as(_dp), w.ctypes.data_as(_dp), ctypes.byref(lw), None,
+          ctypes.byref(ldw), ctypes.byref(info))
+        assert info.value == 0 and w[0] >= 1
+        bad = ctypes.c_int(7)  # lda < N
+        f(ctypes.byref(n), ctypes.byref(L), A.ctypes.data_as(_dp), ctypes.byref(ctypes.c_int(7)),
+          tau.ctypes.data_as(_dp), w.ctypes.data_as(_dp), ctypes.byref(lw), None,
+          ctypes.byref(ldw), ctypes.byref(info))
+        assert info.value == -4
+        f(None, ctypes.byref(L), A.ctypes.data_as(_dp), ctypes.byref(lda),
+          tau.ctypes.data_as(_dp), w.ctypes.data_as(_dp), ctypes.byref(lw), None,
+          ctypes.byref(ldw), ctypes.byref(info))
+        assert info.value == -1
+    m1 = ctypes.c_int(-1)
+    assert lib.hybridxbsofilwork_(ctypes.byref(n), ctypes.byref(L), ctypes.byref(lda),
+                                  ctypes.byref(m1)) == lib.hybridXbsofiLWork(4, 2, 8, -1)

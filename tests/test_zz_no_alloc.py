@@ -2,10 +2,14 @@
 
 It exists for callers that cannot allocate device memory while they invert
 (a memory pool that already holds nearly all of HBM, or a sweep that must not
-be synchronized by cudaMalloc/cudaFree).  This test calls it through the C ABI
-twice in a row on the same device and checks each result against the
-allocating entry point bsofi_device_invert, within the parity tolerance of the
-other GPU tests.  It lives in its own file, collected last.
+be synchronized by cudaMalloc/cudaFree).  These tests call it through the C
+ABI: after bsofi_noalloc_prepare, a call leaves the device's free memory and
+torch's reserved memory exactly as they were; two calls in a row on the same
+device each match the allocating entry point bsofi_device_invert within the
+parity tolerance of the other GPU tests; with no device info word the call
+returns the info word itself.  The file is collected last, and the first test
+is meaningful in a fresh process too (it runs prepare before anything else
+launches a kernel of the library).
 """
 import ctypes
 
@@ -28,6 +32,34 @@ def _run_allocating(torch, M, n, L, ldd, dev):
     assert api.device_invert(n, L, dA.data_ptr(), ldd, dtau.data_ptr(), ws.data_ptr(), 0) == 0
     torch.cuda.synchronize()
     return from_device_colmajor(dA, N), dtau.cpu().numpy()
+
+
+def test_noalloc_after_prepare_allocates_nothing(cuda_device):
+    import torch
+    from gpu_util import from_device_colmajor, to_device_colmajor
+    lib = _lib.load()
+    n, L, ldd = 64, 16, 1024
+    M = hubbard_matrix(8, L, 4.0, seed=43)
+    # Every buffer the call touches exists before the measurement.
+    dA = to_device_colmajor(torch, M, ld=ldd, device=cuda_device)
+    dtau = torch.zeros(n * L, dtype=torch.float64, device=cuda_device)
+    dinfo = torch.full((1,), -5, dtype=torch.int32, device=cuda_device)
+    torch.cuda.synchronize()
+    assert lib.bsofi_noalloc_prepare() == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(cuda_device)
+    reserved0 = torch.cuda.memory_reserved(cuda_device)
+    rc = lib.bsofi_device_invert_noalloc(n, L, dA.data_ptr(), ldd, dtau.data_ptr(),
+                                         dinfo.data_ptr(), None)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(cuda_device)
+    assert rc == 0
+    assert free1 == free0, "device free memory moved by %d bytes" % (free1 - free0)
+    assert torch.cuda.memory_reserved(cuda_device) == reserved0
+    assert int(dinfo.item()) >= 0x7f7f7f7f
+    X = from_device_colmajor(dA, n * L)
+    Xref, _ = _run_allocating(torch, M, n, L, ldd, cuda_device)
+    assert rel_fro(X, Xref) < inverse_tolerance(M, Xref)
 
 
 def test_noalloc_matches_allocating_entry_point(cuda_device):
@@ -54,6 +86,28 @@ def test_noalloc_matches_allocating_entry_point(cuda_device):
             X = from_device_colmajor(dA, N)
             assert rel_fro(X, Xref) < tol
             np.testing.assert_allclose(dtau.cpu().numpy(), tauref, rtol=0, atol=1e-12)
+
+
+def test_noalloc_without_info_word_returns_info(cuda_device):
+    import torch
+    from gpu_util import from_device_colmajor, to_device_colmajor
+    lib = _lib.load()
+    n, L = 24, 7
+    M = random_pcyclic(n, L, seed=44)
+    Xref, _ = _run_allocating(torch, M, n, L, n * L, cuda_device)
+    dA = to_device_colmajor(torch, M, ld=n * L, device=cuda_device)
+    dtau = torch.zeros(n * L, dtype=torch.float64, device=cuda_device)
+    # dinfo = NULL: the call waits for its stream and returns the info word.
+    assert lib.bsofi_device_invert_noalloc(n, L, dA.data_ptr(), n * L, dtau.data_ptr(),
+                                           None, None) == 0
+    assert rel_fro(from_device_colmajor(dA, n * L), Xref) < inverse_tolerance(M, Xref)
+    # An exactly zero diagonal of R: block 0 of the input all zero makes R(1,1) = 0.
+    Z = M.copy()
+    Z[:, 0] = 0.0
+    dA = to_device_colmajor(torch, Z, ld=n * L, device=cuda_device)
+    info = lib.bsofi_device_invert_noalloc(n, L, dA.data_ptr(), n * L, dtau.data_ptr(), None,
+                                           None)
+    assert info == 1
 
 
 def test_noalloc_rejects_oversized_problem(cuda_device):
