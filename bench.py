@@ -61,6 +61,8 @@ def parse():
     p.add_argument("--batch-mixed", type=int, default=64,
                    help="instances in the mixed-size batched sample (0 = skip)")
     p.add_argument("--batch-steps", type=int, default=3)
+    p.add_argument("--mixed-steps", type=int, default=10,
+                   help="timed mixed-precision inversions at the headline size (0 = skip)")
     p.add_argument("--c4-steps", type=int, default=4,
                    help="timed inversions at n=400, p=64, U=6 for the c4 key (0 = skip)")
     p.add_argument("--serve", type=int, default=60,
@@ -378,6 +380,19 @@ def main():
         batched = run_batched(api, torch, dev, specs, args.batch_steps, stream)
         batched["workload"] = ("%d independent FP64 inversions per step, %dx%d lattice, n=%d, "
                                "p=%d (one walker each)" % (args.batch, side, side, n, L))
+    mixed = None
+    if args.mixed_steps > 0:
+        mixed = run_mixed_single(api, torch, dev, stream, side, L, U, args.mixed_steps,
+                                 max(args.warmup, 3), rank, value)
+    batched_mp = None
+    if args.batch > 0 and args.mixed_steps > 0:
+        specs = [(side, L, U, 5000 + 100 * rank + i) for i in range(args.batch)]
+        batched_mp = run_batched(api, torch, dev, specs, args.batch_steps, stream, precision=1)
+        batched_mp["workload"] = ("%d independent inversions per step, %dx%d lattice, n=%d, p=%d;"
+                                  " FP64 factorization, BSOI on the int8 tensor cores (Ozaki "
+                                  "scheme, 8 slices)" % (args.batch, side, side, n, L))
+        if batched and batched.get("value"):
+            batched_mp["ratio_to_fp64_batched"] = batched_mp["value"] / batched["value"]
     batched_mixed = None
     if args.batch_mixed > 0:
         rng = np.random.default_rng(77 + rank)
@@ -424,6 +439,7 @@ def main():
                 "cpu_baseline": cpu, "e2e": e2e, "e2e_pageable": e2e_pageable,
                 "e2e_fp32": e2e_fp32,
                 "batched": batched, "batched_mixed_sizes": batched_mixed, "served": served,
+                "mixed": mixed, "batched_mixed_precision": batched_mp,
                 "gpu_launches": launches_per_step * args.steps,
                 "clocks": clk}
         print(json.dumps(line))
@@ -480,11 +496,75 @@ def run_c4(api, torch, dev, stream, steps, warmup, peak, rank):
             "residual": resid, "plan": plan}
 
 
-def run_batched(api, torch, dev, specs, steps, stream):
-    """Time bsofi_device_invert_batched over `steps` batches.  Every batch
-    starts from fresh inputs copied from pristine device buffers outside the
-    timed window; the reported rate is instances / summed batch time, max
-    over ranks."""
+def run_mixed_single(api, torch, dev, stream, side, L, U, steps, warmup, rank, fp64_value):
+    """Single inversions of the headline size with BSOI on the int8 tensor
+    cores (bsofi_device_invert_mixed, 8 slices), device-resident, CUDA-event
+    timed on the launching stream, a fresh input copy per step made outside
+    the timed window; residual and relative error against the FP64 path on
+    the same matrix."""
+    from bsofi_b200 import replicas
+    n = side * side
+    N = n * L
+    ldd = (N + 31) // 32 * 32
+    blocks = hubbard_pcyclic(side, L, U, 8000 + rank)
+    pristine = pcyclic_device(torch, *blocks, ldd, dev)
+    work = torch.empty_like(pristine)
+    dtau = torch.zeros(N, dtype=torch.float64, device=dev)
+    ws = torch.zeros(api.mixed_workspace_bytes(n, L, ldd) // 8 + 1, dtype=torch.float64,
+                     device=dev)
+    sp = stream.cuda_stream
+    total = 0.0
+    api.timing(True)
+    for it in range(warmup + steps):
+        work.copy_(pristine)
+        torch.cuda.synchronize()
+        if it == warmup:
+            api.timing(True)  # BSOI product launches of the timed steps only
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            rc = api.device_invert_mixed(n, L, work.data_ptr(), ldd, dtau.data_ptr(),
+                                         ws.data_ptr(), 0, sp)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        if rc != 0:
+            raise RuntimeError("bsofi_device_invert_mixed failed: %d" % rc)
+        if it >= warmup:
+            total += e0.elapsed_time(e1)
+    bsoi_ms, bsoi_launches = api.timing_read()
+    api.timing(False)
+    ms = replicas.max_over_ranks(total, dev) / steps
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from gpu_util import block_residual_colmajor
+    resid = block_residual_colmajor(torch, *blocks, work, N)
+    ref = pristine.clone()
+    ws64 = torch.zeros(api.workspace_bytes(n, L, ldd) // 8 + 1, dtype=torch.float64, device=dev)
+    if api.device_invert(n, L, ref.data_ptr(), ldd, dtau.data_ptr(), ws64.data_ptr(), 0) != 0:
+        raise RuntimeError("bsofi_device_invert failed")
+    torch.cuda.synchronize()
+    relerr = float(torch.linalg.norm(work[:, :N] - ref[:, :N]) / torch.linalg.norm(ref[:, :N]))
+    del pristine, work, ws, ws64, ref
+    torch.cuda.empty_cache()
+    value = 1e3 / ms
+    return {"workload": "single inversion, %dx%d lattice, n=%d, p=%d, U=%g: FP64 BSOF/BSTRI, "
+                        "BSOI products on the int8 tensor cores (Ozaki scheme, 8 slices)"
+                        % (side, side, n, L, U),
+            "value": value, "unit": "inversions/s", "ms_per_inversion": ms, "steps": steps,
+            "ratio_to_fp64_single": value / fp64_value if fp64_value else None,
+            "residual": resid, "relative_error_vs_fp64": relerr,
+            "bsoi_ms_per_inversion": bsoi_ms / steps,
+            "bsoi_effective_fp64_tflops": flops_bsoi(n, L) / (bsoi_ms / steps * 1e-3) / 1e12
+            if bsoi_ms > 0 else None,
+            "bsoi_timed_launches": bsoi_launches}
+
+
+def run_batched(api, torch, dev, specs, steps, stream, precision=0):
+    """Time bsofi_device_invert_batched_ex over `steps` batches (precision 0
+    FP64, 1 mixed: BSOI on the int8 tensor cores).  Every batch starts from
+    fresh inputs copied from pristine device buffers outside the timed
+    window; the reported rate is instances / summed batch time, max over
+    ranks."""
     from bsofi_b200 import replicas
     ns, Ls, lds, pristine = [], [], [], []
     flops = 0.0
@@ -499,8 +579,8 @@ def run_batched(api, torch, dev, specs, steps, stream):
         flops += bsofi_flops(n, L)
     work = [torch.empty_like(t) for t in pristine]
     taus = [torch.zeros(n * L, dtype=torch.float64, device=dev) for n, L in zip(ns, Ls)]
-    ws = torch.zeros(api.batch_workspace_bytes(ns, Ls, lds) // 8 + 1, dtype=torch.float64,
-                     device=dev)
+    ws = torch.zeros(api.batch_workspace_bytes(ns, Ls, lds, precision) // 8 + 1,
+                     dtype=torch.float64, device=dev)
     sp = stream.cuda_stream
     total_ms = 0.0
     for it in range(steps + 1):  # the first batch is a warm-up
@@ -513,7 +593,8 @@ def run_batched(api, torch, dev, specs, steps, stream):
         with torch.cuda.stream(stream):
             e0.record(stream)
             rc = api.device_invert_batched(ns, Ls, [w.data_ptr() for w in work], lds,
-                                           [t.data_ptr() for t in taus], ws.data_ptr(), 8, sp)
+                                           [t.data_ptr() for t in taus], ws.data_ptr(), 8, sp,
+                                           precision)
             e1.record(stream)
         torch.cuda.synchronize()
         if rc != 0:
@@ -529,6 +610,30 @@ def run_batched(api, torch, dev, specs, steps, stream):
     ms_max = replicas.max_over_ranks(total_ms, dev)
     rate = world * len(specs) * steps / (ms_max * 1e-3)
     launches = api.last_launches()
+    if precision == 1:
+        # Against the FP64 inverse of the same first instance.
+        ref = pristine[0].clone()
+        dtau0 = torch.zeros(ns[0] * Ls[0], dtype=torch.float64, device=dev)
+        ws0 = torch.zeros(api.workspace_bytes(ns[0], Ls[0], lds[0]) // 8 + 1,
+                          dtype=torch.float64, device=dev)
+        if api.device_invert(ns[0], Ls[0], ref.data_ptr(), lds[0], dtau0.data_ptr(),
+                             ws0.data_ptr(), 0) != 0:
+            raise RuntimeError("bsofi_device_invert failed")
+        torch.cuda.synchronize()
+        N0 = ns[0] * Ls[0]
+        relerr = float(torch.linalg.norm(work[0][:, :N0] - ref[:, :N0]) /
+                       torch.linalg.norm(ref[:, :N0]))
+        del ref, ws0
+        out = {"value": rate, "unit": "inversions/s", "steps": steps,
+               "ms_per_step": ms_max / steps,
+               "tflops": flops * steps * world / (ms_max * 1e-3) / 1e12,
+               "instances_per_step": len(specs), "residual_first_instance": resid,
+               "relative_error_vs_fp64_first_instance": relerr,
+               "gpu_launches_per_step": launches,
+               "slices": 8}
+        del work, pristine, ws
+        torch.cuda.empty_cache()
+        return out
     # The same batch captured once into a CUDA graph and replayed.
     graph_ms = 0.0
     g = api.BatchGraph(ns, Ls, [w.data_ptr() for w in work], lds, [t.data_ptr() for t in taus],

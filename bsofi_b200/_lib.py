@@ -77,8 +77,19 @@ _SIGS = {
     "bsofi_device_bsoi_rows": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp,
                                               _vp, ctypes.c_int, ctypes.c_int, _vp]),
     "bsofi_device_info": (_vp, [_vp]),
+    "bsofi_device_workspace_bytes_mixed": (ctypes.c_ulonglong, [ctypes.c_int] * 4),
+    "bsofi_device_invert_mixed": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int,
+                                                 _vp, _vp, ctypes.c_int, _vp]),
+    "bsofi_selftest_ozaki_scratch_bytes": (ctypes.c_ulonglong, [ctypes.c_int] * 4),
+    "bsofi_selftest_ozaki": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
+                                            ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int,
+                                            ctypes.c_int, _vp, _vp, _vp]),
     "bsofi_device_last_launches": (ctypes.c_longlong, []),
     "bsofi_batch_workspace_bytes": (ctypes.c_ulonglong, [ctypes.c_int, _vp, _vp, _vp]),
+    "bsofi_batch_workspace_bytes_ex": (ctypes.c_ulonglong, [ctypes.c_int, _vp, _vp, _vp,
+                                                            ctypes.c_int]),
+    "bsofi_device_invert_batched_ex": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp,
+                                                      ctypes.c_int, ctypes.c_int, _vp]),
     "bsofi_device_invert_batched": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp,
                                                    ctypes.c_int, _vp]),
     "bsofi_batch_graph_create": (_vp, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int]),
@@ -92,6 +103,11 @@ _SIGS = {
     "bsofi_server_request_bytes": (ctypes.c_ulonglong, [ctypes.c_int] * 3),
     "bsofi_server_submit": (ctypes.c_longlong, [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int,
                                                 _vp, ctypes.c_int]),
+    "bsofi_server_footprint_bytes": (ctypes.c_ulonglong, [ctypes.c_int] * 3),
+    "bsofi_server_submit_blocks": (ctypes.c_longlong, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp,
+                                                       ctypes.c_int]),
+    "bsofi_server_result": (ctypes.c_int, [_vp, ctypes.c_longlong, _vp, _c_int_p, _vp]),
+    "bsofi_server_release": (ctypes.c_int, [_vp, ctypes.c_longlong]),
     "bsofi_server_poll": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int]),
     "bsofi_server_pending": (ctypes.c_int, [_vp]),
     "bsofi_server_destroy": (None, [_vp]),

@@ -169,26 +169,37 @@ def timing_read():
     return ms.value, cnt.value
 
 
-def batch_workspace_bytes(ns, Ls, lddas):
+def batch_workspace_bytes(ns, Ls, lddas, precision=0):
+    """Device workspace of a batch: precision 0 FP64, 1 mixed (int8 BSOI)."""
     import numpy as _np
     n = _np.ascontiguousarray(ns, dtype=_np.int32)
     L = _np.ascontiguousarray(Ls, dtype=_np.int32)
     ld = _np.ascontiguousarray(lddas, dtype=_np.int32)
-    return int(load().bsofi_batch_workspace_bytes(len(n), n.ctypes.data, L.ctypes.data,
-                                                  ld.ctypes.data))
+    return int(load().bsofi_batch_workspace_bytes_ex(len(n), n.ctypes.data, L.ctypes.data,
+                                                     ld.ctypes.data, precision))
 
 
-def device_invert_batched(ns, Ls, dAs, lddas, dtaus, dwork, streams=8, stream=0):
-    """bsofi_device_invert_batched on raw device pointers; asynchronous."""
+def device_invert_batched(ns, Ls, dAs, lddas, dtaus, dwork, streams=8, stream=0, precision=0):
+    """bsofi_device_invert_batched_ex on raw device pointers; asynchronous."""
     import numpy as _np
     n = _np.ascontiguousarray(ns, dtype=_np.int32)
     L = _np.ascontiguousarray(Ls, dtype=_np.int32)
     ld = _np.ascontiguousarray(lddas, dtype=_np.int32)
     pa = _np.ascontiguousarray(dAs, dtype=_np.uint64)
     pt = _np.ascontiguousarray(dtaus, dtype=_np.uint64)
-    return load().bsofi_device_invert_batched(len(n), n.ctypes.data, L.ctypes.data, pa.ctypes.data,
-                                              ld.ctypes.data, pt.ctypes.data, dwork, streams,
-                                              stream)
+    return load().bsofi_device_invert_batched_ex(len(n), n.ctypes.data, L.ctypes.data,
+                                                 pa.ctypes.data, ld.ctypes.data, pt.ctypes.data,
+                                                 dwork, streams, precision, stream)
+
+
+def mixed_workspace_bytes(n, L, ldda, slices=0):
+    return int(load().bsofi_device_workspace_bytes_mixed(n, L, ldda, slices))
+
+
+def device_invert_mixed(n, L, dA, ldda, dtau, dwork, slices=0, stream=0):
+    """bsofi_device_invert_mixed: FP64 factorization, BSOI on the int8 tensor
+    cores (Ozaki scheme); asynchronous."""
+    return load().bsofi_device_invert_mixed(n, L, dA, ldda, dtau, dwork, slices, stream)
 
 
 def autotune(n, L, reps=3, stream=0):
@@ -268,6 +279,29 @@ class Server:
             raise RuntimeError("bsofi_server_submit failed: %d" % rid)
         return rid
 
+    def submit_blocks(self, n, L, dS, dD=0, precision=0):
+        """Server-owned request from packed device blocks (dS: L coupling
+        blocks, dD: L diagonal blocks or 0 for identity); the matrix, tau and
+        workspace come from the pool at admission."""
+        rid = load().bsofi_server_submit_blocks(self.ptr, n, L, dD or None, dS, precision)
+        if rid < 0:
+            raise RuntimeError("bsofi_server_submit_blocks failed: %d" % rid)
+        return rid
+
+    def result(self, rid):
+        """(device address of M^{-1}, its leading dimension, address of tau)
+        of a finished server-owned request, or None."""
+        dA = ctypes.c_void_p(0)
+        dtau = ctypes.c_void_p(0)
+        ld = ctypes.c_int(0)
+        if load().bsofi_server_result(self.ptr, rid, ctypes.byref(dA), ctypes.byref(ld),
+                                      ctypes.byref(dtau)) != 0:
+            return None
+        return dA.value, ld.value, dtau.value
+
+    def release(self, rid):
+        return int(load().bsofi_server_release(self.ptr, rid))
+
     def poll(self):
         """List of (request id, status) that finished since the last poll."""
         k = load().bsofi_server_poll(self.ptr, self._ids.ctypes.data, self._st.ctypes.data,
@@ -293,3 +327,7 @@ class Server:
 
 def server_request_bytes(n, L, ldda):
     return int(load().bsofi_server_request_bytes(n, L, ldda))
+
+
+def server_footprint_bytes(n, L, precision=0):
+    return int(load().bsofi_server_footprint_bytes(n, L, precision))

@@ -19,7 +19,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libbsofi_b200.so")
 ROOT = os.path.dirname(HERE)
 
-CU_SOURCES = ["kernels_bsof.cu", "kernels_bsoi.cu", "kernels_bstri.cu", "kernels_panel.cu", "kernels_tri.cu", "kernels_gemm.cu", "pipeline.cu", "kernels_dqmc.cu", "autotune.cu", "noalloc.cu"]
+CU_SOURCES = ["kernels_bsof.cu", "kernels_bsoi.cu", "kernels_bstri.cu", "kernels_panel.cu", "kernels_tri.cu", "kernels_gemm.cu", "pipeline.cu", "kernels_dqmc.cu", "autotune.cu", "noalloc.cu", "kernels_ozaki.cu"]
 C_SOURCES = ["bsofi_api.c", "batch.c", "server.c"]
 # The single-precision library: the same device objects, the float API and
 # its conversion kernels.

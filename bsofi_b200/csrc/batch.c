@@ -60,12 +60,24 @@ static cudaError_t pool_get(int want, stream_pool **out) {
 
 static double cost(int n, int L) { return 7.0 * (double)n * (double)n * (double)n * L * L; }
 
-unsigned long long bsofi_batch_workspace_bytes(int count, const int *n, const int *L,
-                                               const int *ldda) {
+/* Workspace of one instance at `precision` (0 FP64, 1 mixed). */
+static size_t inst_ws(int n, int L, int ldda, int precision) {
+  return precision == 1 ? bsofi_dev_ws_bytes_mixed(n, L, ldda, BSOFI_MIXED_SLICES)
+                        : bsofi_dev_ws_bytes(n, L, ldda);
+}
+
+unsigned long long bsofi_batch_workspace_bytes_ex(int count, const int *n, const int *L,
+                                                  const int *ldda, int precision) {
   unsigned long long tot = 0;
   int i;
-  for (i = 0; i < count; i++) tot += align256(bsofi_dev_ws_bytes(n[i], L[i], ldda[i]));
+  if (precision != 0 && precision != 1) return 0;
+  for (i = 0; i < count; i++) tot += align256(inst_ws(n[i], L[i], ldda[i], precision));
   return tot;
+}
+
+unsigned long long bsofi_batch_workspace_bytes(int count, const int *n, const int *L,
+                                               const int *ldda) {
+  return bsofi_batch_workspace_bytes_ex(count, n, L, ldda, 0);
 }
 
 typedef struct {
@@ -81,6 +93,12 @@ static int by_cost_desc(const void *a, const void *b) {
 int bsofi_device_invert_batched(int count, const int *n, const int *L, double *const *dA,
                                 const int *ldda, double *const *dtau, void *dwork, int streams,
                                 void *stream) {
+  return bsofi_device_invert_batched_ex(count, n, L, dA, ldda, dtau, dwork, streams, 0, stream);
+}
+
+int bsofi_device_invert_batched_ex(int count, const int *n, const int *L, double *const *dA,
+                                   const int *ldda, double *const *dtau, void *dwork, int streams,
+                                   int precision, void *stream) {
   stream_pool *p;
   order_t *ord;
   size_t *off;
@@ -88,6 +106,7 @@ int bsofi_device_invert_batched(int count, const int *n, const int *L, double *c
   int i, used, r = 0;
   long long launches = 0;
   if (count < 0 || (count > 0 && (!n || !L || !dA || !ldda || !dtau || !dwork))) return -1;
+  if (precision != 0 && precision != 1) return -1;
   for (i = 0; i < count; i++)
     if (n[i] < 1 || n[i] > BSOFI_MAX_BLOCK || L[i] < 2 || ldda[i] < n[i] * L[i] || !dA[i] ||
         !dtau[i])
@@ -111,7 +130,7 @@ int bsofi_device_invert_batched(int count, const int *n, const int *L, double *c
       ord[i].c = cost(n[i], L[i]);
       ord[i].i = i;
       off[i] = o;
-      o += align256(bsofi_dev_ws_bytes(n[i], L[i], ldda[i]));
+      o += align256(inst_ws(n[i], L[i], ldda[i], precision));
     }
   }
   qsort(ord, count, sizeof(order_t), by_cost_desc);
@@ -122,8 +141,12 @@ int bsofi_device_invert_batched(int count, const int *n, const int *L, double *c
     const int k = ord[i].i;
     /* Few BSOF workers per instance: the batch supplies the parallelism. */
     const int workers = n[k] <= 256 ? 6 : 24;
-    r = bsofi_dev_invert_ex(n[k], L[k], dA[k], ldda[k], dtau[k], (char *)dwork + off[k],
-                            p->s[i % used], workers);
+    if (precision == 1)
+      r = bsofi_dev_invert_mixed(n[k], L[k], dA[k], ldda[k], dtau[k], (char *)dwork + off[k],
+                                 p->s[i % used], workers, BSOFI_MIXED_SLICES);
+    else
+      r = bsofi_dev_invert_ex(n[k], L[k], dA[k], ldda[k], dtau[k], (char *)dwork + off[k],
+                              p->s[i % used], workers);
     if (r) {
       e = (cudaError_t)r;
       goto fail;

@@ -1042,6 +1042,41 @@ int bsofi_device_invert(int n, int L, double *dA, int ldda, double *dtau, void *
   return e ? cuda_info((cudaError_t)e) : 0;
 }
 
+static int mixed_slices(int slices) { return slices == 0 ? BSOFI_MIXED_SLICES : slices; }
+
+unsigned long long bsofi_device_workspace_bytes_mixed(int n, int L, int ldda, int slices) {
+  slices = mixed_slices(slices);
+  if (n < 1 || n > BSOFI_MAX_BLOCK || L < 2 || ldda < n * L || slices < 3 || slices > 8) return 0;
+  return (unsigned long long)bsofi_dev_ws_bytes_mixed(n, L, ldda, slices);
+}
+
+int bsofi_device_invert_mixed(int n, int L, double *dA, int ldda, double *dtau, void *dwork,
+                              int slices, void *stream) {
+  int e;
+  slices = mixed_slices(slices);
+  if (!device_args_ok(n, L, dA, ldda, dtau, dwork) || slices < 3 || slices > 8) return -1;
+  e = bsofi_dev_prepare();
+  if (!e) e = bsofi_dev_invert_mixed(n, L, dA, ldda, dtau, dwork, stream, 0, slices);
+  return e ? cuda_info((cudaError_t)e) : 0;
+}
+
+unsigned long long bsofi_selftest_ozaki_scratch_bytes(int M, int N, int K, int slices) {
+  return (unsigned long long)bsofi_dev_ozaki_scratch_bytes(M, N, K, mixed_slices(slices));
+}
+
+int bsofi_selftest_ozaki(int M, int N, int K, const double *dA, int lda, const double *dB, int ldb,
+                         double *dC, int ldc, int slices, void *dscratch, int *derr,
+                         void *stream) {
+  int e;
+  slices = mixed_slices(slices);
+  if (M < 1 || N < 1 || K < 1 || K > 1536 || lda < M || ldb < K || ldc < M || !dA || !dB ||
+      !dC || !dscratch || !derr || slices < 3 || slices > 8)
+    return -1;
+  e = bsofi_dev_selftest_ozaki(M, N, K, dA, lda, dB, ldb, dC, ldc, slices, dscratch, derr,
+                               stream);
+  return e ? cuda_info((cudaError_t)e) : 0;
+}
+
 int *bsofi_device_info(void *dwork) { return bsofi_dev_info_ptr(dwork); }
 
 long long bsofi_device_last_launches(void) { return bsofi_dev_launch_count(); }

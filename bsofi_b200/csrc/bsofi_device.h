@@ -45,6 +45,21 @@ int bsofi_dev_invert(int n, int L, double *dA, int ldd, double *dtau, void *dws,
 int bsofi_dev_invert_ex(int n, int L, double *dA, int ldd, double *dtau, void *dws, void *stream,
                         int workers);
 
+/* The same inversion with BSOI's products on the int8 tensor cores (Ozaki
+ * scheme, `slices` 3..8 slices per operand; 2n <= 1536).  dws holds
+ * bsofi_dev_ws_bytes_mixed bytes: the FP64 workspace followed by the
+ * product's scratch. */
+size_t bsofi_dev_ws_bytes_mixed(int n, int L, int ldd, int slices);
+int bsofi_dev_invert_mixed(int n, int L, double *dA, int ldd, double *dtau, void *dws,
+                           void *stream, int workers, int slices);
+/* One product C = A B (M x K times K x N, column-major) on the int8 tensor
+ * cores, for tests; scratch of bsofi_dev_ozaki_scratch_bytes, derr a device
+ * int set to 1 if a bounded wait gave up. */
+size_t bsofi_dev_ozaki_scratch_bytes(int M, int N, int K, int slices);
+int bsofi_dev_selftest_ozaki(int M, int N, int K, const double *dA, int lda, const double *dB,
+                             int ldb, double *dC, int ldc, int slices, void *scratch, int *derr,
+                             void *stream);
+
 /* BSOI: A (reflectors + R^{-1}) <- M^{-1}. */
 int bsofi_dev_bsoi(int n, int L, double *dA, int ldd, const double *dtau, void *dws,
                    void *stream);

@@ -122,6 +122,34 @@ cudaError_t preload_one(F* f, size_t* local) {
   if (e == cudaSuccess && at.localSizeBytes > *local) *local = at.localSizeBytes;
   return e;
 }
+// FP64 product C = A B on the int8 tensor cores by the Ozaki splitting
+// scheme with S slices (kernels_ozaki.cu).  A (M x K) has two K segments as
+// GemmA (k < ksplit: a0 with the row limit rlim0 and the mask r - roff0 > k;
+// else a1), B is K x N column-major, C goes to two column segments as GemmC
+// (j < nsplit: c0, else c1).  C must not overlap A or B.  scratch: 256-byte
+// aligned, ozaki_scratch_bytes(M, N, K, S).  err: set to 1 when a bounded
+// wait inside the kernel gives up.
+constexpr int kOzakiMinSlices = 3, kOzakiMaxSlices = 8, kOzakiMaxK = 1536;
+struct OzProduct {
+  const double* a0;
+  const double* a1;
+  long long lda0, lda1;
+  int ksplit, rlim0, roff0;
+  int M, K;
+  const double* b;
+  long long ldb;
+  int N;
+  double* c0;
+  double* c1;
+  long long ldc0, ldc1;
+  int nsplit;
+  int S;
+  void* scratch;
+  int* err;
+};
+size_t ozaki_scratch_bytes(int M, int N, int K, int S);
+cudaError_t launch_ozaki_product(const OzProduct& p, cudaStream_t st);
+
 // One per kernel file: every kernel (each template instance) it launches.
 cudaError_t preload_bsof(size_t* local);
 cudaError_t preload_bsoi(size_t* local);
@@ -129,5 +157,6 @@ cudaError_t preload_bstri(size_t* local);
 cudaError_t preload_gemm(size_t* local);
 cudaError_t preload_panel(size_t* local);
 cudaError_t preload_tri(size_t* local);
+cudaError_t preload_ozaki(size_t* local);
 
 }  // namespace bsofi

@@ -1,0 +1,477 @@
+// FP64 products on the int8 tensor cores (tcgen05 kind::i8): the Ozaki
+// splitting scheme.
+//
+// Method (Ozaki, Ogita, Oishi, Rump, "Error-free transformations of matrix
+// multiplication by using fast routines of matrix multiplication and its
+// applications", Numer. Algorithms 59, 2012; its integer form, Ootomo,
+// Ozaki, Yokota, "DGEMM on integer matrix multiplication unit", IJHPCA 2024):
+// every row i of A is scaled by a power of two 2^-e_i so that its largest
+// entry lies in [1/2, 1), and cut into S signed 7-bit integer slices,
+//   A(i,k) = 2^e_i * sum_s a_s(i,k) 2^-7(s+1) + r(i,k),  |r| < 2^(e_i - 7S);
+// every column j of B likewise with 2^f_j and slices b_t.  Products of
+// slices are exact in int32 (|a_s|, |b_t| <= 127, K <= 1536, at most 8
+// products per sum), and the S diagonals
+//   D_d = sum_{s+t=d} a_s b_t,  d = 0 .. S-1
+// accumulate in tensor memory; the terms with s+t >= S are below the
+// slices' resolution and dropped.  The epilogue forms, in FP64,
+//   C(i,j) = 2^(e_i+f_j) * sum_{d=S-1..0} D_d(i,j) 2^-7(d+2),
+// adding the diagonals from the smallest up.  Everything but that final sum
+// is exact, so the result is reproducible bit for bit (a numpy restatement
+// of the same arithmetic matches exactly).  With S = 8 the inverse's
+// residual matches the FP64 path's order; S = 7 reaches about 1e-12.
+//
+// Kernels: ozaki_split_kernel writes the slices and exponents of both
+// operands (one launch); ozaki_gemm_kernel is a warp-specialised tcgen05
+// kernel: warp 0 issues TMA tile loads (32-byte swizzle, K-major) into a
+// 4-stage mbarrier ring, warp 1 issues the S(S+1)/2 MMAs of each 32-deep K
+// step into S int32 accumulators of 128 x 64 in tensor memory, warps 2-5 read
+// the accumulators back (tcgen05.ld) and write the FP64 tile.  The tensor maps
+// cover this GPU's memory only and no load uses cluster multicast.
+#include <cuda.h>
+#include <climits>
+#include <mutex>
+
+#include "bsofi_common.cuh"
+#include "bsofi_kernels.h"
+#include "tcgen05.cuh"
+
+namespace bsofi {
+
+constexpr int OZ_BM = 128, OZ_BN = 64, OZ_BK = 32, OZ_STAGES = 4;
+constexpr int OZ_THREADS = 192;
+constexpr int OZ_EXP_NONFINITE = INT_MIN;  // exponent of a row/column holding Inf or NaN
+
+// ------------------------------------------------------------------ split
+struct OzSplitArgs {
+  // A: M x K, two K segments (k < ksplit: a0 with the masks rows >= rlim0 and
+  // r - roff0 > k zero; else a1), column-major.
+  const double* a0;
+  const double* a1;
+  long long lda0, lda1;
+  int ksplit, rlim0, roff0;
+  int M, K, Kp;
+  int8_t* a_out;       // S slices of M x Kp (row i of slice s at a_out + s*a_slice + i*Kp)
+  long long a_slice;
+  int* a_exp;          // M
+  // B: K x N column-major; column j becomes row j of the B slices.
+  const double* b;
+  long long ldb;
+  int N;
+  int8_t* b_out;
+  long long b_slice;
+  int* b_exp;          // N
+  int S;
+  int a_blocks;        // blocks [0, a_blocks) split A rows, the rest B columns
+};
+
+__device__ __forceinline__ double oz_a(const OzSplitArgs& s, int i, int k) {
+  if (k < s.ksplit) {
+    if (i >= s.rlim0 || i - s.roff0 > k) return 0.0;
+    return s.a0[(long long)k * s.lda0 + i];
+  }
+  return s.a1[(long long)(k - s.ksplit) * s.lda1 + i];
+}
+
+// Cut 16 scaled values (|r| < 1) into S slices of 16 bytes; r is consumed.
+__device__ __forceinline__ void oz_slices16(double (&r)[16], int S, int8_t* dst, long long stride) {
+  for (int s = 0; s < S; s++) {
+    uint32_t w[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      uint32_t word = 0;
+#pragma unroll
+      for (int b = 0; b < 4; b++) {
+        const double t = r[4 * q + b] * 128.0;
+        const double v = trunc(t);
+        r[4 * q + b] = t - v;  // exact
+        word |= ((uint32_t)(int)v & 0xffu) << (8 * b);
+      }
+      w[q] = word;
+    }
+    *reinterpret_cast<uint4*>(dst + (long long)s * stride) = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
+__global__ void __launch_bounds__(128) ozaki_split_kernel(OzSplitArgs s) {
+  if ((int)blockIdx.x < s.a_blocks) {
+    const int i = blockIdx.x * 128 + threadIdx.x;
+    if (i >= s.M) return;
+    double mx = 0.0;
+    for (int k = 0; k < s.K; k++) mx = fmax(mx, fabs(oz_a(s, i, k)));
+    int e = 0;
+    if (!isfinite(mx)) {
+      s.a_exp[i] = OZ_EXP_NONFINITE;
+      mx = 0.0;
+    } else {
+      frexp(mx, &e);
+      s.a_exp[i] = e;
+    }
+    int8_t* row = s.a_out + (long long)i * s.Kp;
+    for (int k0 = 0; k0 < s.Kp; k0 += 16) {
+      double r[16];
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        const int k = k0 + j;
+        r[j] = (mx > 0.0 && k < s.K) ? ldexp(oz_a(s, i, k), -e) : 0.0;
+      }
+      oz_slices16(r, s.S, row + k0, s.a_slice);
+    }
+    return;
+  }
+  // B columns: one warp per column.
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int j = ((int)blockIdx.x - s.a_blocks) * 4 + warp;
+  if (j >= s.N) return;
+  const double* col = s.b + (long long)j * s.ldb;
+  double mx = 0.0;
+  for (int k = lane; k < s.K; k += 32) mx = fmax(mx, fabs(col[k]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  int e = 0;
+  if (!isfinite(mx)) {
+    if (lane == 0) s.b_exp[j] = OZ_EXP_NONFINITE;
+    mx = 0.0;
+  } else {
+    frexp(mx, &e);
+    if (lane == 0) s.b_exp[j] = e;
+  }
+  int8_t* row = s.b_out + (long long)j * s.Kp;
+  for (int k0 = lane * 16; k0 < s.Kp; k0 += 32 * 16) {
+    double r[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      const int k = k0 + q;
+      r[q] = (mx > 0.0 && k < s.K) ? ldexp(col[k], -e) : 0.0;
+    }
+    oz_slices16(r, s.S, row + k0, s.b_slice);
+  }
+}
+
+// ------------------------------------------------------------------ GEMM
+struct OzGemmArgs {
+  int M, N, Kp;
+  const int* a_exp;
+  const int* b_exp;
+  // Output segments: column j < nsplit -> c0 + j*ldc0, else c1 + (j-nsplit)*ldc1.
+  double* c0;
+  double* c1;
+  long long ldc0, ldc1;
+  int nsplit;
+  int* err;
+  long long spin_limit;
+};
+
+template <int S>
+struct OzCfg {
+  static constexpr int A_TILE = OZ_BM * OZ_BK;  // bytes of one A slice tile
+  static constexpr int B_TILE = OZ_BN * OZ_BK;
+  static constexpr int STAGE = S * (A_TILE + B_TILE);
+  // + alignment slack; at least 120 KB so that one CTA holds an SM alone and
+  // its tensor-memory allocation never waits for another CTA's.
+  static constexpr size_t NEED = (size_t)OZ_STAGES * STAGE + 1024;
+  static constexpr size_t SMEM = NEED > 120 * 1024 ? NEED : 120 * 1024;
+  static constexpr uint32_t TMEM_COLS = S * OZ_BN <= 256 ? 256 : 512;
+  static_assert(S * OZ_BN <= 512, "accumulators exceed tensor memory");
+};
+
+template <int S>
+__global__ void __launch_bounds__(OZ_THREADS, 1)
+    ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tma_a,
+                      const __grid_constant__ CUtensorMap tma_b, OzGemmArgs g) {
+  using C = OzCfg<S>;
+  extern __shared__ uint8_t oz_smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)oz_smem_raw + 1023) & ~(uintptr_t)1023);
+  __shared__ __align__(8) uint64_t full[OZ_STAGES];
+  __shared__ __align__(8) uint64_t empty[OZ_STAGES];
+  __shared__ __align__(8) uint64_t acc_full;
+  __shared__ uint32_t tmem_base;
+  __shared__ int abort_flag;
+  __shared__ int no_abort;  // never set: waits that must not give up on an abort
+  volatile int* abort_v = &abort_flag;
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int m0 = blockIdx.x * OZ_BM, n0 = blockIdx.y * OZ_BN;
+  const int nk = g.Kp / OZ_BK;
+  constexpr uint32_t IDESC = tc::idesc_i8(OZ_BM, OZ_BN);
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < OZ_STAGES; i++) {
+      tc::mbar_init(&full[i], 1);
+      tc::mbar_init(&empty[i], 1);
+    }
+    tc::mbar_init(&acc_full, 1);
+    abort_flag = 0;
+    no_abort = 0;
+    tc::fence_barrier_init();
+  }
+  if (warp == 0) {
+    tc::tmem_alloc(&tmem_base, C::TMEM_COLS);
+    tc::tmem_relinquish();
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tbase = tmem_base;
+  int issued = 0;  // K steps whose loads warp 0 issued
+
+  if (warp == 0 && lane == 0) {
+    // TMA producer.
+    tc::prefetch_tmap(&tma_a);
+    tc::prefetch_tmap(&tma_b);
+    for (int kc = 0; kc < nk; kc++) {
+      const int st = kc % OZ_STAGES;
+      if (kc >= OZ_STAGES &&
+          !tc::mbar_wait(&empty[st], ((kc / OZ_STAGES) - 1) & 1, g.spin_limit, abort_v)) {
+        abort_flag = 1;
+        atomicExch(g.err, 1);
+        break;
+      }
+      tc::mbar_arrive_expect_tx(&full[st], C::STAGE);
+      uint8_t* sa = smem + (size_t)st * C::STAGE;
+      uint8_t* sb = sa + S * C::A_TILE;
+      for (int s = 0; s < S; s++) tc::tma_load_3d(sa + s * C::A_TILE, &tma_a, &full[st], kc * OZ_BK, m0, s);
+      for (int t = 0; t < S; t++) tc::tma_load_3d(sb + t * C::B_TILE, &tma_b, &full[st], kc * OZ_BK, n0, t);
+      issued = kc + 1;
+    }
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer: accumulator d (columns d*64 .. d*64+63) collects s + t = d.
+    for (int kc = 0; kc < nk; kc++) {
+      const int st = kc % OZ_STAGES;
+      if (!tc::mbar_wait(&full[st], (kc / OZ_STAGES) & 1, g.spin_limit, abort_v)) {
+        abort_flag = 1;
+        atomicExch(g.err, 1);
+        break;
+      }
+      tc::tc_fence_after();
+      const uint8_t* sa = smem + (size_t)st * C::STAGE;
+      const uint8_t* sb = sa + S * C::A_TILE;
+#pragma unroll
+      for (int s = 0; s < S; s++) {
+        const uint64_t da = tc::desc_k_sw32(sa + s * C::A_TILE);
+#pragma unroll
+        for (int t = 0; s + t < S; t++)
+          tc::mma_i8(tbase + (uint32_t)((s + t) * OZ_BN), da, tc::desc_k_sw32(sb + t * C::B_TILE),
+                     IDESC, (kc > 0 || s > 0) ? 1u : 0u);
+      }
+      tc::mma_commit(&empty[st]);  // the stage is free once these MMAs have read it
+    }
+    tc::mma_commit(&acc_full);  // every MMA issued above is complete
+  } else if (warp >= 2) {
+    // Epilogue: warp w reads tensor-memory lanes 32 (w % 4) .. +31.
+    const int q = warp % 4;
+    // tcgen05.ld is warp-collective: the whole warp goes on or none of it.
+    const bool got = tc::mbar_wait(&acc_full, 0, g.spin_limit, abort_v) && !*abort_v;
+    if (__all_sync(0xffffffffu, got)) {
+      tc::tc_fence_after();
+      const int row = m0 + 32 * q + lane;
+      const int er = row < g.M ? g.a_exp[row] : 0;
+      const uint32_t lane_addr = tbase + ((uint32_t)(32 * q) << 16);
+      for (int c0 = 0; c0 < OZ_BN; c0 += 16) {
+        double acc[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++) acc[j] = 0.0;
+#pragma unroll
+        for (int d = S - 1; d >= 0; d--) {
+          uint32_t v[16];
+          tc::tmem_ld16(lane_addr + (uint32_t)(d * OZ_BN + c0), v);
+          tc::tmem_ld_wait();
+          const double sc = ldexp(1.0, -7 * (d + 2));
+#pragma unroll
+          for (int j = 0; j < 16; j++) acc[j] += (double)(int)v[j] * sc;
+        }
+        if (row < g.M) {
+#pragma unroll
+          for (int j = 0; j < 16; j++) {
+            const int col = n0 + c0 + j;
+            if (col < g.N) {
+              const int ec = g.b_exp[col];
+              double out;
+              if (er == OZ_EXP_NONFINITE || ec == OZ_EXP_NONFINITE) out = __longlong_as_double(0x7ff8000000000000ll);
+              else out = ldexp(acc[j], er + ec);
+              double* p = col < g.nsplit ? g.c0 + (long long)col * g.ldc0
+                                         : g.c1 + (long long)(col - g.nsplit) * g.ldc1;
+              p[row] = out;
+            }
+          }
+        }
+      }
+    } else {
+      abort_flag = 1;
+      atomicExch(g.err, 1);
+    }
+  }
+
+  // Teardown: no TMA write or MMA may still be in flight when the CTA's shared
+  // and tensor memory are released (on the normal path these waits return at
+  // once; after an abort they wait, bounded, for copies and MMAs in flight).
+  if (warp == 0 && lane == 0) {
+    const int from = issued > OZ_STAGES ? issued - OZ_STAGES : 0;
+    for (int kc = from; kc < issued; kc++)
+      tc::mbar_wait(&full[kc % OZ_STAGES], (kc / OZ_STAGES) & 1, g.spin_limit, &no_abort);
+  }
+  if (warp == 1 && lane == 0) tc::mbar_wait(&acc_full, 0, g.spin_limit, &no_abort);
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc::tc_fence_after();
+    tc::tmem_dealloc(tbase, C::TMEM_COLS);
+  }
+}
+
+// ------------------------------------------------------------------ host
+namespace {
+
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                 const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                 const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled from the driver, found once through the runtime.
+EncodeTiled encode_tiled() {
+  static std::once_flag once;
+  static EncodeTiled fn = nullptr;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiled>(p);
+  });
+  return fn;
+}
+
+// Tensor map of `slices` int8 matrices of rows x Kp (K contiguous), read in
+// boxes of 32 (K) x box_rows x 1 with the 32-byte swizzle.
+cudaError_t slice_map(CUtensorMap* m, const int8_t* base, int Kp, int rows, int slices,
+                      int box_rows) {
+  EncodeTiled f = encode_tiled();
+  if (!f) return cudaErrorNotSupported;
+  const cuuint64_t dims[3] = {(cuuint64_t)Kp, (cuuint64_t)rows, (cuuint64_t)slices};
+  const cuuint64_t strides[2] = {(cuuint64_t)Kp, (cuuint64_t)Kp * (cuuint64_t)rows};
+  const cuuint32_t box[3] = {(cuuint32_t)OZ_BK, (cuuint32_t)box_rows, 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  const CUresult r = f(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<int8_t*>(base), dims,
+                       strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
+                       CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
+int kpad(int K) { return (K + OZ_BK - 1) / OZ_BK * OZ_BK; }
+
+struct OzScratch {
+  int8_t* a;
+  int8_t* b;
+  int* ea;
+  int* eb;
+};
+
+OzScratch carve(void* base, int M, int N, int K, int S) {
+  const size_t Kp = (size_t)kpad(K);
+  char* p = static_cast<char*>(base);
+  OzScratch o;
+  o.a = reinterpret_cast<int8_t*>(p);
+  p += al256((size_t)S * M * Kp);
+  o.b = reinterpret_cast<int8_t*>(p);
+  p += al256((size_t)S * N * Kp);
+  o.ea = reinterpret_cast<int*>(p);
+  p += al256(sizeof(int) * (size_t)M);
+  o.eb = reinterpret_cast<int*>(p);
+  return o;
+}
+
+template <int S>
+cudaError_t gemm_s(const CUtensorMap& ma, const CUtensorMap& mb, const OzGemmArgs& g,
+                   cudaStream_t st) {
+  static PerDevice once;
+  const int pend = once.pending();
+  if (pend >= 0) {
+    cudaError_t e = cudaFuncSetAttribute(ozaki_gemm_kernel<S>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)OzCfg<S>::SMEM);
+    if (e != cudaSuccess) return e;
+    once.mark(pend);
+  }
+  const dim3 grid((g.M + OZ_BM - 1) / OZ_BM, (g.N + OZ_BN - 1) / OZ_BN);
+  ozaki_gemm_kernel<S><<<grid, OZ_THREADS, OzCfg<S>::SMEM, st>>>(ma, mb, g);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t ozaki_scratch_bytes(int M, int N, int K, int S) {
+  const size_t Kp = (size_t)kpad(K);
+  return al256((size_t)S * M * Kp) + al256((size_t)S * N * Kp) + al256(sizeof(int) * (size_t)M) +
+         al256(sizeof(int) * (size_t)N);
+}
+
+cudaError_t launch_ozaki_product(const OzProduct& p, cudaStream_t st) {
+  if (p.M <= 0 || p.N <= 0 || p.K <= 0) return cudaSuccess;
+  if (p.S < kOzakiMinSlices || p.S > kOzakiMaxSlices || p.K > kOzakiMaxK) return cudaErrorInvalidValue;
+  if (((uintptr_t)p.scratch & 255) != 0) return cudaErrorInvalidValue;
+  const int Kp = kpad(p.K);
+  OzScratch o = carve(p.scratch, p.M, p.N, p.K, p.S);
+  OzSplitArgs sa;
+  sa.a0 = p.a0;
+  sa.a1 = p.a1;
+  sa.lda0 = p.lda0;
+  sa.lda1 = p.lda1;
+  sa.ksplit = p.ksplit;
+  sa.rlim0 = p.rlim0;
+  sa.roff0 = p.roff0;
+  sa.M = p.M;
+  sa.K = p.K;
+  sa.Kp = Kp;
+  sa.a_out = o.a;
+  sa.a_slice = (long long)p.M * Kp;
+  sa.a_exp = o.ea;
+  sa.b = p.b;
+  sa.ldb = p.ldb;
+  sa.N = p.N;
+  sa.b_out = o.b;
+  sa.b_slice = (long long)p.N * Kp;
+  sa.b_exp = o.eb;
+  sa.S = p.S;
+  sa.a_blocks = (p.M + 127) / 128;
+  const int b_blocks = (p.N + 3) / 4;
+  ozaki_split_kernel<<<sa.a_blocks + b_blocks, 128, 0, st>>>(sa);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  CUtensorMap ma, mb;
+  if ((e = slice_map(&ma, o.a, Kp, p.M, p.S, OZ_BM)) != cudaSuccess) return e;
+  if ((e = slice_map(&mb, o.b, Kp, p.N, p.S, OZ_BN)) != cudaSuccess) return e;
+  OzGemmArgs g;
+  g.M = p.M;
+  g.N = p.N;
+  g.Kp = Kp;
+  g.a_exp = o.ea;
+  g.b_exp = o.eb;
+  g.c0 = p.c0;
+  g.c1 = p.c1;
+  g.ldc0 = p.ldc0;
+  g.ldc1 = p.ldc1;
+  g.nsplit = p.nsplit;
+  g.err = p.err;
+  g.spin_limit = 1ll << 20;  // polls of mbarrier.try_wait: about a second at most
+  switch (p.S) {
+    case 3: return gemm_s<3>(ma, mb, g, st);
+    case 4: return gemm_s<4>(ma, mb, g, st);
+    case 5: return gemm_s<5>(ma, mb, g, st);
+    case 6: return gemm_s<6>(ma, mb, g, st);
+    case 7: return gemm_s<7>(ma, mb, g, st);
+    default: return gemm_s<8>(ma, mb, g, st);
+  }
+}
+
+cudaError_t preload_ozaki(size_t* local) {
+  cudaError_t e;
+  if ((e = preload_one(ozaki_split_kernel, local)) != cudaSuccess) return e;
+  if ((e = preload_one(ozaki_gemm_kernel<3>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(ozaki_gemm_kernel<4>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(ozaki_gemm_kernel<5>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(ozaki_gemm_kernel<6>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(ozaki_gemm_kernel<7>, local)) != cudaSuccess) return e;
+  return preload_one(ozaki_gemm_kernel<8>, local);
+}
+
+}  // namespace bsofi

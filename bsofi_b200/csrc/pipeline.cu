@@ -803,6 +803,50 @@ int run_bsoi_rows(int n, int L, double* dA, int ldd, const double* dtau, void* w
   return 0;
 }
 
+// BSOI with every step's product on the int8 tensor cores (Ozaki scheme with
+// S slices; kernels_ozaki.cu): the same steps, operands and output segments
+// as bsoi_step, the zero structure applied while the operand is sliced.
+// oz: the product's scratch (ozaki_scratch_bytes(N, 2n, 2n, S)), reused by
+// every step (the steps run in order on `st`).
+int run_bsoi_mixed(int n, int L, double* dA, int ldd, void* ws, void* oz, int S, cudaStream_t st) {
+  Layout ly = layout(n, L, ldd);
+  double* G = at<double>(ws, ly.G);
+  double* C[2] = {at<double>(ws, ly.C0), at<double>(ws, ly.C1)};
+  const int N = n * L, n2 = 2 * n;
+  const long long g2 = (long long)n2 * n2;
+  int e = bsoi_carry(n, L, dA, ldd, ws, st);
+  if (e) return e;
+  for (int k = L - 2; k >= 0; k--) {
+    const int rd = (L - 2 - k) & 1;
+    OzProduct p = {};
+    p.a0 = dA + cm(0, (long long)k * n, ldd);
+    p.lda0 = ldd;
+    p.a1 = C[rd];
+    p.lda1 = ldd;
+    p.ksplit = n;
+    p.rlim0 = (k + 1) * n;
+    p.roff0 = k * n;
+    p.M = N;
+    p.K = n2;
+    p.b = G + (size_t)k * g2;
+    p.ldb = n2;
+    p.N = n2;
+    p.c0 = C[rd ^ 1];
+    p.ldc0 = ldd;
+    p.c1 = dA + cm(0, (long long)(k + 1) * n, ldd);
+    p.ldc1 = ldd;
+    p.nsplit = n;
+    p.S = S;
+    p.scratch = oz;
+    p.err = at<int>(ws, ly.info) + 2;
+    if (g_timer.on) CKM(g_timer.mark(st));
+    CKM(launch_ozaki_product(p, st));
+    g_launches += 2;  // the split and the product
+    if (g_timer.on) CKM(g_timer.mark(st));
+  }
+  return bsoi_finish(n, L, dA, ldd, ws, st);
+}
+
 int run_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* ws, cudaStream_t st,
              bool q_ready) {
   Layout ly = layout(n, L, ldd);
@@ -841,6 +885,54 @@ extern "C" {
 
 size_t bsofi_dev_ws_bytes(int n, int L, int ldd) { return layout(n, L, ldd).total; }
 
+size_t bsofi_dev_ws_bytes_mixed(int n, int L, int ldd, int slices) {
+  return layout(n, L, ldd).total + ozaki_scratch_bytes(n * L, 2 * n, 2 * n, slices);
+}
+
+int bsofi_dev_invert_mixed(int n, int L, double* dA, int ldd, double* dtau, void* dws,
+                           void* stream, int workers, int slices) {
+  g_launches = 0;
+  if (slices < kOzakiMinSlices || slices > kOzakiMaxSlices || 2 * n > kOzakiMaxK)
+    return (int)cudaErrorInvalidValue;
+  int e = run_bsoftri(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, true,
+                      bsof_workers(n, L, workers), workers == 0);
+  if (e) return e;
+  void* oz = at<char>(dws, layout(n, L, ldd).total);
+  return run_bsoi_mixed(n, L, dA, ldd, dws, oz, slices, (cudaStream_t)stream);
+}
+
+size_t bsofi_dev_ozaki_scratch_bytes(int M, int N, int K, int slices) {
+  return ozaki_scratch_bytes(M, N, K, slices);
+}
+
+int bsofi_dev_selftest_ozaki(int M, int N, int K, const double* dA, int lda, const double* dB,
+                             int ldb, double* dC, int ldc, int slices, void* scratch, int* derr,
+                             void* stream) {
+  OzProduct p = {};
+  p.a0 = dA;
+  p.lda0 = lda;
+  p.a1 = dA;
+  p.lda1 = lda;
+  p.ksplit = K;
+  p.rlim0 = INT_MAX;
+  p.roff0 = kNoMask;
+  p.M = M;
+  p.K = K;
+  p.b = dB;
+  p.ldb = ldb;
+  p.N = N;
+  p.c0 = dC;
+  p.ldc0 = ldc;
+  p.c1 = dC;
+  p.ldc1 = ldc;
+  p.nsplit = N;
+  p.S = slices;
+  p.scratch = scratch;
+  p.err = derr;
+  g_launches = 2;
+  return (int)launch_ozaki_product(p, (cudaStream_t)stream);
+}
+
 int bsofi_dev_prepare(void) { return (int)gemm_init_attributes(); }
 
 int bsofi_dev_preload(void) {
@@ -853,6 +945,7 @@ int bsofi_dev_preload(void) {
   if ((e = preload_gemm(&local)) != cudaSuccess) return (int)e;
   if ((e = preload_panel(&local)) != cudaSuccess) return (int)e;
   if ((e = preload_tri(&local)) != cudaSuccess) return (int)e;
+  if ((e = preload_ozaki(&local)) != cudaSuccess) return (int)e;
   if ((e = preload_one(build_leaf_t_kernel, &local)) != cudaSuccess) return (int)e;
   // The context's local-memory reservation grows at the launch of a kernel
   // that needs more than it holds; growing it here keeps later launches from

@@ -15,6 +15,17 @@
  *     smaller ones behind it at most BYPASS_LIMIT times, after which nothing
  *     is admitted until it fits (no starvation);
  *   * a request whose workspace exceeds the whole pool fails at submission.
+ * Two kinds of request:
+ *   * caller-owned (bsofi_server_submit): the caller's matrix is inverted in
+ *     place; the pool holds only the workspace;
+ *   * server-owned (bsofi_server_submit_blocks): the request is given by its
+ *     packed p-cyclic blocks; at admission the pool supplies the matrix, tau
+ *     and the workspace together (admission by the full memory footprint, up
+ *     to 17 GB for n = 576, L = 80), the matrix is assembled in the pool and
+ *     inverted there; the workspace returns to the pool when the inversion
+ *     ends, the matrix and tau stay resident until bsofi_server_release.
+ * Precision 0 runs the FP64 pipeline, 1 the mixed one (BSOI on the int8
+ * tensor cores, bsofi_device_invert_mixed).
  * Progress is driven by bsofi_server_poll (no background thread): it retires
  * finished requests (event query, no device synchronisation) and admits new
  * ones.  One server is used by one host thread at a time.
@@ -33,18 +44,30 @@
 typedef struct {
   long long id;
   int n, L, ldda, precision;
-  double *dA, *dtau;
-  size_t ws;
+  double *dA, *dtau;  /* caller-owned request: the caller's buffers */
+  const double *dD, *dS; /* server-owned request: packed blocks (until admission) */
+  int owned;
+  size_t ws;  /* workspace bytes */
+  size_t mat; /* server-owned: matrix + tau bytes, 0 otherwise */
 } request;
 
 typedef struct {
   int busy;
   long long id;
-  size_t off, len;
+  size_t off, len;         /* workspace in the pool */
+  size_t moff, mlen;       /* server-owned matrix + tau in the pool (mlen 0: none) */
+  int ldda, n, L;
   cudaStream_t stream;
   cudaEvent_t done;
   int *hinfo; /* pinned: BSTRI info word, BSOF / BSOI / BSTRI wait error words */
 } slot;
+
+/* A finished server-owned request whose matrix and tau are still resident. */
+typedef struct {
+  long long id;
+  size_t moff, mlen;
+  int ldda, N;
+} resident;
 
 typedef struct {
   size_t off, len;
@@ -61,6 +84,8 @@ struct bsofi_server {
   int qhead, qlen, qcap;
   int bypassed;
   long long next_id;
+  resident *res;
+  int nres, cap_res;
 };
 
 typedef struct bsofi_server bsofi_server;
@@ -179,11 +204,29 @@ void bsofi_server_destroy(bsofi_server *sv) {
   if (sv->pool) cudaFree(sv->pool);
   free(sv->free_list);
   free(sv->queue);
+  free(sv->res);
   free(sv);
 }
 
+static size_t ws_bytes(int n, int L, int ldda, int precision) {
+  return align256(precision == 1 ? bsofi_dev_ws_bytes_mixed(n, L, ldda, BSOFI_MIXED_SLICES)
+                                 : bsofi_dev_ws_bytes(n, L, ldda));
+}
+
+static int owned_ldda(int n, int L) { return (n * L + 31) / 32 * 32; }
+
+static size_t mat_bytes(int n, int L) {
+  const int N = n * L;
+  return align256(sizeof(double) * (size_t)owned_ldda(n, L) * N) + align256(sizeof(double) * N);
+}
+
 unsigned long long bsofi_server_request_bytes(int n, int L, int ldda) {
-  return align256(bsofi_dev_ws_bytes(n, L, ldda));
+  return ws_bytes(n, L, ldda, 0);
+}
+
+unsigned long long bsofi_server_footprint_bytes(int n, int L, int precision) {
+  if (n < 1 || n > BSOFI_MAX_BLOCK || L < 2 || (precision != 0 && precision != 1)) return 0;
+  return ws_bytes(n, L, owned_ldda(n, L), precision) + mat_bytes(n, L);
 }
 
 long long bsofi_server_submit(bsofi_server *sv, int n, int L, double *dA, int ldda,
@@ -191,8 +234,9 @@ long long bsofi_server_submit(bsofi_server *sv, int n, int L, double *dA, int ld
   request r;
   if (!sv) return -1;
   if (n < 1 || n > BSOFI_MAX_BLOCK || L < 2 || ldda < n * L || !dA || !dtau) return -2;
-  if (precision != 0) return -3; /* only the FP64 path is served */
-  r.ws = align256(bsofi_dev_ws_bytes(n, L, ldda));
+  if (precision != 0 && precision != 1) return -3;
+  memset(&r, 0, sizeof(r));
+  r.ws = ws_bytes(n, L, ldda, precision);
   if (r.ws > sv->pool_bytes) return -4; /* can never be admitted */
   r.id = sv->next_id++;
   r.n = n;
@@ -205,10 +249,74 @@ long long bsofi_server_submit(bsofi_server *sv, int n, int L, double *dA, int ld
   return r.id;
 }
 
+long long bsofi_server_submit_blocks(bsofi_server *sv, int n, int L, const double *dD,
+                                     const double *dS, int precision) {
+  request r;
+  if (!sv) return -1;
+  if (n < 1 || n > BSOFI_MAX_BLOCK || L < 2 || !dS) return -2;
+  if (precision != 0 && precision != 1) return -3;
+  memset(&r, 0, sizeof(r));
+  r.ldda = owned_ldda(n, L);
+  r.ws = ws_bytes(n, L, r.ldda, precision);
+  r.mat = mat_bytes(n, L);
+  if (r.ws + r.mat > sv->pool_bytes) return -4;
+  r.id = sv->next_id++;
+  r.n = n;
+  r.L = L;
+  r.precision = precision;
+  r.dD = dD;
+  r.dS = dS;
+  r.owned = 1;
+  if (!queue_push(sv, &r)) return -5;
+  return r.id;
+}
+
+static int find_resident(bsofi_server *sv, long long id) {
+  int i;
+  for (i = 0; i < sv->nres; i++)
+    if (sv->res[i].id == id) return i;
+  return -1;
+}
+
+int bsofi_server_result(bsofi_server *sv, long long id, double **dA, int *ldda, double **dtau) {
+  int i;
+  if (!sv || !dA || !ldda || !dtau) return -1;
+  i = find_resident(sv, id);
+  if (i < 0) return -1;
+  *dA = (double *)(sv->pool + sv->res[i].moff);
+  *ldda = sv->res[i].ldda;
+  *dtau = (double *)(sv->pool + sv->res[i].moff +
+                     align256(sizeof(double) * (size_t)sv->res[i].ldda * sv->res[i].N));
+  return 0;
+}
+
+int bsofi_server_release(bsofi_server *sv, long long id) {
+  int i;
+  if (!sv) return -1;
+  i = find_resident(sv, id);
+  if (i < 0) return -1;
+  if (!pool_free(sv, sv->res[i].moff, sv->res[i].mlen)) return -1;
+  sv->res[i] = sv->res[sv->nres - 1];
+  sv->nres--;
+  return 0;
+}
+
 static int launch(bsofi_server *sv, slot *sl, const request *r) {
-  int e, workers = r->n <= 256 ? 6 : 24;
+  int e = 0, workers = r->n <= 256 ? 6 : 24;
   void *ws = sv->pool + sl->off;
-  e = bsofi_dev_invert_ex(r->n, r->L, r->dA, r->ldda, r->dtau, ws, sl->stream, workers);
+  double *dA = r->dA, *dtau = r->dtau;
+  if (r->owned) {
+    dA = (double *)(sv->pool + sl->moff);
+    dtau = (double *)(sv->pool + sl->moff +
+                      align256(sizeof(double) * (size_t)r->ldda * r->n * r->L));
+    e = bsofi_device_assemble(r->n, r->L, r->dD, r->dS, dA, r->ldda, sl->stream);
+    if (e) return e <= BSOFI_INFO_CUDA ? BSOFI_INFO_CUDA - e : (int)cudaErrorInvalidValue;
+  }
+  if (r->precision == 1)
+    e = bsofi_dev_invert_mixed(r->n, r->L, dA, r->ldda, dtau, ws, sl->stream, workers,
+                               BSOFI_MIXED_SLICES);
+  else
+    e = bsofi_dev_invert_ex(r->n, r->L, dA, r->ldda, dtau, ws, sl->stream, workers);
   if (!e)
     e = (int)cudaMemcpyAsync(sl->hinfo, bsofi_dev_info_ptr(ws), 4 * sizeof(int),
                              cudaMemcpyDeviceToHost, sl->stream);
@@ -229,10 +337,21 @@ static int admit(bsofi_server *sv, long long *done_ids, int *done_status, int ma
         break;
       }
     if (!sl) break;
-    if (!pool_alloc(sv, r->ws, &off)) {
-      if (pos == 0 && sv->bypassed >= BYPASS_LIMIT) break; /* hold for the head */
-      pos++;
-      continue;
+    {
+      /* The whole footprint or nothing: workspace, then the owned matrix. */
+      size_t moff = 0;
+      int fits = pool_alloc(sv, r->ws, &off);
+      if (fits && r->mat > 0 && !pool_alloc(sv, r->mat, &moff)) {
+        pool_free(sv, off, r->ws);
+        fits = 0;
+      }
+      if (!fits) {
+        if (pos == 0 && sv->bypassed >= BYPASS_LIMIT) break; /* hold for the head */
+        pos++;
+        continue;
+      }
+      sl->moff = moff;
+      sl->mlen = r->mat;
     }
     if (pos > 0) sv->bypassed++;
     else sv->bypassed = 0;
@@ -240,11 +359,16 @@ static int admit(bsofi_server *sv, long long *done_ids, int *done_status, int ma
     sl->id = r->id;
     sl->off = off;
     sl->len = r->ws;
+    sl->ldda = r->ldda;
+    sl->n = r->n;
+    sl->L = r->L;
     {
       const int e = launch(sv, sl, r);
       if (e != 0) { /* a launch error retires the request at once */
         sl->busy = 0;
         pool_free(sv, off, r->ws);
+        if (sl->mlen) pool_free(sv, sl->moff, sl->mlen);
+        sl->mlen = 0;
         if (*ndone < max) {
           done_ids[*ndone] = r->id;
           done_status[*ndone] = BSOFI_INFO_CUDA - e;
@@ -274,6 +398,28 @@ int bsofi_server_poll(bsofi_server *sv, long long *done_ids, int *done_status, i
     ndone++;
     sl->busy = 0;
     pool_free(sv, sl->off, sl->len);
+    if (sl->mlen) {
+      /* The owned matrix and tau stay resident until bsofi_server_release. */
+      if (sv->nres == sv->cap_res) {
+        const int ncap = sv->cap_res ? 2 * sv->cap_res : 64;
+        resident *nr = (resident *)realloc(sv->res, sizeof(resident) * ncap);
+        if (!nr) { /* no host memory to track it: give the memory back */
+          pool_free(sv, sl->moff, sl->mlen);
+          done_status[ndone - 1] = BSOFI_INFO_CUDA - (int)cudaErrorMemoryAllocation;
+          sl->mlen = 0;
+          continue;
+        }
+        sv->res = nr;
+        sv->cap_res = ncap;
+      }
+      sv->res[sv->nres].id = sl->id;
+      sv->res[sv->nres].moff = sl->moff;
+      sv->res[sv->nres].mlen = sl->mlen;
+      sv->res[sv->nres].ldda = sl->ldda;
+      sv->res[sv->nres].N = sl->n * sl->L;
+      sv->nres++;
+      sl->mlen = 0;
+    }
   }
   admit(sv, done_ids, done_status, max, &ndone);
   return ndone;

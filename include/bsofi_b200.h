@@ -182,6 +182,25 @@ int bsofi_device_bsoi(int n, int L, double *dA, int ldda, const double *dtau, vo
 int bsofi_device_bsoi_rows(int n, int L, double *dA, int ldda, const double *dtau, void *dwork,
                            int row0, int row1, void *stream);
 int *bsofi_device_info(void *dwork);
+
+/* Mixed-precision inversion (no reference counterpart; the reference's
+ * BSOI products are FP64 LAPACK/MAGMA calls, src/bsofi_cpu.c:234-245 and
+ * src/bsofi_gpu.c:397-411).  The factorization (BSOF), the triangular
+ * inverse (BSTRI), tau, the reflectors and the diagonal TRTRI stay FP64; the
+ * p-1 BSOI products X(:,k:k+1) Q_k^T run on the int8 tensor cores by the
+ * Ozaki splitting scheme: each row of X and each column of Q_k^T is scaled by
+ * a power of two and cut into `slices` signed 7-bit integers, the slice
+ * products are summed exactly in int32 in tensor memory, and the result is
+ * formed in FP64 (slices = 0 means BSOFI_MIXED_SLICES = 8; valid 3..8).  With 8
+ * slices ||M X - I||_F / ||X||_F stays at the FP64 path's level (about 1e-14 on
+ * the Hubbard matrices); with 7 about 1e-12.  The result is deterministic.
+ * dwork holds bsofi_device_workspace_bytes_mixed bytes (the FP64 workspace
+ * plus the slices of one N x 2n operand; returns 0 for illegal arguments).
+ * Returns as bsofi_device_invert; the info word is at bsofi_device_info(dwork). */
+#define BSOFI_MIXED_SLICES 8
+unsigned long long bsofi_device_workspace_bytes_mixed(int n, int L, int ldda, int slices);
+int bsofi_device_invert_mixed(int n, int L, double *dA, int ldda, double *dtau, void *dwork,
+                              int slices, void *stream);
 /* Kernels launched by the last bsofi_device_* call on this thread. */
 long long bsofi_device_last_launches(void);
 
@@ -231,6 +250,14 @@ unsigned long long bsofi_batch_workspace_bytes(int count, const int *n, const in
 int bsofi_device_invert_batched(int count, const int *n, const int *L, double *const *dA,
                                 const int *ldda, double *const *dtau, void *dwork, int streams,
                                 void *stream);
+/* The same batch at a chosen precision: 0 FP64 (as above), 1 mixed (every
+ * instance as bsofi_device_invert_mixed with BSOFI_MIXED_SLICES slices).  The
+ * workspace query returns 0 for an unknown precision. */
+unsigned long long bsofi_batch_workspace_bytes_ex(int count, const int *n, const int *L,
+                                                  const int *ldda, int precision);
+int bsofi_device_invert_batched_ex(int count, const int *n, const int *L, double *const *dA,
+                                   const int *ldda, double *const *dtau, void *dwork, int streams,
+                                   int precision, void *stream);
 
 /* The same batch captured once into a CUDA graph and replayed (no reference
  * counterpart).  A Monte Carlo sweep re-inverts the same walkers' buffers
@@ -286,13 +313,32 @@ void bsofi_plan_clear(void);
  * ids and statuses: 0, info > 0 for an exactly singular R, or
  * BSOFI_INFO_CUDA - cudaError_t) and admits queued ones; it never blocks.
  * submit returns the request id (>= 0) or -1 bad server, -2 illegal size,
- * -3 unsupported precision (only 0 = FP64), -4 workspace larger than the
- * pool, -5 out of host memory.  One host thread per server. */
+ * -3 unsupported precision (0 = FP64, 1 = mixed as bsofi_device_invert_mixed
+ * with BSOFI_MIXED_SLICES slices), -4 workspace larger than the pool, -5 out
+ * of host memory.  One host thread per server. */
 typedef struct bsofi_server bsofi_server;
 bsofi_server *bsofi_server_create(int slots, unsigned long long pool_bytes);
 unsigned long long bsofi_server_request_bytes(int n, int L, int ldda);
 long long bsofi_server_submit(bsofi_server *server, int n, int L, double *dA, int ldda,
                               double *dtau, int precision);
+/* Server-owned requests.  The request is given by its packed p-cyclic blocks
+ * in device memory (dD: L diagonal blocks or NULL for identity blocks, dS: L
+ * coupling blocks, as bsofi_device_assemble takes them; both must stay valid
+ * until the request completes).  At admission the pool supplies the matrix
+ * (leading dimension n*L rounded up to 32), tau and the workspace together,
+ * bsofi_server_footprint_bytes(n, L, precision) bytes in all: admission is by
+ * the request's full memory footprint.  After the request completes, the
+ * workspace returns to the pool and bsofi_server_result gives the device
+ * addresses of M^{-1} and tau (0, or -1 for an unknown or released id);
+ * they stay resident, and count against the pool, until
+ * bsofi_server_release (0 or -1).  submit_blocks returns the id or the
+ * submit error codes above (-4: the footprint exceeds the pool). */
+unsigned long long bsofi_server_footprint_bytes(int n, int L, int precision);
+long long bsofi_server_submit_blocks(bsofi_server *server, int n, int L, const double *dD,
+                                     const double *dS, int precision);
+int bsofi_server_result(bsofi_server *server, long long id, double **dA, int *ldda,
+                        double **dtau);
+int bsofi_server_release(bsofi_server *server, long long id);
 int bsofi_server_poll(bsofi_server *server, long long *done_ids, int *done_status, int max);
 int bsofi_server_pending(bsofi_server *server);
 void bsofi_server_destroy(bsofi_server *server);
@@ -379,6 +425,17 @@ void bsofi_device_set_wait_test(int on);
 int bsofi_selftest_gemm(int M, int N, int K, double alpha, const double *dA, int lda,
                         int upper_a, const double *dB, int ldb, int upper_b, double beta,
                         double *dC, int ldc, int tile, void *stream);
+
+/* Diagnostic entry point (no reference counterpart): one product C = A B
+ * (column-major, M x K times K x N, K <= 1536) on the int8 tensor cores by the
+ * Ozaki scheme with `slices` slices (0 = 8), as the mixed-precision BSOI
+ * computes each step.  dscratch: device memory of
+ * bsofi_selftest_ozaki_scratch_bytes (256-byte aligned); derr: a device int
+ * set to 1 if a bounded wait inside the kernel gave up.  Enqueued on
+ * `stream`; returns 0, -1 for an illegal argument or BSOFI_INFO_CUDA - error. */
+unsigned long long bsofi_selftest_ozaki_scratch_bytes(int M, int N, int K, int slices);
+int bsofi_selftest_ozaki(int M, int N, int K, const double *dA, int lda, const double *dB, int ldb,
+                         double *dC, int ldc, int slices, void *dscratch, int *derr, void *stream);
 
 #ifdef __cplusplus
 }

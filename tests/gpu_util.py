@@ -68,3 +68,18 @@ def block_residual_colmajor(torch, diag, sub, T, N):
         Y[r * n:(r + 1) * n, :] -= eye
         acc += float((Y * Y).sum())
     return (acc ** 0.5) / float(torch.linalg.norm(Xt))
+
+
+class _DevBuf:
+    """__cuda_array_interface__ of raw device memory (no copy)."""
+
+    def __init__(self, ptr, shape):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f8",
+                                         "data": (int(ptr), False), "version": 3,
+                                         "strides": None}
+
+
+def device_view(torch, ptr, ncols, ld, device="cuda:0"):
+    """A float64 torch view (ncols, ld) of column-major device memory at ptr,
+    laid out as to_device_colmajor lays out its buffers."""
+    return torch.as_tensor(_DevBuf(ptr, (ncols, ld)), device=device)

@@ -16,8 +16,8 @@
 
 Tolerances as in test_gpu_parity: inverse forward error <= 8 sqrt(N) kappa_F
 eps, residual <= 1e-13, reflectors within 1e-10, determinant sign exact; tau
-within 1e-10 absolute at C4 (rounding differences of the first panels are
-carried through 63 panels of U = 6).
+within 1e-11 absolute (the oracle's plain-C restatement and the reference
+differ by up to 5e-13 in tau at n = 400, p = 64, U = 6).
 """
 import numpy as np
 import pytest
@@ -62,7 +62,7 @@ def test_c4_n400_p64_U6_vs_reference(cuda_device):
     # Handle API: the state between the two calls and the inverse.
     X, state, tau, info = api.invert(M, n, L)
     assert info == 0
-    np.testing.assert_allclose(tau, taur, rtol=0, atol=1e-10)
+    np.testing.assert_allclose(tau, taur, rtol=0, atol=1e-11)
     up, refl = split_state(state, n, L)
     rup, rrefl = split_state(Ar, n, L)
     assert rel_fro(up, rup) < tol
