@@ -65,9 +65,12 @@ def parse():
                    help="timed mixed-precision inversions at the headline size (0 = skip)")
     p.add_argument("--c4-steps", type=int, default=4,
                    help="timed inversions at n=400, p=64, U=6 for the c4 key (0 = skip)")
-    p.add_argument("--serve", type=int, default=60,
-                   help="requests in the served Poisson stream (0 = skip)")
-    p.add_argument("--serve-rate", type=float, default=12.0, help="mean arrivals per second")
+    p.add_argument("--serve", type=int, default=1000,
+                   help="requests in the served Poisson stream (0 = skip; 10000 = the full "
+                        "serving configuration)")
+    p.add_argument("--serve-rate", type=float, default=16.0, help="mean arrivals per second")
+    p.add_argument("--serve-mixed", type=float, default=0.5,
+                   help="fraction of served requests at mixed precision")
     return p.parse_args()
 
 
@@ -407,7 +410,8 @@ def main():
 
     served = None
     if args.serve > 0:
-        served = run_serving(api, torch, dev, args.serve, args.serve_rate, 31 + rank)
+        served = run_serving(api, torch, dev, args.serve, args.serve_rate, 31 + rank,
+                             args.serve_mixed if args.mixed_steps > 0 else 0.0)
 
     e2e = e2e_pageable = e2e_fp32 = None
     if not args.no_e2e and args.e2e_steps > 0:
@@ -665,59 +669,83 @@ def run_batched(api, torch, dev, specs, steps, stream, precision=0):
     return out
 
 
-def run_serving(api, torch, dev, nreq, rate, seed):
+def run_serving(api, torch, dev, nreq, rate, seed, mixed_frac=0.5):
     """A Poisson stream of inversion requests through the continuous-batching
-    server (bsofi_server_*).  Sizes follow the serving configuration (lattice
-    side uniform in 8..24, so n = 64..576; p uniform in 10..80; U in 2..6);
-    every request's matrix is built in HBM at its arrival and stays there.
-    Latency is wall clock from submission to the poll that sees it finish."""
+    server (bsofi_server_*), server-owned: each request is submitted as its
+    packed coupling blocks (built on the device at its arrival), and the
+    server's pool supplies matrix, tau and workspace at admission (admission
+    by full memory footprint, up to 17 GB at n = 576, p = 80).  Sizes follow
+    the serving configuration (lattice side uniform in 8..24, so n = 64..576;
+    p uniform in 10..80; U in 2..6); a fraction mixed_frac of the requests
+    runs mixed precision (BSOI on the int8 tensor cores).  Latency is wall
+    clock from submission to the poll that sees the request finish; the
+    result is then released."""
     from bsofi_b200 import replicas
+    from bsofi_b200.hubbard import expm_sym, lattice_adjacency
     rng = np.random.default_rng(seed)
     specs = [(int(rng.integers(8, 25)), int(rng.integers(10, 81)), float(rng.uniform(2, 6)),
-              70000 + 97 * seed + i) for i in range(nreq)]
+              int(rng.random() < mixed_frac)) for _ in range(nreq)]
     arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
-    blocks = [hubbard_pcyclic(sd, L, U, sdd) for sd, L, U, sdd in specs]
+    expk = {}
     flops = sum(bsofi_flops(sd * sd, L) for sd, L, _, _ in specs)
-    srv = api.Server(slots=8, pool_bytes=24 << 30)
-    submit_t, lat, bufs = {}, [], {}
+    free, _ = torch.cuda.mem_get_info(dev)
+    pool = int(min(free - (12 << 30), 140 << 30))
+    srv = api.Server(slots=8, pool_bytes=pool)
+    submit_t, lat, keep, prec_of = {}, [], {}, {}
     nxt, done = 0, 0
     replicas.barrier()
     t0 = time.perf_counter()
     while done < nreq:
         now = time.perf_counter() - t0
         while nxt < nreq and arrivals[nxt] <= now:
-            sd, L, U, _ = specs[nxt]
+            sd, L, U, prec = specs[nxt]
             n = sd * sd
-            N = n * L
-            ld = (N + 31) // 32 * 32
-            A = pcyclic_device(torch, *blocks[nxt], ld, dev)
-            tau = torch.zeros(N, dtype=torch.float64, device=dev)
-            torch.cuda.current_stream().synchronize()  # the matrix is in HBM before submission
-            rid = srv.submit(n, L, A.data_ptr(), ld, tau.data_ptr())
+            if sd not in expk:
+                expk[sd] = torch.from_numpy(expm_sym(0.125 * lattice_adjacency(sd))).to(dev)
+            lam = float(np.arccosh(np.exp(U * 0.125 / 2.0)))
+            h = torch.from_numpy(rng.choice(np.array([-1.0, 1.0]), size=(L, n))).to(dev)
+            # Packed column-major blocks: block k is B_{k+1} = expK diag(exp(lam h_k)),
+            # negated below the diagonal, +B_p in the corner.
+            S = expk[sd][None, :, :] * torch.exp(lam * h)[:, :, None]
+            S[:L - 1] *= -1.0
+            torch.cuda.current_stream().synchronize()  # blocks in HBM before submission
+            rid = srv.submit_blocks(n, L, S.data_ptr(), precision=prec)
             submit_t[rid] = time.perf_counter() - t0
-            bufs[rid] = (A, tau)
+            keep[rid] = S
+            prec_of[rid] = prec
             nxt += 1
         for rid, st in srv.poll():
             if st != 0:
                 raise RuntimeError("served request %d failed: %d" % (rid, st))
-            lat.append(time.perf_counter() - t0 - submit_t[rid])
-            del bufs[rid]
+            lat.append((time.perf_counter() - t0 - submit_t[rid], prec_of[rid]))
+            srv.release(rid)
+            del keep[rid]
             done += 1
         time.sleep(0.0002)
     t_end = time.perf_counter() - t0
     srv.close()
     torch.cuda.empty_cache()
-    lat = np.array(lat) * 1e3
+    ms = np.array([x for x, _ in lat]) * 1e3
+    pr = np.array([p for _, p in lat])
     span = t_end - arrivals[0]
+
+    def pct(a, q):
+        return float(np.percentile(a, q)) if len(a) else None
+
     return {"requests": nreq, "arrival_rate_per_s": rate,
             "value": nreq / span, "unit": "inversions/s",
             "tflops": flops / span / 1e12,
-            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-            "max_ms": float(lat.max()), "precision_mix": "all FP64",
+            "p50_ms": pct(ms, 50), "p99_ms": pct(ms, 99), "max_ms": float(ms.max()),
+            "p50_ms_fp64": pct(ms[pr == 0], 50), "p99_ms_fp64": pct(ms[pr == 0], 99),
+            "p50_ms_mixed": pct(ms[pr == 1], 50), "p99_ms_mixed": pct(ms[pr == 1], 99),
+            "requests_mixed": int(pr.sum()), "precision_mix": "%d%% mixed (BSOI on the int8 "
+            "tensor cores), the rest FP64" % round(100 * mixed_frac),
+            "pool_gib": pool / 2 ** 30,
             "workload": "Poisson stream, lattice side uniform in 8..24 (n = 64..576), p uniform "
-                        "in 10..80, U uniform in 2..6; %d requests (a bounded sample of the "
-                        "10,000-request serving configuration), 8 slots, 24 GiB workspace pool"
-                        % nreq}
+                        "in 10..80, U uniform in 2..6; %d requests%s, 8 slots, server-owned "
+                        "memory (matrix + tau + workspace per request from one pool)"
+                        % (nreq, "" if nreq >= 10000 else
+                           " (a sample of the 10,000-request serving configuration)")}
 
 
 def run_e2e(api, torch, dist, world, side, L, U, rank, steps, pinned=True):
