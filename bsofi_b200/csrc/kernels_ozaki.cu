@@ -97,9 +97,14 @@ __global__ void __launch_bounds__(128) ozaki_split_kernel(OzSplitArgs s) {
     const int i = blockIdx.x * 128 + threadIdx.x;
     if (i >= s.M) return;
     double mx = 0.0;
-    for (int k = 0; k < s.K; k++) mx = fmax(mx, fabs(oz_a(s, i, k)));
+    bool bad = false;  // fmax drops NaN, so non-finite values are tracked apart
+    for (int k = 0; k < s.K; k++) {
+      const double v = oz_a(s, i, k);
+      bad |= !isfinite(v);
+      mx = fmax(mx, fabs(v));
+    }
     int e = 0;
-    if (!isfinite(mx)) {
+    if (bad) {
       s.a_exp[i] = OZ_EXP_NONFINITE;
       mx = 0.0;
     } else {
@@ -124,11 +129,16 @@ __global__ void __launch_bounds__(128) ozaki_split_kernel(OzSplitArgs s) {
   if (j >= s.N) return;
   const double* col = s.b + (long long)j * s.ldb;
   double mx = 0.0;
-  for (int k = lane; k < s.K; k += 32) mx = fmax(mx, fabs(col[k]));
+  bool bad = false;  // fmax drops NaN, so non-finite values are tracked apart
+  for (int k = lane; k < s.K; k += 32) {
+    bad |= !isfinite(col[k]);
+    mx = fmax(mx, fabs(col[k]));
+  }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  bad = __any_sync(0xffffffffu, bad);
   int e = 0;
-  if (!isfinite(mx)) {
+  if (bad) {
     if (lane == 0) s.b_exp[j] = OZ_EXP_NONFINITE;
     mx = 0.0;
   } else {

@@ -2,6 +2,7 @@
 
     python -m bsofi_b200.diag bsof-timeline N_BLOCK L [REPS] [--cholqr=0|1]
     python -m bsofi_b200.diag invert N_BLOCK L [REPS] [U] [--cholqr=0|1]
+    python -m bsofi_b200.diag invert-mixed N_BLOCK L [REPS] [SLICES]
 
 bsof-timeline inverts a seeded Hubbard matrix (a random p-cyclic one when n is
 not a square) with bsofi_device_invert and prints, for the last run, the BSOF
@@ -112,6 +113,47 @@ def invert_timing(n, L, reps=3, U=4.0):
             "plan": api.plan_get(n, L)}
 
 
+def invert_mixed_timing(n, L, reps=3, U=4.0, slices=0):
+    """Device-resident inversions with BSOI's products on the int8 tensor cores
+    (bsofi_device_invert_mixed); fastest of reps, the BSOI products' time
+    (split + product launches, CUDA events) and the residual."""
+    import torch
+    from .flops import bsofi_flops, flops_bsoi
+    side = int(round(n ** 0.5))
+    N = n * L
+    ldd = (N + 31) // 32 * 32
+    M = hubbard_matrix(side, L, U, seed=1) if side * side == n else random_pcyclic(n, L, seed=1)
+    dev = torch.device("cuda:0")
+    src = torch.zeros((N, ldd), dtype=torch.float64, device=dev)
+    src[:, :N] = torch.from_numpy(np.ascontiguousarray(M.T)).to(dev)
+    dA = torch.empty_like(src)
+    dtau = torch.zeros(N, dtype=torch.float64, device=dev)
+    ws = torch.empty(api.mixed_workspace_bytes(n, L, ldd, slices), dtype=torch.uint8, device=dev)
+    best, bsoi = float("inf"), float("inf")
+    stream = torch.cuda.current_stream()
+    for r in range(reps + 1):
+        dA.copy_(src)
+        api.timing(True)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rc = api.device_invert_mixed(n, L, dA.data_ptr(), ldd, dtau.data_ptr(), ws.data_ptr(),
+                                     slices, stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms, _ = api.timing_read()
+        api.timing(False)
+        if rc != 0:
+            raise RuntimeError("bsofi_device_invert_mixed failed (%d)" % rc)
+        if r > 0:
+            best = min(best, e0.elapsed_time(e1))
+            bsoi = min(bsoi, ms)
+    X = dA[:, :N].T.cpu().numpy()
+    res = np.linalg.norm(M @ X - np.eye(N)) / np.linalg.norm(X) if N <= 12000 else None
+    return {"invert_ms": best, "tflops": bsofi_flops(n, L) / best / 1e9, "bsoi_ms": bsoi,
+            "bsoi_tflops": flops_bsoi(n, L) / bsoi / 1e9, "residual": res}
+
+
 def main(argv):
     # --cholqr=0 times the column-by-column leaf factorization of the BSOF
     # chain instead of CholeskyQR2 with Householder reconstruction.
@@ -137,6 +179,16 @@ def main(argv):
         print("n %d L %d (plan %s): invert %.3f ms = %.2f TFLOP/s of the flop model; BSOI %.3f ms "
               "= %.2f TFLOP/s; BSOF chain %.3f ms" % (n, L, r["plan"], r["invert_ms"], r["tflops"],
                                                       r["bsoi_ms"], r["bsoi_tflops"], r["chain_ms"]))
+        return 0
+    if len(argv) >= 3 and argv[0] == "invert-mixed":
+        n, L = int(argv[1]), int(argv[2])
+        reps = int(argv[3]) if len(argv) > 3 else 3
+        slices = int(argv[4]) if len(argv) > 4 else 0
+        r = invert_mixed_timing(n, L, reps, 4.0, slices)
+        print("n %d L %d mixed (slices %s): invert %.3f ms = %.2f TFLOP/s of the flop model; "
+              "BSOI products %.3f ms = %.2f TFLOP/s effective FP64; residual %s"
+              % (n, L, slices or 8, r["invert_ms"], r["tflops"], r["bsoi_ms"], r["bsoi_tflops"],
+                 r["residual"]))
         return 0
     print(__doc__)
     return 2
