@@ -58,8 +58,8 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--batch", type=int, default=16,
                    help="instances of the headline size per batched step (0 = skip)")
-    p.add_argument("--batch-mixed", type=int, default=64,
-                   help="instances in the mixed-size batched sample (0 = skip)")
+    p.add_argument("--batch-mixed", type=int, default=256,
+                   help="instances of the mixed-size batched configuration (0 = skip)")
     p.add_argument("--batch-steps", type=int, default=3)
     p.add_argument("--mixed-steps", type=int, default=10,
                    help="timed mixed-precision inversions at the headline size (0 = skip)")
@@ -396,17 +396,23 @@ def main():
                                   "scheme, 8 slices)" % (args.batch, side, side, n, L))
         if batched and batched.get("value"):
             batched_mp["ratio_to_fp64_batched"] = batched_mp["value"] / batched["value"]
-    batched_mixed = None
+    batched_mixed = batched_mixed_mp = None
     if args.batch_mixed > 0:
         rng = np.random.default_rng(77 + rank)
         specs = [(int(rng.choice([8, 10, 12, 14, 16])), int(rng.integers(8, 65)),
                   float(rng.uniform(2.0, 6.0)), 9000 + 1000 * rank + i)
                  for i in range(args.batch_mixed)]
-        batched_mixed = run_batched(api, torch, dev, specs, args.batch_steps, stream)
-        batched_mixed["workload"] = ("%d independent FP64 inversions per step, lattice side in "
-                                     "{8,10,12,14,16}, p uniform in [8,64], U uniform in [2,6] "
-                                     "(a sample of the 256-walker batched configuration)"
-                                     % args.batch_mixed)
+        wl = ("%d independent inversions per step, lattice side in {8,10,12,14,16}, p uniform "
+              "in [8,64], U uniform in [2,6]%s" % (args.batch_mixed, " (the batched configuration)"
+                                                   if args.batch_mixed >= 256 else ""))
+        batched_mixed = run_batched_packed(api, torch, dev, specs, args.batch_steps, stream)
+        batched_mixed["workload"] = wl
+        if args.mixed_steps > 0:
+            batched_mixed_mp = run_batched_packed(api, torch, dev, specs, args.batch_steps, stream,
+                                                  precision=1)
+            batched_mixed_mp["workload"] = wl
+            batched_mixed_mp["ratio_to_fp64_batched"] = (batched_mixed_mp["value"] /
+                                                         batched_mixed["value"])
 
     served = None
     if args.serve > 0:
@@ -444,6 +450,7 @@ def main():
                 "e2e_fp32": e2e_fp32,
                 "batched": batched, "batched_mixed_sizes": batched_mixed, "served": served,
                 "mixed": mixed, "batched_mixed_precision": batched_mp,
+                "batched_mixed_sizes_mixed_precision": batched_mixed_mp,
                 "gpu_launches": launches_per_step * args.steps,
                 "clocks": clk}
         print(json.dumps(line))
@@ -561,6 +568,73 @@ def run_mixed_single(api, torch, dev, stream, side, L, U, steps, warmup, rank, f
             "bsoi_effective_fp64_tflops": flops_bsoi(n, L) / (bsoi_ms / steps * 1e-3) / 1e12
             if bsoi_ms > 0 else None,
             "bsoi_timed_launches": bsoi_launches}
+
+
+def run_batched_packed(api, torch, dev, specs, steps, stream, precision=0):
+    """The batched configuration at its full size: every instance keeps only
+    its packed coupling blocks on the device, and before each timed batch the
+    inputs are re-assembled into the instances' matrices with
+    bsofi_device_assemble (outside the timed window), so no second copy of
+    the matrices is held.  Rate = instances / summed batch time (CUDA events,
+    max over ranks)."""
+    from bsofi_b200 import replicas
+    ns, Ls, lds, bufs, packs = [], [], [], [], []
+    flops = 0.0
+    for side, L, U, seed in specs:
+        n = side * side
+        N = n * L
+        ld = (N + 31) // 32 * 32
+        _, sub = hubbard_pcyclic(side, L, U, seed)
+        packs.append(torch.from_numpy(np.ascontiguousarray(np.transpose(sub, (0, 2, 1))))
+                     .to(dev))
+        bufs.append(torch.empty((N, ld), dtype=torch.float64, device=dev))
+        ns.append(n)
+        Ls.append(L)
+        lds.append(ld)
+        flops += bsofi_flops(n, L)
+    taus = [torch.zeros(n * L, dtype=torch.float64, device=dev) for n, L in zip(ns, Ls)]
+    ws = torch.zeros(api.batch_workspace_bytes(ns, Ls, lds, precision) // 8 + 1,
+                     dtype=torch.float64, device=dev)
+    sp = stream.cuda_stream
+    total_ms = 0.0
+    for it in range(steps + 1):  # the first batch is a warm-up
+        for n, L, b, pk, ld in zip(ns, Ls, bufs, packs, lds):
+            if api.device_assemble(n, L, 0, pk.data_ptr(), b.data_ptr(), ld) != 0:
+                raise RuntimeError("bsofi_device_assemble failed")
+        torch.cuda.synchronize()
+        replicas.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            rc = api.device_invert_batched(ns, Ls, [b.data_ptr() for b in bufs], lds,
+                                           [t.data_ptr() for t in taus], ws.data_ptr(), 8, sp,
+                                           precision)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        if rc != 0:
+            raise RuntimeError("bsofi_device_invert_batched_ex failed: %d" % rc)
+        if it > 0:
+            total_ms += e0.elapsed_time(e1)
+    launches = api.last_launches()
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from gpu_util import block_residual_colmajor
+    worst = 0.0
+    for i in range(0, len(specs), max(1, len(specs) // 8)):  # 8 instances checked
+        side, L, U, seed = specs[i]
+        worst = max(worst, block_residual_colmajor(torch, *hubbard_pcyclic(side, L, U, seed),
+                                                   bufs[i], ns[i] * Ls[i]))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    ms_max = replicas.max_over_ranks(total_ms, dev)
+    out = {"value": world * len(specs) * steps / (ms_max * 1e-3), "unit": "inversions/s",
+           "steps": steps, "ms_per_step": ms_max / steps,
+           "tflops": flops * steps * world / (ms_max * 1e-3) / 1e12,
+           "instances_per_step": len(specs), "worst_residual_of_8_checked": worst,
+           "gpu_launches_per_step": launches, "precision": "FP64" if precision == 0 else
+           "mixed (BSOI on the int8 tensor cores, 8 slices)"}
+    del bufs, packs, ws, taus
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_batched(api, torch, dev, specs, steps, stream, precision=0):

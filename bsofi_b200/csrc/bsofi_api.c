@@ -1112,6 +1112,4 @@ void bsofi_device_set_bsof_workers(int workers) { bsofi_dev_set_bsof_workers(wor
 
 void bsofi_device_set_bstri_overlap(int on) { bsofi_dev_set_bstri_overlap(on); }
 
-void bsofi_device_set_bsof_cholqr(int on) { bsofi_dev_set_bsof_cholqr(on); }
-
 void bsofi_device_set_wait_test(int on) { bsofi_dev_set_wait_test(on); }

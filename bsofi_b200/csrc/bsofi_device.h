@@ -135,9 +135,6 @@ int bsofi_dev_timing_read(double *ms, long long *launches);
  * number of leaves. */
 int bsofi_dev_bsof_timeline(int n, int L, int ldd, void *dws, unsigned long long **ptr);
 void bsofi_dev_set_bsof_workers(int w);
-/* Leaf factorization of the BSOF chain: CholeskyQR2 + Householder
- * reconstruction (1, default) or column by column (0); process-wide. */
-void bsofi_dev_set_bsof_cholqr(int on);
 /* Diagnostics: persistent BSOI launches of this thread poll a word that
  * nothing writes in every step wait (short limit), so the waits give up. */
 void bsofi_dev_set_wait_test(int on);

@@ -48,8 +48,6 @@ cudaError_t launch_wy_apply(const WyArgs& a, int batch, cudaStream_t st);
 // a later launch continues with the counters the earlier one left, after
 // next_task is zeroed again.
 int bsof_leaf_width(int n);
-int bsof_cholqr_enabled();
-void bsof_set_cholqr(int on);
 int bsof_tiles(int n);
 cudaError_t launch_bsof_persistent(double* A, long long ld, int n, int L, double* tau, double* T,
                                    double* G, int maxleaves, int* cnt, int* factored,

@@ -23,7 +23,6 @@
 // only on tasks earlier in that order and all CTAs are co-resident
 // (cooperative launch), so the schedule cannot deadlock; every spin is
 // bounded and sets an error word instead of hanging.
-#include <atomic>
 #include <climits>
 #include "bsofi_common.cuh"
 #include "bsofi_kernels.h"
@@ -36,7 +35,6 @@ constexpr int BW = BT / 32;
 struct BsofGeom {
   int n, L, NB, nl, S;
   int form_g;  // 1: leaves also update G_k = Q_k^T (identity-initialised by the caller)
-  int cqr;     // 1: full-width leaves by CholeskyQR2 + Householder reconstruction
 };
 
 // Leaf s -> panel k, leaf index l in the panel, tile (m, t), panel column j0.
@@ -257,22 +255,9 @@ struct Smem {
   double T[NB][NB + 1];
   double redW[BW][NB][NB + 1];
   double W[NB][NB + 1];
-  // CholeskyQR2 leaf factorization (factor_leaf_cqr): Gram matrix, R1, R2, a
-  // triangular inverse, the LU of Q_top - S, the leaf's top rows, the final
-  // multiplier, reciprocal diagonals and the signs S.
-  double G[NB][NB + 1];
-  double R1[NB][NB + 1];
-  double R2[NB][NB + 1];
-  double Mi[NB][NB + 1];
-  double LU[NB][NB + 1];
-  double Rf[NB][NB + 1];
-  double Mf[NB][NB + 1];
-  double dv[NB];
-  double sgn[NB];
   int flag;
   int task;
   int pflag;  // next-tile prefetch of the panel CTA succeeded
-  int cqr_ok;
 };
 
 // T(0:I, I) = -tau_I T(0:I,0:I) g_I (LAPACK dlarft), run by one warp one
@@ -418,310 +403,6 @@ BSOFI_DEVINL void factor_leaf(double (&a)[R][NB], Smem<NB>& sm, int m, int w, do
       a[i][NB - 1] = t0;
     }
   }
-}
-
-// ------------------------------------------------ CholeskyQR2 leaf factorization
-// Householder QR of a full-width leaf by CholeskyQR2 and Householder
-// reconstruction (Ballard, Demmel, Grigori, Jacquelin, Knight, Nguyen,
-// "Reconstructing Householder vectors from tall-skinny QR", JPDC 2015):
-//   R1 = chol(A^T A), Q1 = A R1^-1, R2 = chol(Q1^T Q1), Q = Q1 R2^-1;
-//   LU without pivoting of Q - [S; 0] with S_jj = -sign of the j-th pivot
-//   before the shift, so |pivot| = 1 + |.| >= 1: L = Y (the reflectors, unit
-//   diagonal), U;  T = -U S Y1^-T (the dlarft factor, tau = diag T = 1 + |.|),
-//   R = S R2 R1.
-// S reproduces dlarfg's sign choice (beta = -sign(alpha) ||(alpha, x)||, the
-// pivot's sign being alpha's), so in exact arithmetic Y, tau, T and R are the
-// Householder QR's.  The serial part is a handful of 16 x 16 (8 x 8)
-// factorizations in one warp; the rest is two Gram matrices (DMMA) and two
-// row-wise triangular products, instead of one block reduction per column.
-
-// Barrier of the factor threads (all CTA threads when FW == BW).
-template <int FW>
-BSOFI_DEVINL void factor_bar() {
-  if constexpr (FW == BW) __syncthreads();
-  else named_bar(FW * 32);
-}
-
-// sm.G = A^T A for the staged leaf sA (column-major, column stride SA, `rows`
-// rows, a multiple of 8 FW), DMMA with K split over the FW factor warps.
-template <int NB, int FW>
-BSOFI_DEVINL void leaf_gram(const double* sA, int SA, int rows, Smem<NB>& sm) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int g = lane >> 2, t = lane & 3;
-  const int KW = rows / FW, k1 = warp * KW;
-  if constexpr (NB == 16) {
-    double acc[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
-#pragma unroll 4
-    for (int k0 = k1; k0 < k1 + KW; k0 += 8) {
-      const double a0 = sA[g * SA + k0 + t], a1 = sA[(g + 8) * SA + k0 + t];
-      const double a2 = sA[g * SA + k0 + t + 4], a3 = sA[(g + 8) * SA + k0 + t + 4];
-      dmma_16x8x8(acc[0], a0, a1, a2, a3, a0, a2);  // columns 0..7
-      dmma_16x8x8(acc[1], a0, a1, a2, a3, a1, a3);  // columns 8..15
-    }
-#pragma unroll
-    for (int j = 0; j < 2; j++) {
-      sm.redW[warp][g][8 * j + 2 * t] = acc[j][0];
-      sm.redW[warp][g][8 * j + 2 * t + 1] = acc[j][1];
-      sm.redW[warp][g + 8][8 * j + 2 * t] = acc[j][2];
-      sm.redW[warp][g + 8][8 * j + 2 * t + 1] = acc[j][3];
-    }
-  } else {
-    double acc[2] = {0.0, 0.0};
-#pragma unroll 4
-    for (int k0 = k1; k0 < k1 + KW; k0 += 4) {
-      const double a0 = sA[g * SA + k0 + t];
-      dmma_8x8x4(acc, a0, a0);
-    }
-    sm.redW[warp][g][2 * t] = acc[0];
-    sm.redW[warp][g][2 * t + 1] = acc[1];
-  }
-  factor_bar<FW>();
-  for (int e = tid; e < NB * NB; e += FW * 32) {
-    const int i = e % NB, c = e / NB;
-    double s2 = 0.0;
-#pragma unroll
-    for (int w = 0; w < FW; w++) s2 += sm.redW[w][i][c];
-    sm.G[i][c] = s2;
-  }
-  factor_bar<FW>();
-}
-
-// Warp-wide Cholesky of sm.G: lane c < NB writes column c of R (R(j, c), zero
-// for j > c) to Rout and 1 / R(c, c) to sm.dv.  False when a pivot is not
-// above tol.
-template <int NB>
-BSOFI_DEVINL bool warp_chol(Smem<NB>& sm, double (&Rout)[NB][NB + 1], int lane, double tol) {
-  double col[NB];
-#pragma unroll
-  for (int i = 0; i < NB; i++) col[i] = lane < NB ? sm.G[i][lane] : 0.0;
-  bool ok = true;
-#pragma unroll
-  for (int j = 0; j < NB; j++) {
-    const double gjj = __shfl_sync(0xffffffffu, col[j], j);
-    ok = ok && gjj > tol;
-    const double rs = rsqrt(gjj);
-    const double rjc = col[j] * rs;
-    if (lane < NB) Rout[j][lane] = lane >= j ? rjc : 0.0;
-    if (lane == j) sm.dv[j] = 1.0 / rjc;
-#pragma unroll
-    for (int i = j + 1; i < NB; i++)
-      col[i] = fma(-__shfl_sync(0xffffffffu, rjc, i), rjc, col[i]);
-  }
-  __syncwarp();
-  return ok;
-}
-
-// Column `lane` of the inverse of the upper triangular M (dinv = 1 / diag).
-template <int NB>
-BSOFI_DEVINL void warp_triinv_col(const double (&M)[NB][NB + 1], const double* dinv,
-                                  double (&x)[NB], int lane) {
-#pragma unroll
-  for (int j = NB - 1; j >= 0; j--) {
-    double s2 = 0.0;
-#pragma unroll
-    for (int k = j + 1; k < NB; k++) s2 = fma(M[j][k], x[k], s2);
-    x[j] = j > lane ? 0.0 : (j == lane ? dinv[j] : -s2 * dinv[j]);
-  }
-}
-
-// Warp 0 after the first Gram matrix: R1 = chol(G), sm.Mi = R1^-1.
-template <int NB>
-__device__ __noinline__ bool cqr_first(Smem<NB>& sm, int lane) {
-  double dmax = lane < NB ? sm.G[lane][lane] : 0.0;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
-  const bool ok = warp_chol<NB>(sm, sm.R1, lane, 1e-12 * dmax) && dmax > 0.0;
-  double x[NB];
-  warp_triinv_col<NB>(sm.R1, sm.dv, x, lane);
-  if (lane < NB) {
-#pragma unroll
-    for (int j = 0; j < NB; j++) sm.Mi[j][lane] = x[j];
-  }
-  __syncwarp();
-  return ok;
-}
-
-// Warp 0 after the second Gram matrix (sQ: the staged Q1): R2, the
-// reconstruction, and everything the rows need: sm.T, sm.Rf (the leaf's top
-// NB rows), sm.Mf = R2^-1 U^-1 (Y_rest = Q1_rest Mf), tau.
-template <int NB>
-__device__ __noinline__ bool cqr_second(Smem<NB>& sm, const double* sQ, int SA, int lane, double* tau_out) {
-  // Q1 is orthonormal to about kappa^2 eps, so the pivots of R2 are near 1.
-  const bool ok = warp_chol<NB>(sm, sm.R2, lane, 0.25);
-  {
-    double x[NB];
-    warp_triinv_col<NB>(sm.R2, sm.dv, x, lane);  // column lane of R2^-1
-    if (lane < NB) {
-#pragma unroll
-      for (int j = 0; j < NB; j++) sm.Mi[j][lane] = x[j];
-    }
-  }
-  // R = R2 R1 (column lane, unsigned for now).
-  if (lane < NB) {
-#pragma unroll
-    for (int i = 0; i < NB; i++) {
-      double s2 = 0.0;
-#pragma unroll
-      for (int k = i; k < NB; k++) s2 = fma(sm.R2[i][k], sm.R1[k][lane], s2);
-      sm.Rf[i][lane] = s2;
-    }
-  }
-  __syncwarp();
-  // Q_top = Q1(0:NB, :) R2^-1, column lane.
-  double qt[NB];
-#pragma unroll
-  for (int i = 0; i < NB; i++) {
-    double s2 = 0.0;
-#pragma unroll
-    for (int k = 0; k < NB; k++) s2 = fma(sQ[k * SA + i], lane < NB ? sm.Mi[k][lane] : 0.0, s2);
-    qt[i] = s2;
-  }
-  // LU of Q_top - S without pivoting; S_jj = -sign(pivot), +0 counting as
-  // positive (dlarfg's sign(1, +0) = +1).
-#pragma unroll
-  for (int j = 0; j < NB; j++) {
-    const double qjj = __shfl_sync(0xffffffffu, qt[j], j);
-    const double sj = qjj >= 0.0 ? -1.0 : 1.0;
-    if (lane == 0) sm.sgn[j] = sj;
-    if (lane == j) {
-      const double ujj = qjj - sj;
-      const double inv = 1.0 / ujj;
-#pragma unroll
-      for (int i = j + 1; i < NB; i++) qt[i] *= inv;
-      qt[j] = ujj;
-    }
-#pragma unroll
-    for (int i = j + 1; i < NB; i++) {
-      const double yij = __shfl_sync(0xffffffffu, qt[i], j);
-      if (lane > j) qt[i] = fma(-yij, qt[j], qt[i]);
-    }
-  }
-  // Column lane: U(i, lane) for i <= lane, Y(i, lane) below.
-  if (lane < NB) {
-#pragma unroll
-    for (int i = 0; i < NB; i++) sm.LU[i][lane] = qt[i];
-    sm.dv[lane] = 1.0 / qt[lane];
-  }
-  __syncwarp();
-  if (lane < NB) tau_out[lane] = -qt[lane] * sm.sgn[lane];
-  {
-    // z = Y1^-T e_lane (unit upper triangular solve), T(:, lane) = -U S z.
-    double z[NB];
-#pragma unroll
-    for (int j = NB - 1; j >= 0; j--) {
-      double s2 = 0.0;
-#pragma unroll
-      for (int k = j + 1; k < NB; k++) s2 = fma(sm.LU[k][j], z[k], s2);
-      z[j] = j > lane ? 0.0 : (j == lane ? 1.0 : -s2);
-    }
-    if (lane < NB) {
-#pragma unroll
-      for (int i = 0; i < NB; i++) {
-        double t2 = 0.0;
-#pragma unroll
-        for (int k = i; k < NB; k++) t2 = fma(sm.LU[i][k] * sm.sgn[k], z[k], t2);
-        sm.T[i][lane] = i <= lane ? -t2 : 0.0;
-      }
-    }
-  }
-  {
-    // U^-1 (column lane), then Mf = R2^-1 U^-1.
-    double x[NB];
-    warp_triinv_col<NB>(sm.LU, sm.dv, x, lane);
-    if (lane < NB) {
-#pragma unroll
-      for (int i = 0; i < NB; i++) {
-        double m2 = 0.0;
-#pragma unroll
-        for (int k = i; k < NB; k++) m2 = fma(sm.Mi[i][k], x[k], m2);
-        sm.Mf[i][lane] = m2;
-        sm.Rf[i][lane] = i <= lane ? sm.sgn[i] * sm.Rf[i][lane] : sm.LU[i][lane];
-      }
-    }
-  }
-  __syncwarp();
-  return ok;
-}
-
-// The thread's rows of the staged leaf back into registers.
-template <int FR, int NB, int FT>
-BSOFI_DEVINL void reload_rows(double (&a)[FR][NB], const double* sA, int SA) {
-#pragma unroll
-  for (int i = 0; i < FR; i++)
-#pragma unroll
-    for (int c = 0; c < NB; c++) a[i][c] = sA[c * SA + threadIdx.x + FT * i];
-}
-
-// a <- a M for the thread's FR rows, M upper triangular in shared memory:
-// each entry of M is read once and applied to every row; columns from the
-// last, so that column c only reads columns <= c of a.
-template <int FR, int NB>
-BSOFI_DEVINL void rows_times_upper(double (&a)[FR][NB], const double (&M)[NB][NB + 1]) {
-#pragma unroll
-  for (int c = NB - 1; c >= 0; c--) {
-    double s2[FR];
-#pragma unroll
-    for (int i = 0; i < FR; i++) s2[i] = 0.0;
-#pragma unroll
-    for (int j = 0; j <= c; j++) {
-      const double m = M[j][c];
-#pragma unroll
-      for (int i = 0; i < FR; i++) s2[i] = fma(a[i][j], m, s2[i]);
-    }
-#pragma unroll
-    for (int i = 0; i < FR; i++) a[i][c] = s2[i];
-  }
-}
-
-// Factor threads: thread t owns rows t + FT i of the leaf in a (rows >= m
-// zero); the leaf is full width (NB columns) with m >= NB rows.  sA: shared
-// staging of FR * FT rows with column stride SA.  On success a holds the
-// dgeqr2 layout (R on and above the diagonal, reflectors below), tau_out[0..NB)
-// and sm.T the dlarft factor; returns false (a, tau and sm.T then unusable)
-// when a Cholesky pivot is below 1e-12 of the largest squared column norm
-// (condition number above about 1e6).
-template <int FR, int NB, int FW>
-BSOFI_DEVINL bool factor_leaf_cqr(double (&a)[FR][NB], Smem<NB>& sm, double* sA, int SA,
-                                  double* tau_out) {
-  constexpr int FT = FW * 32, ROWS = FR * FT;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-#pragma unroll
-  for (int i = 0; i < FR; i++)
-#pragma unroll
-    for (int c = 0; c < NB; c++) sA[c * SA + tid + FT * i] = a[i][c];
-  factor_bar<FW>();
-  leaf_gram<NB, FW>(sA, SA, ROWS, sm);
-  if (warp == 0) {
-    const bool ok = cqr_first<NB>(sm, lane);
-    if (lane == 0) sm.cqr_ok = ok;
-  }
-  factor_bar<FW>();
-  if (!sm.cqr_ok) return false;
-  // The leaf is reloaded from its staged copy (not kept in registers across
-  // the serial sections), then Q1 = A R1^-1 in place.
-  reload_rows<FR, NB, FT>(a, sA, SA);
-  rows_times_upper<FR, NB>(a, sm.Mi);
-#pragma unroll
-  for (int i = 0; i < FR; i++)
-#pragma unroll
-    for (int c = 0; c < NB; c++) sA[c * SA + tid + FT * i] = a[i][c];
-  factor_bar<FW>();
-  leaf_gram<NB, FW>(sA, SA, ROWS, sm);
-  if (warp == 0) {
-    const bool ok = cqr_second<NB>(sm, sA, SA, lane, tau_out);
-    if (lane == 0) sm.cqr_ok = ok;
-  }
-  factor_bar<FW>();
-  if (!sm.cqr_ok) return false;
-  // The top NB rows are R (on and above the diagonal) and Y's top block; the
-  // others Y_rest = Q1_rest Mf (in place, columns from the last).
-  reload_rows<FR, NB, FT>(a, sA, SA);
-  rows_times_upper<FR, NB>(a, sm.Mf);
-  if (tid < NB) {  // row tid of slice 0
-#pragma unroll
-    for (int c = 0; c < NB; c++) a[0][c] = sm.Rf[tid][c];
-  }
-  return true;
 }
 
 // 16-wide block reflector applied with DMMA (mma.sync m16n8k4 f64):
@@ -1032,26 +713,7 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
           for (int c = 0; c < NB; c++)
             a[i][c] = (r < mrows && c < f.w) ? __ldcg(P + cm(r, c, st.ld)) : 0.0;
         }
-        double* tau_leaf = st.tau + (long long)f.k * g.n + f.j0;
-        constexpr int SA = NB == 16 ? Pass<R>::SV : Stage8<R>::S8;
-        const bool cqr = g.cqr && f.w == NB && mrows >= NB;
-        if (!cqr || !factor_leaf_cqr<FR, NB, FW>(a, sm, sC, SA, tau_leaf)) {
-          if (cqr) {
-            // Rank-deficient or ill-conditioned leaf: the column-by-column
-            // Householder factorization, from the stored values.
-#pragma unroll
-            for (int i = 0; i < FR; i++) {
-              const int r = tid + FW * 32 * i;
-#pragma unroll
-              for (int c = 0; c < NB; c++)
-                a[i][c] = (r < mrows && c < f.w) ? __ldcg(P + cm(r, c, st.ld)) : 0.0;
-            }
-            for (int e = tid; e < NB * (NB + 1); e += FW * 32) (&sm.T[0][0])[e] = 0.0;
-            if (tid < 2 * NB) (&sm.gsh[0][0])[tid] = 0.0;
-            factor_bar<FW>();
-          }
-          factor_leaf<FR, NB, FW>(a, sm, mrows, f.w, tau_leaf);
-        }
+        factor_leaf<FR, NB, FW>(a, sm, mrows, f.w, st.tau + (long long)f.k * g.n + f.j0);
 #pragma unroll
         for (int i = 0; i < FR; i++) {
           const int r = tid + FW * 32 * i;
@@ -1186,12 +848,6 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
 // (16-wide leaves with two staging passes measured slower at n = 400.)
 int bsof_leaf_width(int n) { return n <= 256 ? 16 : 8; }
 
-// Leaf factorization of the chain: CholeskyQR2 with Householder
-// reconstruction (1, the default) or column by column (0); process-wide.
-static std::atomic<int> g_cholqr{1};
-int bsof_cholqr_enabled() { return g_cholqr.load(); }
-void bsof_set_cholqr(int on) { g_cholqr.store(on ? 1 : 0); }
-
 int bsof_tiles(int n) { return (n + bsof_leaf_width(n) - 1) / bsof_leaf_width(n); }
 
 template <int R, int NB>
@@ -1225,7 +881,6 @@ cudaError_t launch_bsof_persistent(double* A, long long ld, int n, int L, double
                                    int workers, cudaStream_t st, int s_begin, int s_end) {
   BsofGeom g;
   g.form_g = G != nullptr;
-  g.cqr = bsof_cholqr_enabled();
   g.n = n;
   g.L = L;
   g.NB = bsof_leaf_width(n);

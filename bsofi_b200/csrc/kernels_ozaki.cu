@@ -61,7 +61,7 @@ struct OzSplitArgs {
   long long b_slice;
   int* b_exp;          // N
   int S;
-  int a_blocks;        // blocks [0, a_blocks) split A rows, the rest B columns
+  int a_blocks;        // blocks [0, a_blocks) split A rows (32 each), the rest B columns (8 each)
 };
 
 __device__ __forceinline__ double oz_a(const OzSplitArgs& s, int i, int k) {
@@ -92,44 +92,78 @@ __device__ __forceinline__ void oz_slices16(double (&r)[16], int S, int8_t* dst,
   }
 }
 
-__global__ void __launch_bounds__(128) ozaki_split_kernel(OzSplitArgs s) {
+// Scale factor 2^-e as one exact multiplication when 2^-e is a normal
+// double; `exact` false means the caller uses ldexp per element.
+__device__ __forceinline__ double pow2_neg(int e, bool& exact) {
+  exact = e > -1000 && e < 1000;
+  return exact ? ldexp(1.0, -e) : 1.0;
+}
+
+// A rows: a CTA of 256 threads takes 32 consecutive rows.  Pass 1, the row
+// maxima: warp w reads columns w, w+8, ... with lane = row (coalesced).
+// Pass 2: warp w cuts rows 4w..4w+3, lane l columns 16l..16l+15 (+512 j), so
+// each slice row is written as one contiguous segment per warp; the reads of
+// the four rows share their 32-byte sectors through L1.
+// B columns: one warp per column (K contiguous), eight per CTA.
+constexpr int OZ_SPLIT_ROWS = 32, OZ_SPLIT_THREADS = 256;
+
+__global__ void __launch_bounds__(OZ_SPLIT_THREADS) ozaki_split_kernel(OzSplitArgs s) {
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   if ((int)blockIdx.x < s.a_blocks) {
-    const int i = blockIdx.x * 128 + threadIdx.x;
-    if (i >= s.M) return;
-    double mx = 0.0;
-    bool bad = false;  // fmax drops NaN, so non-finite values are tracked apart
-    for (int k = 0; k < s.K; k++) {
-      const double v = oz_a(s, i, k);
-      bad |= !isfinite(v);
-      mx = fmax(mx, fabs(v));
-    }
-    int e = 0;
-    if (bad) {
-      s.a_exp[i] = OZ_EXP_NONFINITE;
-      mx = 0.0;
-    } else {
-      frexp(mx, &e);
-      s.a_exp[i] = e;
-    }
-    int8_t* row = s.a_out + (long long)i * s.Kp;
-    for (int k0 = 0; k0 < s.Kp; k0 += 16) {
-      double r[16];
-#pragma unroll
-      for (int j = 0; j < 16; j++) {
-        const int k = k0 + j;
-        r[j] = (mx > 0.0 && k < s.K) ? ldexp(oz_a(s, i, k), -e) : 0.0;
+    __shared__ double s_max[8][OZ_SPLIT_ROWS];
+    __shared__ int s_bad[8][OZ_SPLIT_ROWS];
+    const int r0 = blockIdx.x * OZ_SPLIT_ROWS;
+    {
+      const int i = r0 + lane;
+      double mx = 0.0;
+      bool bad = false;  // fmax drops NaN, so non-finite values are tracked apart
+      if (i < s.M) {
+        for (int k = warp; k < s.K; k += 8) {
+          const double v = oz_a(s, i, k);
+          bad |= !isfinite(v);
+          mx = fmax(mx, fabs(v));
+        }
       }
-      oz_slices16(r, s.S, row + k0, s.a_slice);
+      s_max[warp][lane] = mx;
+      s_bad[warp][lane] = bad;
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int rr = 0; rr < 4; rr++) {
+      const int lr = 4 * warp + rr, i = r0 + lr;
+      if (i >= s.M) break;  // warp-uniform
+      double mx = 0.0;
+      bool bad = false;
+#pragma unroll
+      for (int w = 0; w < 8; w++) {
+        mx = fmax(mx, s_max[w][lr]);
+        bad |= s_bad[w][lr] != 0;
+      }
+      int e = 0;
+      if (bad) mx = 0.0;
+      else frexp(mx, &e);
+      if (lane == 0) s.a_exp[i] = bad ? OZ_EXP_NONFINITE : e;
+      bool exact;
+      const double sc = pow2_neg(e, exact);
+      int8_t* row = s.a_out + (long long)i * s.Kp;
+      for (int k0 = 16 * lane; k0 < s.Kp; k0 += 32 * 16) {
+        double r[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+          const int k = k0 + j;
+          const double v = (mx > 0.0 && k < s.K) ? oz_a(s, i, k) : 0.0;
+          r[j] = exact ? v * sc : ldexp(v, -e);
+        }
+        oz_slices16(r, s.S, row + k0, s.a_slice);
+      }
     }
     return;
   }
-  // B columns: one warp per column.
-  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  const int j = ((int)blockIdx.x - s.a_blocks) * 4 + warp;
+  const int j = ((int)blockIdx.x - s.a_blocks) * 8 + warp;
   if (j >= s.N) return;
   const double* col = s.b + (long long)j * s.ldb;
   double mx = 0.0;
-  bool bad = false;  // fmax drops NaN, so non-finite values are tracked apart
+  bool bad = false;
   for (int k = lane; k < s.K; k += 32) {
     bad |= !isfinite(col[k]);
     mx = fmax(mx, fabs(col[k]));
@@ -138,20 +172,19 @@ __global__ void __launch_bounds__(128) ozaki_split_kernel(OzSplitArgs s) {
   for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
   bad = __any_sync(0xffffffffu, bad);
   int e = 0;
-  if (bad) {
-    if (lane == 0) s.b_exp[j] = OZ_EXP_NONFINITE;
-    mx = 0.0;
-  } else {
-    frexp(mx, &e);
-    if (lane == 0) s.b_exp[j] = e;
-  }
+  if (bad) mx = 0.0;
+  else frexp(mx, &e);
+  if (lane == 0) s.b_exp[j] = bad ? OZ_EXP_NONFINITE : e;
+  bool exact;
+  const double sc = pow2_neg(e, exact);
   int8_t* row = s.b_out + (long long)j * s.Kp;
   for (int k0 = lane * 16; k0 < s.Kp; k0 += 32 * 16) {
     double r[16];
 #pragma unroll
     for (int q = 0; q < 16; q++) {
       const int k = k0 + q;
-      r[q] = (mx > 0.0 && k < s.K) ? ldexp(col[k], -e) : 0.0;
+      const double v = (mx > 0.0 && k < s.K) ? col[k] : 0.0;
+      r[q] = exact ? v * sc : ldexp(v, -e);
     }
     oz_slices16(r, s.S, row + k0, s.b_slice);
   }
@@ -442,9 +475,9 @@ cudaError_t launch_ozaki_product(const OzProduct& p, cudaStream_t st) {
   sa.b_slice = (long long)p.N * Kp;
   sa.b_exp = o.eb;
   sa.S = p.S;
-  sa.a_blocks = (p.M + 127) / 128;
-  const int b_blocks = (p.N + 3) / 4;
-  ozaki_split_kernel<<<sa.a_blocks + b_blocks, 128, 0, st>>>(sa);
+  sa.a_blocks = (p.M + OZ_SPLIT_ROWS - 1) / OZ_SPLIT_ROWS;
+  const int b_blocks = (p.N + 7) / 8;
+  ozaki_split_kernel<<<sa.a_blocks + b_blocks, OZ_SPLIT_THREADS, 0, st>>>(sa);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   CUtensorMap ma, mb;

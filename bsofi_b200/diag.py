@@ -1,7 +1,7 @@
 """Diagnostics of the device pipeline through the C ABI.
 
-    python -m bsofi_b200.diag bsof-timeline N_BLOCK L [REPS] [--cholqr=0|1]
-    python -m bsofi_b200.diag invert N_BLOCK L [REPS] [U] [--cholqr=0|1]
+    python -m bsofi_b200.diag bsof-timeline N_BLOCK L [REPS]
+    python -m bsofi_b200.diag invert N_BLOCK L [REPS] [U]
     python -m bsofi_b200.diag invert-mixed N_BLOCK L [REPS] [SLICES]
 
 bsof-timeline inverts a seeded Hubbard matrix (a random p-cyclic one when n is
@@ -155,12 +155,6 @@ def invert_mixed_timing(n, L, reps=3, U=4.0, slices=0):
 
 
 def main(argv):
-    # --cholqr=0 times the column-by-column leaf factorization of the BSOF
-    # chain instead of CholeskyQR2 with Householder reconstruction.
-    for a in list(argv):
-        if a.startswith("--cholqr="):
-            _lib.load().bsofi_device_set_bsof_cholqr(int(a.split("=", 1)[1]))
-            argv = [x for x in argv if x != a]
     if len(argv) >= 3 and argv[0] == "bsof-timeline":
         n, L = int(argv[1]), int(argv[2])
         reps = int(argv[3]) if len(argv) > 3 else 3

@@ -408,16 +408,6 @@ void bsofi_device_set_bsof_workers(int workers);
  * results are the same as without the split).  on = 0 turns this off for the
  * process, 1 (the default) on. */
 void bsofi_device_set_bstri_overlap(int on);
-/* How the BSOF chain factors each leaf of 16 (8 when n > 256) columns (no
- * reference counterpart; the reference calls dgeqrf, src/bsofi_cpu.c:97):
- * on = 1 (the default) by CholeskyQR2 and Householder reconstruction -- two
- * Gram matrices and small factorizations in one warp, giving LAPACK's
- * reflectors, tau and R to rounding -- falling back to the column-by-column
- * Householder factorization for a leaf whose Cholesky pivot falls below
- * 1e-12 of its largest squared column norm (rank-deficient or condition number
- * above about 1e6) and for a narrower last leaf; on = 0 always column by
- * column.  Process-wide. */
-void bsofi_device_set_bsof_cholqr(int on);
 /* Diagnostics (no reference counterpart): with on = 1, the persistent BSOI
  * launches made by this thread wait, in every step after the first, on a
  * zeroed workspace word that nothing writes, under a short poll limit (about
