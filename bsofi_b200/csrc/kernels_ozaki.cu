@@ -22,11 +22,15 @@
 //
 // Kernels: ozaki_split_kernel writes the slices and exponents of both
 // operands (one launch); ozaki_gemm_kernel is a warp-specialised tcgen05
-// kernel: warp 0 issues TMA tile loads (32-byte swizzle, K-major) into a
-// 4-stage mbarrier ring, warp 1 issues the S(S+1)/2 MMAs of each 32-deep K
-// step into S int32 accumulators of 128 x 64 in tensor memory, warps 2-5 read
-// the accumulators back (tcgen05.ld) and write the FP64 tile.  The tensor maps
-// cover this GPU's memory only and no load uses cluster multicast.
+// kernel: warp 0 issues TMA tile loads (K-major, 128-byte swizzle, so every
+// box row is a whole 128-byte line) -- per 128-byte K chunk all S slices of B
+// into one of two buffers, then the S slices of A one by one through a
+// 4-stage ring; warp 1 issues the S(S+1)/2 MMAs of each 32-byte K step (four
+// per chunk, the descriptor advanced inside the swizzle atom) into S int32
+// accumulators of 128 x 64 in tensor memory; warps 2-5 read the accumulators
+// back (tcgen05.ld) and write the FP64 tile.  (Boxes of 32-byte rows, one
+// sector per TMA request, held the kernel to a quarter of the int8 peak.)  The
+// tensor maps cover this GPU's memory only and no load uses cluster multicast.
 #include <cuda.h>
 #include <climits>
 #include <mutex>
@@ -37,7 +41,7 @@
 
 namespace bsofi {
 
-constexpr int OZ_BM = 128, OZ_BN = 64, OZ_BK = 32, OZ_STAGES = 4;
+constexpr int OZ_BM = 128, OZ_BN = 64, OZ_BK = 128, OZ_ASTAGES = 4, OZ_BBUFS = 2;
 constexpr int OZ_THREADS = 192;
 constexpr int OZ_EXP_NONFINITE = INT_MIN;  // exponent of a row/column holding Inf or NaN
 
@@ -204,14 +208,18 @@ struct OzGemmArgs {
   long long spin_limit;
 };
 
+// Shared-memory layout of the product kernel: a ring of OZ_ASTAGES A tiles
+// (one slice, 128 rows x 128 K bytes each) and OZ_BBUFS buffers holding every B
+// slice of one 128-byte K chunk (64 rows x 128 bytes each).  Tiles are loaded
+// by TMA with the 128-byte swizzle, so each box row is a whole 128-byte line.
 template <int S>
 struct OzCfg {
-  static constexpr int A_TILE = OZ_BM * OZ_BK;  // bytes of one A slice tile
-  static constexpr int B_TILE = OZ_BN * OZ_BK;
-  static constexpr int STAGE = S * (A_TILE + B_TILE);
+  static constexpr int A_TILE = OZ_BM * OZ_BK;  // 16 KB
+  static constexpr int B_TILE = OZ_BN * OZ_BK;  // 8 KB
+  static constexpr int B_CHUNK = S * B_TILE;
   // + alignment slack; at least 120 KB so that one CTA holds an SM alone and
   // its tensor-memory allocation never waits for another CTA's.
-  static constexpr size_t NEED = (size_t)OZ_STAGES * STAGE + 1024;
+  static constexpr size_t NEED = (size_t)OZ_ASTAGES * A_TILE + (size_t)OZ_BBUFS * B_CHUNK + 1024;
   static constexpr size_t SMEM = NEED > 120 * 1024 ? NEED : 120 * 1024;
   static constexpr uint32_t TMEM_COLS = S * OZ_BN <= 256 ? 256 : 512;
   static_assert(S * OZ_BN <= 512, "accumulators exceed tensor memory");
@@ -224,8 +232,12 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
   using C = OzCfg<S>;
   extern __shared__ uint8_t oz_smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)oz_smem_raw + 1023) & ~(uintptr_t)1023);
-  __shared__ __align__(8) uint64_t full[OZ_STAGES];
-  __shared__ __align__(8) uint64_t empty[OZ_STAGES];
+  uint8_t* sA = smem;                                  // OZ_ASTAGES x A_TILE
+  uint8_t* sB = smem + (size_t)OZ_ASTAGES * C::A_TILE;  // OZ_BBUFS x B_CHUNK
+  __shared__ __align__(8) uint64_t a_full[OZ_ASTAGES];
+  __shared__ __align__(8) uint64_t a_empty[OZ_ASTAGES];
+  __shared__ __align__(8) uint64_t b_full[OZ_BBUFS];
+  __shared__ __align__(8) uint64_t b_empty[OZ_BBUFS];
   __shared__ __align__(8) uint64_t acc_full;
   __shared__ uint32_t tmem_base;
   __shared__ int abort_flag;
@@ -237,9 +249,13 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
   constexpr uint32_t IDESC = tc::idesc_i8(OZ_BM, OZ_BN);
 
   if (threadIdx.x == 0) {
-    for (int i = 0; i < OZ_STAGES; i++) {
-      tc::mbar_init(&full[i], 1);
-      tc::mbar_init(&empty[i], 1);
+    for (int i = 0; i < OZ_ASTAGES; i++) {
+      tc::mbar_init(&a_full[i], 1);
+      tc::mbar_init(&a_empty[i], 1);
+    }
+    for (int i = 0; i < OZ_BBUFS; i++) {
+      tc::mbar_init(&b_full[i], 1);
+      tc::mbar_init(&b_empty[i], 1);
     }
     tc::mbar_init(&acc_full, 1);
     abort_flag = 0;
@@ -254,48 +270,78 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
   __syncthreads();
   tc::tc_fence_after();
   const uint32_t tbase = tmem_base;
-  int issued = 0;  // K steps whose loads warp 0 issued
+  int a_issued = 0, b_issued = 0;  // loads warp 0 issued
 
   if (warp == 0 && lane == 0) {
-    // TMA producer.
+    // TMA producer: per 128-byte K chunk, every B slice into a B buffer, then
+    // the S A slices one by one through the A ring.
     tc::prefetch_tmap(&tma_a);
     tc::prefetch_tmap(&tma_b);
-    for (int kc = 0; kc < nk; kc++) {
-      const int st = kc % OZ_STAGES;
-      if (kc >= OZ_STAGES &&
-          !tc::mbar_wait(&empty[st], ((kc / OZ_STAGES) - 1) & 1, g.spin_limit, abort_v)) {
-        abort_flag = 1;
-        atomicExch(g.err, 1);
+    bool ok = true;
+    for (int kc = 0; kc < nk && ok; kc++) {
+      const int bb = kc % OZ_BBUFS;
+      if (kc >= OZ_BBUFS &&
+          !tc::mbar_wait(&b_empty[bb], ((kc / OZ_BBUFS) - 1) & 1, g.spin_limit, abort_v)) {
+        ok = false;
         break;
       }
-      tc::mbar_arrive_expect_tx(&full[st], C::STAGE);
-      uint8_t* sa = smem + (size_t)st * C::STAGE;
-      uint8_t* sb = sa + S * C::A_TILE;
-      for (int s = 0; s < S; s++) tc::tma_load_3d(sa + s * C::A_TILE, &tma_a, &full[st], kc * OZ_BK, m0, s);
-      for (int t = 0; t < S; t++) tc::tma_load_3d(sb + t * C::B_TILE, &tma_b, &full[st], kc * OZ_BK, n0, t);
-      issued = kc + 1;
+      tc::mbar_arrive_expect_tx(&b_full[bb], C::B_CHUNK);
+      for (int t = 0; t < S; t++)
+        tc::tma_load_3d(sB + (size_t)bb * C::B_CHUNK + t * C::B_TILE, &tma_b, &b_full[bb],
+                        kc * OZ_BK, n0, t);
+      b_issued = kc + 1;
+      for (int s = 0; s < S; s++) {
+        const int ai = kc * S + s, st = ai % OZ_ASTAGES;
+        if (ai >= OZ_ASTAGES &&
+            !tc::mbar_wait(&a_empty[st], ((ai / OZ_ASTAGES) - 1) & 1, g.spin_limit, abort_v)) {
+          ok = false;
+          break;
+        }
+        tc::mbar_arrive_expect_tx(&a_full[st], C::A_TILE);
+        tc::tma_load_3d(sA + (size_t)st * C::A_TILE, &tma_a, &a_full[st], kc * OZ_BK, m0, s);
+        a_issued = ai + 1;
+      }
+    }
+    if (!ok) {
+      abort_flag = 1;
+      atomicExch(g.err, 1);
     }
   } else if (warp == 1 && lane == 0) {
-    // MMA issuer: accumulator d (columns d*64 .. d*64+63) collects s + t = d.
-    for (int kc = 0; kc < nk; kc++) {
-      const int st = kc % OZ_STAGES;
-      if (!tc::mbar_wait(&full[st], (kc / OZ_STAGES) & 1, g.spin_limit, abort_v)) {
-        abort_flag = 1;
-        atomicExch(g.err, 1);
+    // MMA issuer: accumulator d (columns d*64 .. d*64+63) collects s + t = d;
+    // each 128-byte chunk is four 32-byte K steps inside the swizzle atom.
+    bool ok = true;
+    for (int kc = 0; kc < nk && ok; kc++) {
+      const int bb = kc % OZ_BBUFS;
+      if (!tc::mbar_wait(&b_full[bb], (kc / OZ_BBUFS) & 1, g.spin_limit, abort_v)) {
+        ok = false;
         break;
       }
-      tc::tc_fence_after();
-      const uint8_t* sa = smem + (size_t)st * C::STAGE;
-      const uint8_t* sb = sa + S * C::A_TILE;
-#pragma unroll
+      const uint8_t* sb = sB + (size_t)bb * C::B_CHUNK;
       for (int s = 0; s < S; s++) {
-        const uint64_t da = tc::desc_k_sw32(sa + s * C::A_TILE);
+        const int ai = kc * S + s, st = ai % OZ_ASTAGES;
+        if (!tc::mbar_wait(&a_full[st], (ai / OZ_ASTAGES) & 1, g.spin_limit, abort_v)) {
+          ok = false;
+          break;
+        }
+        tc::tc_fence_after();
+        const uint64_t da = tc::desc_k_sw128(sA + (size_t)st * C::A_TILE);
 #pragma unroll
-        for (int t = 0; s + t < S; t++)
-          tc::mma_i8(tbase + (uint32_t)((s + t) * OZ_BN), da, tc::desc_k_sw32(sb + t * C::B_TILE),
-                     IDESC, (kc > 0 || s > 0) ? 1u : 0u);
+        for (int kk = 0; kk < OZ_BK / 32; kk++) {
+#pragma unroll
+          for (int t = 0; t < S; t++) {
+            if (s + t < S)
+              tc::mma_i8(tbase + (uint32_t)((s + t) * OZ_BN), da + 2 * kk,
+                         tc::desc_k_sw128(sb + t * C::B_TILE) + 2 * kk, IDESC,
+                         (kc > 0 || s > 0 || kk > 0) ? 1u : 0u);
+          }
+        }
+        tc::mma_commit(&a_empty[st]);  // the A stage is free once these MMAs have read it
       }
-      tc::mma_commit(&empty[st]);  // the stage is free once these MMAs have read it
+      if (ok) tc::mma_commit(&b_empty[bb]);
+    }
+    if (!ok) {
+      abort_flag = 1;
+      atomicExch(g.err, 1);
     }
     tc::mma_commit(&acc_full);  // every MMA issued above is complete
   } else if (warp >= 2) {
@@ -328,8 +374,10 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
             if (col < g.N) {
               const int ec = g.b_exp[col];
               double out;
-              if (er == OZ_EXP_NONFINITE || ec == OZ_EXP_NONFINITE) out = __longlong_as_double(0x7ff8000000000000ll);
-              else out = ldexp(acc[j], er + ec);
+              if (er == OZ_EXP_NONFINITE || ec == OZ_EXP_NONFINITE)
+                out = __longlong_as_double(0x7ff8000000000000ll);
+              else
+                out = ldexp(acc[j], er + ec);
               double* p = col < g.nsplit ? g.c0 + (long long)col * g.ldc0
                                          : g.c1 + (long long)(col - g.nsplit) * g.ldc1;
               p[row] = out;
@@ -347,9 +395,10 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
   // and tensor memory are released (on the normal path these waits return at
   // once; after an abort they wait, bounded, for copies and MMAs in flight).
   if (warp == 0 && lane == 0) {
-    const int from = issued > OZ_STAGES ? issued - OZ_STAGES : 0;
-    for (int kc = from; kc < issued; kc++)
-      tc::mbar_wait(&full[kc % OZ_STAGES], (kc / OZ_STAGES) & 1, g.spin_limit, &no_abort);
+    for (int ai = a_issued > OZ_ASTAGES ? a_issued - OZ_ASTAGES : 0; ai < a_issued; ai++)
+      tc::mbar_wait(&a_full[ai % OZ_ASTAGES], (ai / OZ_ASTAGES) & 1, g.spin_limit, &no_abort);
+    for (int kc = b_issued > OZ_BBUFS ? b_issued - OZ_BBUFS : 0; kc < b_issued; kc++)
+      tc::mbar_wait(&b_full[kc % OZ_BBUFS], (kc / OZ_BBUFS) & 1, g.spin_limit, &no_abort);
   }
   if (warp == 1 && lane == 0) tc::mbar_wait(&acc_full, 0, g.spin_limit, &no_abort);
   tc::tc_fence_before();
@@ -384,7 +433,7 @@ EncodeTiled encode_tiled() {
 }
 
 // Tensor map of `slices` int8 matrices of rows x Kp (K contiguous), read in
-// boxes of 32 (K) x box_rows x 1 with the 32-byte swizzle.
+// boxes of 128 (K) x box_rows x 1 with the 128-byte swizzle.
 cudaError_t slice_map(CUtensorMap* m, const int8_t* base, int Kp, int rows, int slices,
                       int box_rows) {
   EncodeTiled f = encode_tiled();
@@ -394,7 +443,7 @@ cudaError_t slice_map(CUtensorMap* m, const int8_t* base, int Kp, int rows, int 
   const cuuint32_t box[3] = {(cuuint32_t)OZ_BK, (cuuint32_t)box_rows, 1};
   const cuuint32_t es[3] = {1, 1, 1};
   const CUresult r = f(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<int8_t*>(base), dims,
-                       strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
+                       strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }

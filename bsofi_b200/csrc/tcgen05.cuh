@@ -144,6 +144,15 @@ __device__ __forceinline__ uint64_t desc_k_sw32(const void* tile) {
   return a | (1ull << 16) | (16ull << 32) | (1ull << 46) | (6ull << 61);
 }
 
+// The same for a tile stored with the 128-byte swizzle: rows of 128 bytes,
+// 8-row groups 1024 bytes apart (swizzle mode 2).  The tile must start on a
+// 1024-byte boundary; a K step of 32 bytes inside the 128-byte atom adds 2
+// (32 >> 4) to the start address field.
+__device__ __forceinline__ uint64_t desc_k_sw128(const void* tile) {
+  const uint64_t a = (smem_u32(tile) & 0x3FFFFu) >> 4;
+  return a | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
+}
+
 // Instruction descriptor of kind::i8: signed A and B, int32 accumulator,
 // both operands K-major, M x N.  c_format bits 4-5 (2 = s32), a_format 7-9
 // and b_format 10-12 (1 = signed), N >> 3 in bits 17-22, M >> 4 in 24-28.
