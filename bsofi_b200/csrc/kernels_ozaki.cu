@@ -22,15 +22,14 @@
 //
 // Kernels: ozaki_split_kernel writes the slices and exponents of both
 // operands (one launch); ozaki_gemm_kernel is a warp-specialised tcgen05
-// kernel: warp 0 issues TMA tile loads (K-major, 128-byte swizzle, so every
-// box row is a whole 128-byte line) -- per 128-byte K chunk all S slices of B
-// into one of two buffers, then the S slices of A one by one through a
-// 4-stage ring; warp 1 issues the S(S+1)/2 MMAs of each 32-byte K step (four
-// per chunk, the descriptor advanced inside the swizzle atom) into S int32
+// kernel: warp 0 issues TMA tile loads (32-byte swizzle, K-major) into a
+// 4-stage mbarrier ring, each stage holding all S slices of A and B for 32 K
+// bytes; warp 1 issues the S(S+1)/2 MMAs of each 32-deep K step into S int32
 // accumulators of 128 x 64 in tensor memory; warps 2-5 read the accumulators
-// back (tcgen05.ld) and write the FP64 tile.  (Boxes of 32-byte rows, one
-// sector per TMA request, held the kernel to a quarter of the int8 peak.)  The
-// tensor maps cover this GPU's memory only and no load uses cluster multicast.
+// back (tcgen05.ld) and write the FP64 tile.  (A variant with 128-byte
+// swizzled rows, one A slice per stage, measured 45% slower: less data in
+// flight.)  The tensor maps cover this GPU's memory only and no load uses
+// cluster multicast.
 #include <cuda.h>
 #include <climits>
 #include <mutex>
@@ -41,7 +40,7 @@
 
 namespace bsofi {
 
-constexpr int OZ_BM = 128, OZ_BN = 64, OZ_BK = 128, OZ_ASTAGES = 4, OZ_BBUFS = 2;
+constexpr int OZ_BM = 128, OZ_BN = 64, OZ_BK = 32, OZ_STAGES = 4;
 constexpr int OZ_THREADS = 192;
 constexpr int OZ_EXP_NONFINITE = INT_MIN;  // exponent of a row/column holding Inf or NaN
 
@@ -105,17 +104,22 @@ __device__ __forceinline__ double pow2_neg(int e, bool& exact) {
 
 // A rows: a CTA of 256 threads takes 32 consecutive rows.  Pass 1, the row
 // maxima: warp w reads columns w, w+8, ... with lane = row (coalesced).
-// Pass 2: warp w cuts rows 4w..4w+3, lane l columns 16l..16l+15 (+512 j), so
-// each slice row is written as one contiguous segment per warp; the reads of
-// the four rows share their 32-byte sectors through L1.
+// Pass 2, per chunk of 128 columns: the 32 x 128 block is staged in shared
+// memory by the same coalesced column reads, then warp w cuts rows
+// 4w..4w+3 with lane l on columns 4l..4l+3 (two 16-byte shared loads), and
+// writes one packed 4-byte word per slice: 128 contiguous bytes per warp.
 // B columns: one warp per column (K contiguous), eight per CTA.
-constexpr int OZ_SPLIT_ROWS = 32, OZ_SPLIT_THREADS = 256;
+constexpr int OZ_SPLIT_ROWS = 32, OZ_SPLIT_THREADS = 256, OZ_SPLIT_CHUNK = 128;
+constexpr int OZ_SPLIT_LD = OZ_SPLIT_CHUNK + 2;  // row stride of the staged block (16-byte rows)
 
 __global__ void __launch_bounds__(OZ_SPLIT_THREADS) ozaki_split_kernel(OzSplitArgs s) {
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   if ((int)blockIdx.x < s.a_blocks) {
     __shared__ double s_max[8][OZ_SPLIT_ROWS];
     __shared__ int s_bad[8][OZ_SPLIT_ROWS];
+    __shared__ __align__(16) double s_blk[OZ_SPLIT_ROWS][OZ_SPLIT_LD];
+    __shared__ double s_sc[OZ_SPLIT_ROWS];
+    __shared__ int s_e[OZ_SPLIT_ROWS];
     const int r0 = blockIdx.x * OZ_SPLIT_ROWS;
     {
       const int i = r0 + lane;
@@ -132,10 +136,8 @@ __global__ void __launch_bounds__(OZ_SPLIT_THREADS) ozaki_split_kernel(OzSplitAr
       s_bad[warp][lane] = bad;
     }
     __syncthreads();
-#pragma unroll 1
-    for (int rr = 0; rr < 4; rr++) {
-      const int lr = 4 * warp + rr, i = r0 + lr;
-      if (i >= s.M) break;  // warp-uniform
+    if (threadIdx.x < OZ_SPLIT_ROWS) {
+      const int lr = threadIdx.x, i = r0 + lr;
       double mx = 0.0;
       bool bad = false;
 #pragma unroll
@@ -144,21 +146,50 @@ __global__ void __launch_bounds__(OZ_SPLIT_THREADS) ozaki_split_kernel(OzSplitAr
         bad |= s_bad[w][lr] != 0;
       }
       int e = 0;
-      if (bad) mx = 0.0;
-      else frexp(mx, &e);
-      if (lane == 0) s.a_exp[i] = bad ? OZ_EXP_NONFINITE : e;
+      if (!bad) frexp(mx, &e);
+      // Scale 0 makes every slice of a zero or non-finite row zero.
       bool exact;
       const double sc = pow2_neg(e, exact);
-      int8_t* row = s.a_out + (long long)i * s.Kp;
-      for (int k0 = 16 * lane; k0 < s.Kp; k0 += 32 * 16) {
-        double r[16];
-#pragma unroll
-        for (int j = 0; j < 16; j++) {
-          const int k = k0 + j;
-          const double v = (mx > 0.0 && k < s.K) ? oz_a(s, i, k) : 0.0;
-          r[j] = exact ? v * sc : ldexp(v, -e);
+      s_sc[lr] = (bad || !(mx > 0.0)) ? 0.0 : (exact ? sc : -1.0);  // -1: ldexp per element
+      s_e[lr] = e;
+      if (i < s.M) s.a_exp[i] = bad ? OZ_EXP_NONFINITE : e;
+    }
+    for (int k0 = 0; k0 < s.Kp; k0 += OZ_SPLIT_CHUNK) {
+      __syncthreads();  // s_sc ready / the previous chunk consumed
+      {
+        const int i = r0 + lane;
+        for (int c = warp; c < OZ_SPLIT_CHUNK; c += 8) {
+          const int k = k0 + c;
+          s_blk[lane][c] = (i < s.M && k < s.K) ? oz_a(s, i, k) : 0.0;
         }
-        oz_slices16(r, s.S, row + k0, s.a_slice);
+      }
+      __syncthreads();
+#pragma unroll 1
+      for (int rr = 0; rr < 4; rr++) {
+        const int lr = 4 * warp + rr, i = r0 + lr;
+        if (i >= s.M) break;  // warp-uniform
+        // Kp is a multiple of 32 (4-column groups never straddle it); the last
+        // chunk may end before 128 columns.
+        if (k0 + 4 * lane >= s.Kp) continue;
+        const double sc = s_sc[lr];
+        const double2 p0 = *reinterpret_cast<const double2*>(&s_blk[lr][4 * lane]);
+        const double2 p1 = *reinterpret_cast<const double2*>(&s_blk[lr][4 * lane + 2]);
+        double r[4] = {p0.x, p0.y, p1.x, p1.y};
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          r[q] = sc == 0.0 ? 0.0 : (sc > 0.0 ? r[q] * sc : ldexp(r[q], -s_e[lr]));
+        int8_t* dst = s.a_out + (long long)i * s.Kp + k0 + 4 * lane;
+        for (int sl = 0; sl < s.S; sl++) {
+          uint32_t word = 0;
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            const double t = r[q] * 128.0;
+            const double v = trunc(t);
+            r[q] = t - v;  // exact
+            word |= ((uint32_t)(int)v & 0xffu) << (8 * q);
+          }
+          *reinterpret_cast<uint32_t*>(dst + (long long)sl * s.a_slice) = word;
+        }
       }
     }
     return;
@@ -208,18 +239,14 @@ struct OzGemmArgs {
   long long spin_limit;
 };
 
-// Shared-memory layout of the product kernel: a ring of OZ_ASTAGES A tiles
-// (one slice, 128 rows x 128 K bytes each) and OZ_BBUFS buffers holding every B
-// slice of one 128-byte K chunk (64 rows x 128 bytes each).  Tiles are loaded
-// by TMA with the 128-byte swizzle, so each box row is a whole 128-byte line.
 template <int S>
 struct OzCfg {
-  static constexpr int A_TILE = OZ_BM * OZ_BK;  // 16 KB
-  static constexpr int B_TILE = OZ_BN * OZ_BK;  // 8 KB
-  static constexpr int B_CHUNK = S * B_TILE;
+  static constexpr int A_TILE = OZ_BM * OZ_BK;  // bytes of one A slice tile
+  static constexpr int B_TILE = OZ_BN * OZ_BK;
+  static constexpr int STAGE = S * (A_TILE + B_TILE);
   // + alignment slack; at least 120 KB so that one CTA holds an SM alone and
   // its tensor-memory allocation never waits for another CTA's.
-  static constexpr size_t NEED = (size_t)OZ_ASTAGES * A_TILE + (size_t)OZ_BBUFS * B_CHUNK + 1024;
+  static constexpr size_t NEED = (size_t)OZ_STAGES * STAGE + 1024;
   static constexpr size_t SMEM = NEED > 120 * 1024 ? NEED : 120 * 1024;
   static constexpr uint32_t TMEM_COLS = S * OZ_BN <= 256 ? 256 : 512;
   static_assert(S * OZ_BN <= 512, "accumulators exceed tensor memory");
@@ -232,12 +259,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
   using C = OzCfg<S>;
   extern __shared__ uint8_t oz_smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)oz_smem_raw + 1023) & ~(uintptr_t)1023);
-  uint8_t* sA = smem;                                  // OZ_ASTAGES x A_TILE
-  uint8_t* sB = smem + (size_t)OZ_ASTAGES * C::A_TILE;  // OZ_BBUFS x B_CHUNK
-  __shared__ __align__(8) uint64_t a_full[OZ_ASTAGES];
-  __shared__ __align__(8) uint64_t a_empty[OZ_ASTAGES];
-  __shared__ __align__(8) uint64_t b_full[OZ_BBUFS];
-  __shared__ __align__(8) uint64_t b_empty[OZ_BBUFS];
+  __shared__ __align__(8) uint64_t full[OZ_STAGES];
+  __shared__ __align__(8) uint64_t empty[OZ_STAGES];
   __shared__ __align__(8) uint64_t acc_full;
   __shared__ uint32_t tmem_base;
   __shared__ int abort_flag;
@@ -249,13 +272,9 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
   constexpr uint32_t IDESC = tc::idesc_i8(OZ_BM, OZ_BN);
 
   if (threadIdx.x == 0) {
-    for (int i = 0; i < OZ_ASTAGES; i++) {
-      tc::mbar_init(&a_full[i], 1);
-      tc::mbar_init(&a_empty[i], 1);
-    }
-    for (int i = 0; i < OZ_BBUFS; i++) {
-      tc::mbar_init(&b_full[i], 1);
-      tc::mbar_init(&b_empty[i], 1);
+    for (int i = 0; i < OZ_STAGES; i++) {
+      tc::mbar_init(&full[i], 1);
+      tc::mbar_init(&empty[i], 1);
     }
     tc::mbar_init(&acc_full, 1);
     abort_flag = 0;
@@ -270,78 +289,48 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
   __syncthreads();
   tc::tc_fence_after();
   const uint32_t tbase = tmem_base;
-  int a_issued = 0, b_issued = 0;  // loads warp 0 issued
+  int issued = 0;  // K steps whose loads warp 0 issued
 
   if (warp == 0 && lane == 0) {
-    // TMA producer: per 128-byte K chunk, every B slice into a B buffer, then
-    // the S A slices one by one through the A ring.
+    // TMA producer.
     tc::prefetch_tmap(&tma_a);
     tc::prefetch_tmap(&tma_b);
-    bool ok = true;
-    for (int kc = 0; kc < nk && ok; kc++) {
-      const int bb = kc % OZ_BBUFS;
-      if (kc >= OZ_BBUFS &&
-          !tc::mbar_wait(&b_empty[bb], ((kc / OZ_BBUFS) - 1) & 1, g.spin_limit, abort_v)) {
-        ok = false;
+    for (int kc = 0; kc < nk; kc++) {
+      const int st = kc % OZ_STAGES;
+      if (kc >= OZ_STAGES &&
+          !tc::mbar_wait(&empty[st], ((kc / OZ_STAGES) - 1) & 1, g.spin_limit, abort_v)) {
+        abort_flag = 1;
+        atomicExch(g.err, 1);
         break;
       }
-      tc::mbar_arrive_expect_tx(&b_full[bb], C::B_CHUNK);
-      for (int t = 0; t < S; t++)
-        tc::tma_load_3d(sB + (size_t)bb * C::B_CHUNK + t * C::B_TILE, &tma_b, &b_full[bb],
-                        kc * OZ_BK, n0, t);
-      b_issued = kc + 1;
-      for (int s = 0; s < S; s++) {
-        const int ai = kc * S + s, st = ai % OZ_ASTAGES;
-        if (ai >= OZ_ASTAGES &&
-            !tc::mbar_wait(&a_empty[st], ((ai / OZ_ASTAGES) - 1) & 1, g.spin_limit, abort_v)) {
-          ok = false;
-          break;
-        }
-        tc::mbar_arrive_expect_tx(&a_full[st], C::A_TILE);
-        tc::tma_load_3d(sA + (size_t)st * C::A_TILE, &tma_a, &a_full[st], kc * OZ_BK, m0, s);
-        a_issued = ai + 1;
-      }
-    }
-    if (!ok) {
-      abort_flag = 1;
-      atomicExch(g.err, 1);
+      tc::mbar_arrive_expect_tx(&full[st], C::STAGE);
+      uint8_t* sa = smem + (size_t)st * C::STAGE;
+      uint8_t* sb = sa + S * C::A_TILE;
+      for (int s = 0; s < S; s++) tc::tma_load_3d(sa + s * C::A_TILE, &tma_a, &full[st], kc * OZ_BK, m0, s);
+      for (int t = 0; t < S; t++) tc::tma_load_3d(sb + t * C::B_TILE, &tma_b, &full[st], kc * OZ_BK, n0, t);
+      issued = kc + 1;
     }
   } else if (warp == 1 && lane == 0) {
-    // MMA issuer: accumulator d (columns d*64 .. d*64+63) collects s + t = d;
-    // each 128-byte chunk is four 32-byte K steps inside the swizzle atom.
-    bool ok = true;
-    for (int kc = 0; kc < nk && ok; kc++) {
-      const int bb = kc % OZ_BBUFS;
-      if (!tc::mbar_wait(&b_full[bb], (kc / OZ_BBUFS) & 1, g.spin_limit, abort_v)) {
-        ok = false;
+    // MMA issuer: accumulator d (columns d*64 .. d*64+63) collects s + t = d.
+    for (int kc = 0; kc < nk; kc++) {
+      const int st = kc % OZ_STAGES;
+      if (!tc::mbar_wait(&full[st], (kc / OZ_STAGES) & 1, g.spin_limit, abort_v)) {
+        abort_flag = 1;
+        atomicExch(g.err, 1);
         break;
       }
-      const uint8_t* sb = sB + (size_t)bb * C::B_CHUNK;
+      tc::tc_fence_after();
+      const uint8_t* sa = smem + (size_t)st * C::STAGE;
+      const uint8_t* sb = sa + S * C::A_TILE;
+#pragma unroll
       for (int s = 0; s < S; s++) {
-        const int ai = kc * S + s, st = ai % OZ_ASTAGES;
-        if (!tc::mbar_wait(&a_full[st], (ai / OZ_ASTAGES) & 1, g.spin_limit, abort_v)) {
-          ok = false;
-          break;
-        }
-        tc::tc_fence_after();
-        const uint64_t da = tc::desc_k_sw128(sA + (size_t)st * C::A_TILE);
+        const uint64_t da = tc::desc_k_sw32(sa + s * C::A_TILE);
 #pragma unroll
-        for (int kk = 0; kk < OZ_BK / 32; kk++) {
-#pragma unroll
-          for (int t = 0; t < S; t++) {
-            if (s + t < S)
-              tc::mma_i8(tbase + (uint32_t)((s + t) * OZ_BN), da + 2 * kk,
-                         tc::desc_k_sw128(sb + t * C::B_TILE) + 2 * kk, IDESC,
-                         (kc > 0 || s > 0 || kk > 0) ? 1u : 0u);
-          }
-        }
-        tc::mma_commit(&a_empty[st]);  // the A stage is free once these MMAs have read it
+        for (int t = 0; s + t < S; t++)
+          tc::mma_i8(tbase + (uint32_t)((s + t) * OZ_BN), da, tc::desc_k_sw32(sb + t * C::B_TILE),
+                     IDESC, (kc > 0 || s > 0) ? 1u : 0u);
       }
-      if (ok) tc::mma_commit(&b_empty[bb]);
-    }
-    if (!ok) {
-      abort_flag = 1;
-      atomicExch(g.err, 1);
+      tc::mma_commit(&empty[st]);  // the stage is free once these MMAs have read it
     }
     tc::mma_commit(&acc_full);  // every MMA issued above is complete
   } else if (warp >= 2) {
@@ -374,10 +363,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
             if (col < g.N) {
               const int ec = g.b_exp[col];
               double out;
-              if (er == OZ_EXP_NONFINITE || ec == OZ_EXP_NONFINITE)
-                out = __longlong_as_double(0x7ff8000000000000ll);
-              else
-                out = ldexp(acc[j], er + ec);
+              if (er == OZ_EXP_NONFINITE || ec == OZ_EXP_NONFINITE) out = __longlong_as_double(0x7ff8000000000000ll);
+              else out = ldexp(acc[j], er + ec);
               double* p = col < g.nsplit ? g.c0 + (long long)col * g.ldc0
                                          : g.c1 + (long long)(col - g.nsplit) * g.ldc1;
               p[row] = out;
@@ -395,10 +382,9 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
   // and tensor memory are released (on the normal path these waits return at
   // once; after an abort they wait, bounded, for copies and MMAs in flight).
   if (warp == 0 && lane == 0) {
-    for (int ai = a_issued > OZ_ASTAGES ? a_issued - OZ_ASTAGES : 0; ai < a_issued; ai++)
-      tc::mbar_wait(&a_full[ai % OZ_ASTAGES], (ai / OZ_ASTAGES) & 1, g.spin_limit, &no_abort);
-    for (int kc = b_issued > OZ_BBUFS ? b_issued - OZ_BBUFS : 0; kc < b_issued; kc++)
-      tc::mbar_wait(&b_full[kc % OZ_BBUFS], (kc / OZ_BBUFS) & 1, g.spin_limit, &no_abort);
+    const int from = issued > OZ_STAGES ? issued - OZ_STAGES : 0;
+    for (int kc = from; kc < issued; kc++)
+      tc::mbar_wait(&full[kc % OZ_STAGES], (kc / OZ_STAGES) & 1, g.spin_limit, &no_abort);
   }
   if (warp == 1 && lane == 0) tc::mbar_wait(&acc_full, 0, g.spin_limit, &no_abort);
   tc::tc_fence_before();
@@ -433,7 +419,7 @@ EncodeTiled encode_tiled() {
 }
 
 // Tensor map of `slices` int8 matrices of rows x Kp (K contiguous), read in
-// boxes of 128 (K) x box_rows x 1 with the 128-byte swizzle.
+// boxes of 32 (K) x box_rows x 1 with the 32-byte swizzle.
 cudaError_t slice_map(CUtensorMap* m, const int8_t* base, int Kp, int rows, int slices,
                       int box_rows) {
   EncodeTiled f = encode_tiled();
@@ -443,7 +429,7 @@ cudaError_t slice_map(CUtensorMap* m, const int8_t* base, int Kp, int rows, int 
   const cuuint32_t box[3] = {(cuuint32_t)OZ_BK, (cuuint32_t)box_rows, 1};
   const cuuint32_t es[3] = {1, 1, 1};
   const CUresult r = f(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<int8_t*>(base), dims,
-                       strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                       strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
