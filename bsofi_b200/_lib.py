@@ -124,6 +124,7 @@ _SIGS = {
     "bsofi_device_bsof_timeline": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
                                                   _vp, ctypes.c_int]),
     "bsofi_device_set_bsof_workers": (None, [ctypes.c_int]),
+    "bsofi_device_set_bsof_factor_warps": (None, [ctypes.c_int]),
     "bsofi_device_set_wait_test": (None, [ctypes.c_int]),
     "bsofi_device_set_bstri_overlap": (None, [ctypes.c_int]),
     "bsofi_device_timing": (None, [ctypes.c_int]),

@@ -1112,4 +1112,6 @@ void bsofi_device_set_bsof_workers(int workers) { bsofi_dev_set_bsof_workers(wor
 
 void bsofi_device_set_bstri_overlap(int on) { bsofi_dev_set_bstri_overlap(on); }
 
+void bsofi_device_set_bsof_factor_warps(int warps) { bsofi_dev_set_bsof_factor_warps(warps); }
+
 void bsofi_device_set_wait_test(int on) { bsofi_dev_set_wait_test(on); }

@@ -135,6 +135,9 @@ int bsofi_dev_timing_read(double *ms, long long *launches);
  * number of leaves. */
 int bsofi_dev_bsof_timeline(int n, int L, int ldd, void *dws, unsigned long long **ptr);
 void bsofi_dev_set_bsof_workers(int w);
+/* Factor warps of 16-wide BSOF leaves: 4 (default, the other 4 stage the next
+ * tile meanwhile) or 8; process-wide. */
+void bsofi_dev_set_bsof_factor_warps(int w);
 /* Diagnostics: persistent BSOI launches of this thread poll a word that
  * nothing writes in every step wait (short limit), so the waits give up. */
 void bsofi_dev_set_wait_test(int on);

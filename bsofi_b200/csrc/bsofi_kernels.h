@@ -48,6 +48,7 @@ cudaError_t launch_wy_apply(const WyArgs& a, int batch, cudaStream_t st);
 // a later launch continues with the counters the earlier one left, after
 // next_task is zeroed again.
 int bsof_leaf_width(int n);
+void bsof_set_factor_warps(int w);
 int bsof_tiles(int n);
 cudaError_t launch_bsof_persistent(double* A, long long ld, int n, int L, double* tau, double* T,
                                    double* G, int maxleaves, int* cnt, int* factored,

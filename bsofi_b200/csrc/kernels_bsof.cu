@@ -23,6 +23,7 @@
 // only on tasks earlier in that order and all CTAs are co-resident
 // (cooperative launch), so the schedule cannot deadlock; every spin is
 // bounded and sets an error word instead of hanging.
+#include <atomic>
 #include <climits>
 #include "bsofi_common.cuh"
 #include "bsofi_kernels.h"
@@ -655,7 +656,10 @@ BSOFI_DEVINL void apply_qt_mma8(double* sV, double* sC, const double (&a)[R][8],
   __syncthreads();
 }
 
-template <int R, int NB>
+// FW4: 16-wide leaves of at most 2 BT rows are factored by 4 warps while the
+// other 4 stage the next leaf's tile (true), or by all 8 warps with the tile
+// staged after the factorization (false).
+template <int R, int NB, bool FW4 = true>
 __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, BsofState st) {
   __shared__ Smem<NB> sm;
   extern __shared__ __align__(16) double sC[];  // NB x (R*BT) staged tile
@@ -670,7 +674,7 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
     // 4 warps meanwhile wait for the next leaf's tile to be ready and stage it
     // in shared memory for the update that follows (PREFETCH).  Taller leaves
     // use all warps for the factorization.
-    constexpr int FW = (NB == 16 && R <= 2) ? 4 : BW;
+    constexpr int FW = (FW4 && NB == 16 && R <= 2) ? 4 : BW;
     constexpr int FR = R * BW / FW;
     constexpr bool PREFETCH = NB == 16 && FW < BW && Pass<R>::NP == 1;
     const int warp = tid >> 5;
@@ -856,24 +860,29 @@ static size_t dyn_smem() {
                   : sizeof(double) * 2 * 8 * (size_t)Stage8<R>::S8;
 }
 
-template <int R, int NB>
+template <int R, int NB, bool FW4 = true>
 static cudaError_t launch_R(const BsofGeom& g, const BsofState& st, int grid, cudaStream_t s) {
   void* args[] = {(void*)&g, (void*)&st};
-  return cudaLaunchCooperativeKernel((const void*)bsof_persistent_kernel<R, NB>, dim3(grid),
+  return cudaLaunchCooperativeKernel((const void*)bsof_persistent_kernel<R, NB, FW4>, dim3(grid),
                                      dim3(BT), args, dyn_smem<R, NB>(), s);
 }
 
-template <int R, int NB>
+template <int R, int NB, bool FW4 = true>
 static int max_grid() {
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaFuncSetAttribute(bsof_persistent_kernel<R, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)dyn_smem<R, NB>());
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bsof_persistent_kernel<R, NB>, BT,
+  cudaFuncSetAttribute(bsof_persistent_kernel<R, NB, FW4>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem<R, NB>());
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bsof_persistent_kernel<R, NB, FW4>, BT,
                                                 dyn_smem<R, NB>());
   return sms * (per > 0 ? per : 1);
 }
+
+// Factor warps of 16-wide leaves: 4 with the next tile staged meanwhile (the
+// default), or 8; process-wide.
+static std::atomic<int> g_factor8{0};
+void bsof_set_factor_warps(int w) { g_factor8.store(w == 8 ? 1 : 0); }
 
 cudaError_t launch_bsof_persistent(double* A, long long ld, int n, int L, double* tau, double* T,
                                    double* G, int maxleaves, int* cnt, int* factored,
@@ -906,8 +915,20 @@ cudaError_t launch_bsof_persistent(double* A, long long ld, int n, int L, double
   int grid = 1 + workers;
   if (g.NB == 16) {
     switch (R) {
-      case 1: grid = min(grid, max_grid<1, 16>()); return launch_R<1, 16>(g, s, grid, st);
-      case 2: grid = min(grid, max_grid<2, 16>()); return launch_R<2, 16>(g, s, grid, st);
+      case 1:
+        if (g_factor8.load()) {
+          grid = min(grid, max_grid<1, 16, false>());
+          return launch_R<1, 16, false>(g, s, grid, st);
+        }
+        grid = min(grid, max_grid<1, 16>());
+        return launch_R<1, 16>(g, s, grid, st);
+      case 2:
+        if (g_factor8.load()) {
+          grid = min(grid, max_grid<2, 16, false>());
+          return launch_R<2, 16, false>(g, s, grid, st);
+        }
+        grid = min(grid, max_grid<2, 16>());
+        return launch_R<2, 16>(g, s, grid, st);
       default: return cudaErrorInvalidValue;
     }
   }
@@ -924,6 +945,8 @@ cudaError_t preload_bsof(size_t* local) {
   cudaError_t e;
   if ((e = preload_one(bsof_persistent_kernel<1, 16>, local)) != cudaSuccess) return e;
   if ((e = preload_one(bsof_persistent_kernel<2, 16>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(bsof_persistent_kernel<1, 16, false>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(bsof_persistent_kernel<2, 16, false>, local)) != cudaSuccess) return e;
   if ((e = preload_one(bsof_persistent_kernel<3, 8>, local)) != cudaSuccess) return e;
   if ((e = preload_one(bsof_persistent_kernel<4, 8>, local)) != cudaSuccess) return e;
   if ((e = preload_one(bsof_persistent_kernel<5, 8>, local)) != cudaSuccess) return e;

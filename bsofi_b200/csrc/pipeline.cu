@@ -1058,6 +1058,8 @@ int bsofi_dev_bsof_timeline(int n, int L, int ldd, void* dws, unsigned long long
 
 void bsofi_dev_set_bsof_workers(int w) { g_workers_override = w > 0 ? w : 0; }
 
+void bsofi_dev_set_bsof_factor_warps(int w) { bsof_set_factor_warps(w); }
+
 void bsofi_dev_set_wait_test(int on) { g_wait_test = on != 0; }
 
 void bsofi_dev_set_bstri_overlap(int on) { g_overlap_enabled.store(on ? 1 : 0); }

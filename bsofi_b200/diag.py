@@ -155,6 +155,11 @@ def invert_mixed_timing(n, L, reps=3, U=4.0, slices=0):
 
 
 def main(argv):
+    # --factor-warps=8: 16-wide BSOF leaves factored by all eight warps.
+    for a in list(argv):
+        if a.startswith("--factor-warps="):
+            _lib.load().bsofi_device_set_bsof_factor_warps(int(a.split("=", 1)[1]))
+            argv = [x for x in argv if x != a]
     if len(argv) >= 3 and argv[0] == "bsof-timeline":
         n, L = int(argv[1]), int(argv[2])
         reps = int(argv[3]) if len(argv) > 3 else 3

@@ -408,6 +408,11 @@ void bsofi_device_set_bsof_workers(int workers);
  * results are the same as without the split).  on = 0 turns this off for the
  * process, 1 (the default) on. */
 void bsofi_device_set_bstri_overlap(int on);
+/* Diagnostics (no reference counterpart): warps that factor a 16-wide leaf of
+ * the BSOF chain (n <= 256): 4 (the default; the CTA's other 4 warps stage the
+ * next leaf's tile meanwhile) or 8 (the tile is staged after the
+ * factorization).  Results are the same either way to rounding.  Process-wide. */
+void bsofi_device_set_bsof_factor_warps(int warps);
 /* Diagnostics (no reference counterpart): with on = 1, the persistent BSOI
  * launches made by this thread wait, in every step after the first, on a
  * zeroed workspace word that nothing writes, under a short poll limit (about
