@@ -126,10 +126,19 @@ __global__ void __launch_bounds__(OZ_SPLIT_THREADS) ozaki_split_kernel(OzSplitAr
       double mx = 0.0;
       bool bad = false;  // fmax drops NaN, so non-finite values are tracked apart
       if (i < s.M) {
-        for (int k = warp; k < s.K; k += 8) {
-          const double v = oz_a(s, i, k);
-          bad |= !isfinite(v);
-          mx = fmax(mx, fabs(v));
+        // Eight independent loads in flight per iteration (columns k, k+8, ...).
+        for (int k0 = warp; k0 < s.K; k0 += 64) {
+          double v[8];
+#pragma unroll
+          for (int j = 0; j < 8; j++) {
+            const int k = k0 + 8 * j;
+            v[j] = k < s.K ? oz_a(s, i, k) : 0.0;
+          }
+#pragma unroll
+          for (int j = 0; j < 8; j++) {
+            bad |= !isfinite(v[j]);
+            mx = fmax(mx, fabs(v[j]));
+          }
         }
       }
       s_max[warp][lane] = mx;
@@ -158,10 +167,14 @@ __global__ void __launch_bounds__(OZ_SPLIT_THREADS) ozaki_split_kernel(OzSplitAr
       __syncthreads();  // s_sc ready / the previous chunk consumed
       {
         const int i = r0 + lane;
-        for (int c = warp; c < OZ_SPLIT_CHUNK; c += 8) {
-          const int k = k0 + c;
-          s_blk[lane][c] = (i < s.M && k < s.K) ? oz_a(s, i, k) : 0.0;
+        double v[OZ_SPLIT_CHUNK / 8];  // all 16 loads of this warp in flight at once
+#pragma unroll
+        for (int j = 0; j < OZ_SPLIT_CHUNK / 8; j++) {
+          const int k = k0 + warp + 8 * j;
+          v[j] = (i < s.M && k < s.K) ? oz_a(s, i, k) : 0.0;
         }
+#pragma unroll
+        for (int j = 0; j < OZ_SPLIT_CHUNK / 8; j++) s_blk[lane][warp + 8 * j] = v[j];
       }
       __syncthreads();
 #pragma unroll 1
