@@ -3,6 +3,7 @@
     python -m bsofi_b200.diag bsof-timeline N_BLOCK L [REPS]
     python -m bsofi_b200.diag invert N_BLOCK L [REPS] [U]
     python -m bsofi_b200.diag invert-mixed N_BLOCK L [REPS] [SLICES]
+    python -m bsofi_b200.diag split-phases N_BLOCK L [REPS]
 
 bsof-timeline inverts a seeded Hubbard matrix (a random p-cyclic one when n is
 not a square) with bsofi_device_invert and prints, for the last run, the BSOF
@@ -154,6 +155,41 @@ def invert_mixed_timing(n, L, reps=3, U=4.0, slices=0):
             "bsoi_tflops": flops_bsoi(n, L) / bsoi / 1e9, "residual": res}
 
 
+def split_phases_timing(n, L, reps=2):
+    """bsofi_device_bsoftri then bsofi_device_bsoi as separate calls: BSOI then
+    forms every Q_k^T from the stored reflectors and tau (build_leaf_t_kernel,
+    wy_apply_kernel), as the split entry points of the reference's API do."""
+    import torch
+    side = int(round(n ** 0.5))
+    N = n * L
+    ldd = (N + 31) // 32 * 32
+    M = hubbard_matrix(side, L, 4.0, seed=1) if side * side == n else random_pcyclic(n, L, seed=1)
+    dev = torch.device("cuda:0")
+    src = torch.zeros((N, ldd), dtype=torch.float64, device=dev)
+    src[:, :N] = torch.from_numpy(np.ascontiguousarray(M.T)).to(dev)
+    dA = torch.empty_like(src)
+    dtau = torch.zeros(N, dtype=torch.float64, device=dev)
+    ws = torch.empty(api.workspace_bytes(n, L, ldd), dtype=torch.uint8, device=dev)
+    best = float("inf")
+    stream = torch.cuda.current_stream()
+    for r in range(reps + 1):
+        dA.copy_(src)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rc = api.device_bsoftri(n, L, dA.data_ptr(), ldd, dtau.data_ptr(), ws.data_ptr(),
+                                stream.cuda_stream)
+        rc = rc or api.device_bsoi(n, L, dA.data_ptr(), ldd, dtau.data_ptr(), ws.data_ptr(),
+                                   stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if rc != 0:
+            raise RuntimeError("split phases failed (%d)" % rc)
+        if r > 0:
+            best = min(best, e0.elapsed_time(e1))
+    return best
+
+
 def main(argv):
     # --factor-warps=8: 16-wide BSOF leaves factored by all eight warps.
     for a in list(argv):
@@ -188,6 +224,12 @@ def main(argv):
               "BSOI products %.3f ms = %.2f TFLOP/s effective FP64; residual %s"
               % (n, L, slices or 8, r["invert_ms"], r["tflops"], r["bsoi_ms"], r["bsoi_tflops"],
                  r["residual"]))
+        return 0
+    if len(argv) >= 3 and argv[0] == "split-phases":
+        n, L = int(argv[1]), int(argv[2])
+        reps = int(argv[3]) if len(argv) > 3 else 2
+        print("n %d L %d: bsoftri + bsoi as separate calls %.3f ms"
+              % (n, L, split_phases_timing(n, L, reps)))
         return 0
     print(__doc__)
     return 2
