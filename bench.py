@@ -71,6 +71,8 @@ def parse():
     p.add_argument("--serve-rate", type=float, default=16.0, help="mean arrivals per second")
     p.add_argument("--serve-mixed", type=float, default=0.5,
                    help="fraction of served requests at mixed precision")
+    p.add_argument("--serve-only", action="store_true",
+                   help="run only the served Poisson stream and print its JSON line")
     return p.parse_args()
 
 
@@ -288,6 +290,16 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=dev)
+
+    if args.serve_only:
+        served = run_serving(api, torch, dev, args.serve, args.serve_rate, 31 + rank,
+                             args.serve_mixed)
+        if rank == 0:
+            print(json.dumps({"metric": "served Poisson stream (inversions/s, p50/p99 latency)",
+                              "n_gpus": world, "served": served}))
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     side, L, U = args.side, args.L, args.U
     n = side * side

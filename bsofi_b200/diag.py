@@ -4,6 +4,7 @@
     python -m bsofi_b200.diag invert N_BLOCK L [REPS] [U]
     python -m bsofi_b200.diag invert-mixed N_BLOCK L [REPS] [SLICES]
     python -m bsofi_b200.diag split-phases N_BLOCK L [REPS]
+    python -m bsofi_b200.diag batch COUNT STREAMS [PRECISION]
 
 bsof-timeline inverts a seeded Hubbard matrix (a random p-cyclic one when n is
 not a square) with bsofi_device_invert and prints, for the last run, the BSOF
@@ -190,6 +191,54 @@ def split_phases_timing(n, L, reps=2):
     return best
 
 
+def batch_timing(count, streams, precision=0, reps=2, seed=77):
+    """The batched configuration (side in {8,..,16}, p in [8, 64], U in [2, 6]),
+    `count` instances per call with `streams` internal streams; inputs are
+    re-assembled from packed blocks before each timed call.  Returns the best
+    call's time in ms and the rate."""
+    import torch
+    from .hubbard import hubbard_blocks
+    rng = np.random.default_rng(seed)
+    specs = [(int(rng.choice([8, 10, 12, 14, 16])), int(rng.integers(8, 65)),
+              float(rng.uniform(2.0, 6.0)), 9000 + i) for i in range(count)]
+    dev = torch.device("cuda:0")
+    ns, Ls, lds, bufs, packs, taus = [], [], [], [], [], []
+    for side, L, U, sd in specs:
+        n = side * side
+        N = n * L
+        ld = (N + 31) // 32 * 32
+        B = hubbard_blocks(side, L, U, seed=sd)
+        sub = -B
+        sub[L - 1] = B[L - 1]
+        packs.append(torch.from_numpy(np.ascontiguousarray(np.transpose(sub, (0, 2, 1)))).to(dev))
+        bufs.append(torch.empty((N, ld), dtype=torch.float64, device=dev))
+        taus.append(torch.zeros(N, dtype=torch.float64, device=dev))
+        ns.append(n)
+        Ls.append(L)
+        lds.append(ld)
+    ws = torch.empty(api.batch_workspace_bytes(ns, Ls, lds, precision), dtype=torch.uint8,
+                     device=dev)
+    stream = torch.cuda.current_stream()
+    best = float("inf")
+    for r in range(reps + 1):
+        for n, L, b, pk, ld in zip(ns, Ls, bufs, packs, lds):
+            api.device_assemble(n, L, 0, pk.data_ptr(), b.data_ptr(), ld)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rc = api.device_invert_batched(ns, Ls, [b.data_ptr() for b in bufs], lds,
+                                       [t.data_ptr() for t in taus], ws.data_ptr(), streams,
+                                       stream.cuda_stream, precision)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if rc != 0:
+            raise RuntimeError("batched inversion failed (%d)" % rc)
+        if r > 0:
+            best = min(best, e0.elapsed_time(e1))
+    return best, count / (best * 1e-3)
+
+
 def main(argv):
     # --factor-warps=8: 16-wide BSOF leaves factored by all eight warps.
     for a in list(argv):
@@ -224,6 +273,13 @@ def main(argv):
               "BSOI products %.3f ms = %.2f TFLOP/s effective FP64; residual %s"
               % (n, L, slices or 8, r["invert_ms"], r["tflops"], r["bsoi_ms"], r["bsoi_tflops"],
                  r["residual"]))
+        return 0
+    if len(argv) >= 3 and argv[0] == "batch":
+        count, streams = int(argv[1]), int(argv[2])
+        precision = int(argv[3]) if len(argv) > 3 else 0
+        ms, rate = batch_timing(count, streams, precision)
+        print("batch of %d (streams %d, precision %d): %.1f ms = %.1f inversions/s"
+              % (count, streams, precision, ms, rate))
         return 0
     if len(argv) >= 3 and argv[0] == "split-phases":
         n, L = int(argv[1]), int(argv[2])
