@@ -66,12 +66,18 @@ static size_t inst_ws(int n, int L, int ldda, int precision) {
                         : bsofi_dev_ws_bytes(n, L, ldda);
 }
 
+/* FP64 batches run BSOI as one grouped persistent launch per tile shape (1,
+ * the default) or as one persistent launch per instance (0). */
+static int g_grouped = 1;
+void bsofi_device_set_batch_grouped(int on) { g_grouped = on ? 1 : 0; }
+
 unsigned long long bsofi_batch_workspace_bytes_ex(int count, const int *n, const int *L,
                                                   const int *ldda, int precision) {
   unsigned long long tot = 0;
   int i;
   if (precision != 0 && precision != 1) return 0;
   for (i = 0; i < count; i++) tot += align256(inst_ws(n[i], L[i], ldda[i], precision));
+  if (precision == 0) tot += align256(bsofi_dev_bsoi_group_bytes(count));
   return tot;
 }
 
@@ -88,6 +94,66 @@ typedef struct {
 static int by_cost_desc(const void *a, const void *b) {
   double x = ((const order_t *)a)->c, y = ((const order_t *)b)->c;
   return x < y ? 1 : (x > y ? -1 : 0);
+}
+
+/* Join the `used` pool streams into streams a and b (a == b allowed). */
+static cudaError_t join2(stream_pool *p, int used, cudaStream_t a, cudaStream_t b) {
+  cudaError_t e;
+  int i;
+  for (i = 0; i < used; i++) {
+    if ((e = cudaEventRecord(p->ev[i + 1], p->s[i])) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(a, p->ev[i + 1], 0)) != cudaSuccess) return e;
+    if (b != a && (e = cudaStreamWaitEvent(b, p->ev[i + 1], 0)) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+/* FP64 batch with a grouped BSOI: BSOF + BSTRI (forming every Q_k^T) and the
+ * first BSOI carry per instance over the pool streams; all streams joined;
+ * the grouped BSOI launches on pool streams 0 and 1; forked again for each
+ * instance's last BSOI copy.  Returns 0 or a cudaError_t value. */
+static int grouped_fp64(stream_pool *p, int used, int count, const int *n, const int *L,
+                        double *const *dA, const int *ldda, double *const *dtau, void *dwork,
+                        const order_t *ord, const size_t *off, long long *launches) {
+  void **ws = (void **)malloc(sizeof(void *) * count);
+  cudaStream_t a = p->s[0], b = p->s[used > 1 ? 1 : 0];
+  size_t end = 0;
+  cudaError_t e;
+  int i, r = 0;
+  if (!ws) return (int)cudaErrorMemoryAllocation;
+  for (i = 0; i < count; i++) {
+    ws[i] = (char *)dwork + off[i];
+    end = off[i] + align256(inst_ws(n[i], L[i], ldda[i], 0)) > end
+              ? off[i] + align256(inst_ws(n[i], L[i], ldda[i], 0))
+              : end;
+  }
+  for (i = 0; i < count && !r; i++) {
+    const int k = ord[i].i;
+    const int workers = n[k] <= 256 ? 6 : 24;
+    r = bsofi_dev_bsoftri_q_ex(n[k], L[k], dA[k], ldda[k], dtau[k], ws[k], p->s[i % used],
+                               workers);
+    *launches += bsofi_dev_launch_count();
+    if (!r) r = bsofi_dev_bsoi_group_prepare(n[k], L[k], dA[k], ldda[k], ws[k], p->s[i % used]);
+    *launches += 1;
+  }
+  if (!r && (e = join2(p, used, a, b)) != cudaSuccess) r = (int)e;
+  if (!r) {
+    r = bsofi_dev_bsoi_group_run(count, n, L, dA, ldda, ws, (char *)dwork + end, a, b);
+    *launches += bsofi_dev_launch_count();
+  }
+  /* fork: every stream waits for both grouped launches */
+  if (!r && (e = cudaEventRecord(p->ev[1], a)) != cudaSuccess) r = (int)e;
+  if (!r && b != a && (e = cudaEventRecord(p->ev[2], b)) != cudaSuccess) r = (int)e;
+  for (i = 0; i < used && !r; i++) {
+    if ((e = cudaStreamWaitEvent(p->s[i], p->ev[1], 0)) != cudaSuccess) r = (int)e;
+    else if (b != a && (e = cudaStreamWaitEvent(p->s[i], p->ev[2], 0)) != cudaSuccess) r = (int)e;
+  }
+  for (i = 0; i < count && !r; i++) {
+    r = bsofi_dev_bsoi_group_finish(n[i], L[i], dA[i], ldda[i], ws[i], p->s[i % used]);
+    *launches += 1;
+  }
+  free(ws);
+  return r;
 }
 
 int bsofi_device_invert_batched(int count, const int *n, const int *L, double *const *dA,
@@ -137,7 +203,14 @@ int bsofi_device_invert_batched_ex(int count, const int *n, const int *L, double
   if ((e = cudaEventRecord(p->ev[0], (cudaStream_t)stream)) != cudaSuccess) goto fail;
   for (i = 0; i < used; i++)
     if ((e = cudaStreamWaitEvent(p->s[i], p->ev[0], 0)) != cudaSuccess) goto fail;
-  for (i = 0; i < count; i++) {
+  if (precision == 0 && g_grouped) {
+    r = grouped_fp64(p, used, count, n, L, dA, ldda, dtau, dwork, ord, off, &launches);
+    if (r) {
+      e = (cudaError_t)r;
+      goto fail;
+    }
+  }
+  for (i = 0; i < count && !(precision == 0 && g_grouped); i++) {
     const int k = ord[i].i;
     /* Few BSOF workers per instance: the batch supplies the parallelism. */
     const int workers = n[k] <= 256 ? 6 : 24;

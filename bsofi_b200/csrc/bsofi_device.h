@@ -60,6 +60,22 @@ int bsofi_dev_selftest_ozaki(int M, int N, int K, const double *dA, int lda, con
                              int ldb, double *dC, int ldc, int slices, void *scratch, int *derr,
                              void *stream);
 
+/* BSOI of a whole batch in one persistent launch per tile shape (per 256
+ * instances).  bsoftri_q_ex: BSOF (forming every Q_k^T) + BSTRI with `workers`
+ * BSOF worker CTAs and no side streams; group_prepare: the instance's first
+ * carry and zeroed BSOI counters; group_run: the grouped launches (64 x 64
+ * tiles on stream_small, 128 x 128 on stream_large), gws holding
+ * bsofi_dev_bsoi_group_bytes(count) device bytes; group_finish: the
+ * instance's column block 0 and its info word. */
+int bsofi_dev_bsoftri_q_ex(int n, int L, double *dA, int ldd, double *dtau, void *dws,
+                           void *stream, int workers);
+int bsofi_dev_bsoi_group_prepare(int n, int L, double *dA, int ldd, void *dws, void *stream);
+size_t bsofi_dev_bsoi_group_bytes(int count);
+int bsofi_dev_bsoi_group_run(int count, const int *n, const int *L, double *const *dA,
+                             const int *ldd, void *const *dws, void *gws, void *stream_small,
+                             void *stream_large);
+int bsofi_dev_bsoi_group_finish(int n, int L, double *dA, int ldd, void *dws, void *stream);
+
 /* BSOI: A (reflectors + R^{-1}) <- M^{-1}. */
 int bsofi_dev_bsoi(int n, int L, double *dA, int ldd, const double *dtau, void *dws,
                    void *stream);

@@ -82,6 +82,35 @@ cudaError_t launch_bsoi_persistent(double* A, long long ld, double* carry0, doub
                                    int* next, int* err, bool small, cudaStream_t st,
                                    int row0 = 0, int row1 = -1, const int* never = nullptr);
 
+// BSOI of many instances in one persistent launch (kernels_bsoi.cu).  Each
+// instance: its matrix, carries, G_k, sizes, its done counters ((L-1) *
+// bsoi_row_bands(N) ints, zeroed) and BSOI error word, and the global index
+// of its first tile (prefix sums of bsoi_group_tiles, instance order).
+struct BsoiInst {
+  double* A;
+  long long ld;
+  double* carry[2];
+  long long ldc;
+  const double* G;
+  int n, L, N;
+  int* done;
+  int* err;
+  long long tile0;
+};
+// Passed by value as the kernel's (__grid_constant__) parameter: up to
+// kBsoiGroupMax instances per launch (kernel parameters may take 32,764 bytes).
+constexpr int kBsoiGroupMax = 256;
+struct BsoiGroup {
+  BsoiInst inst[kBsoiGroupMax];
+  int count;
+  long long total;           // tiles of all instances
+  unsigned long long* next;  // tile counter, zeroed
+  long long spin_limit;
+};
+static_assert(sizeof(BsoiGroup) <= 32764, "kernel parameter limit");
+long long bsoi_group_tiles(int n, int L, bool small);
+cudaError_t launch_bsoi_grouped(const BsoiGroup& g, bool small, bool aligned, cudaStream_t st);
+
 // In-place inversion of the upper triangles of nblk n x n blocks (block b at
 // A + b * bstride); tmp: device scratch of nblk * n * n / 4 doubles.  A zero
 // diagonal is reported as the global index of diagonal block boff + b.

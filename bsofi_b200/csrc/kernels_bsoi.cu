@@ -175,8 +175,135 @@ cudaError_t launch_bsoi_persistent(double* A, long long ld, double* carry0, doub
   return al ? launch_al<CfgM, true>(s, st) : launch_al<CfgM, false>(s, st);
 }
 
+// ------------------------------------------------------------------ grouped
+// BSOI of many independent instances in one persistent launch.  The tiles of
+// all instances form one queue: instance by instance, each instance's tiles
+// in the (step, row band, column) order of bsoi_persistent_kernel.  A tile
+// waits only for tiles of its own instance claimed before it, whose CTAs are
+// already running, so progress needs no co-residency; while the last steps of
+// one instance finish, idle CTAs claim the next instance's tiles instead of
+// idling at a launch boundary.
+template <class Cfg, bool ALIGNED>
+__global__ void __launch_bounds__(Cfg::THREADS, 1)
+    bsoi_grouped_kernel(const __grid_constant__ BsoiGroup g) {
+  extern __shared__ __align__(16) double smem_bsoig[];
+  __shared__ long long s_tile;
+  __shared__ int s_inst, s_ok;
+  for (;;) {
+    __syncthreads();  // the previous tile's shared memory is no longer read
+    if (threadIdx.x == 0) {
+      const long long t = atomicAdd(g.next, 1ull);
+      int lo = 0, hi = g.count - 1;  // last instance with tile0 <= t
+      if (t < g.total) {
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) / 2;
+          if (g.inst[mid].tile0 <= (long long)t) lo = mid;
+          else hi = mid - 1;
+        }
+      }
+      s_tile = (long long)t;
+      s_inst = lo;
+    }
+    __syncthreads();
+    const long long tile = s_tile;
+    if (tile >= g.total) return;
+    const BsoiInst& I = g.inst[s_inst];
+    const int n2 = 2 * I.n;
+    const int RT = (I.N + Cfg::BM - 1) / Cfg::BM, CT = (n2 + Cfg::BN - 1) / Cfg::BN;
+    const long long local = tile - I.tile0;
+    const int step = (int)(local / ((long long)RT * CT));  // 0 = k = L-2
+    const int rem = (int)(local % ((long long)RT * CT));
+    const int rb = rem / CT, cb = rem % CT;
+    const int k = I.L - 2 - step;
+    if (step > 0) {
+      if (threadIdx.x == 0) {
+        const int* flag = I.done + (long long)(step - 1) * RT + rb;
+        long long it = 0;
+        int ok = 1;
+        while (ld_acq(flag) < CT) {
+          if (ld_acq(I.err) != 0 || ++it > g.spin_limit) {
+            atomicExch(I.err, 1);
+            ok = 0;
+            break;
+          }
+          __nanosleep(64);
+        }
+        s_ok = ok;
+      }
+      __syncthreads();
+      if (!s_ok) continue;  // this instance failed; its info word reports it
+    }
+    GemmDims d = {I.N, n2, n2};
+    GemmA a;
+    a.p0 = I.A + cm(0, (long long)k * I.n, I.ld);
+    a.ld0 = I.ld;
+    a.p1 = I.carry[(I.L - 2 - k) & 1];
+    a.ld1 = I.ldc;
+    a.bs0 = a.bs1 = 0;
+    a.ksplit = I.n;
+    a.rlim0 = (k + 1) * I.n;
+    a.roff0 = k * I.n;
+    a.rlim1 = INT_MAX;
+    a.roff1 = kNoMask;
+    GemmB b = {I.G + (long long)k * n2 * n2, n2, 0, kNoMask};
+    GemmC c;
+    c.p0 = I.carry[(I.L - 1 - k) & 1];
+    c.ld0 = I.ldc;
+    c.p1 = I.A + cm(0, (long long)(k + 1) * I.n, I.ld);
+    c.ld1 = I.ld;
+    c.bs0 = c.bs1 = 0;
+    c.nsplit = I.n;
+    c.alpha = 1.0;
+    c.beta0 = c.beta1 = 0.0;
+    gemm_tile<Cfg, ALIGNED>(d, a, b, c, rb * Cfg::BM, cb * Cfg::BN, 0, smem_bsoig);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(I.done + (long long)step * RT + rb)
+                   : "memory");
+    }
+  }
+}
+
+long long bsoi_group_tiles(int n, int L, bool small) {
+  const int BM = small ? CfgS::BM : CfgM::BM, BN = small ? CfgS::BN : CfgM::BN;
+  return (long long)(L - 1) * ((n * L + BM - 1) / BM) * ((2 * n + BN - 1) / BN);
+}
+
+template <class Cfg, bool AL>
+static cudaError_t group_launch(const BsoiGroup& g, cudaStream_t st) {
+  static PerDevice once;
+  const int pend = once.pending();
+  if (pend >= 0) {
+    cudaError_t e = cudaFuncSetAttribute(bsoi_grouped_kernel<Cfg, AL>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)Cfg::SMEM);
+    if (e != cudaSuccess) return e;
+    once.mark(pend);
+  }
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bsoi_grouped_kernel<Cfg, AL>, Cfg::THREADS,
+                                                Cfg::SMEM);
+  long long grid = (long long)sms * (per > 0 ? per : 1);
+  if (g.total < grid) grid = g.total;
+  if (grid < 1) return cudaSuccess;
+  bsoi_grouped_kernel<Cfg, AL><<<(int)grid, Cfg::THREADS, Cfg::SMEM, st>>>(g);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bsoi_grouped(const BsoiGroup& g, bool small, bool aligned, cudaStream_t st) {
+  if (small) return aligned ? group_launch<CfgS, true>(g, st) : group_launch<CfgS, false>(g, st);
+  return aligned ? group_launch<CfgM, true>(g, st) : group_launch<CfgM, false>(g, st);
+}
+
 cudaError_t preload_bsoi(size_t* local) {
   cudaError_t e;
+  if ((e = preload_one(bsoi_grouped_kernel<CfgM, true>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(bsoi_grouped_kernel<CfgM, false>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(bsoi_grouped_kernel<CfgS, true>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(bsoi_grouped_kernel<CfgS, false>, local)) != cudaSuccess) return e;
   if ((e = preload_one(bsoi_persistent_kernel<CfgM, true>, local)) != cudaSuccess) return e;
   if ((e = preload_one(bsoi_persistent_kernel<CfgM, false>, local)) != cudaSuccess) return e;
   if ((e = preload_one(bsoi_persistent_kernel<CfgS, true>, local)) != cudaSuccess) return e;

@@ -901,6 +901,90 @@ int bsofi_dev_invert_mixed(int n, int L, double* dA, int ldd, double* dtau, void
   return run_bsoi_mixed(n, L, dA, ldd, dws, oz, slices, (cudaStream_t)stream);
 }
 
+int bsofi_dev_bsoftri_q_ex(int n, int L, double* dA, int ldd, double* dtau, void* dws,
+                           void* stream, int workers) {
+  g_launches = 0;
+  return run_bsoftri(n, L, dA, ldd, dtau, dws, (cudaStream_t)stream, true,
+                     bsof_workers(n, L, workers), false);
+}
+
+int bsofi_dev_bsoi_group_prepare(int n, int L, double* dA, int ldd, void* dws, void* stream) {
+  const Layout ly = layout(n, L, ldd);
+  int e = bsoi_carry(n, L, dA, ldd, dws, (cudaStream_t)stream);
+  if (e) return e;
+  CKM(cudaMemsetAsync(at<int>(dws, ly.bsync), 0, sizeof(int) * ly.bsync_ints,
+                      (cudaStream_t)stream));
+  return 0;
+}
+
+int bsofi_dev_bsoi_group_finish(int n, int L, double* dA, int ldd, void* dws, void* stream) {
+  return bsoi_finish(n, L, dA, ldd, dws, (cudaStream_t)stream);
+}
+
+// Tile counters of the grouped launches: at most two tile shapes, each in
+// chunks of kBsoiGroupMax instances.
+static int group_launches_max(int count) { return 2 * ((count + kBsoiGroupMax - 1) / kBsoiGroupMax); }
+
+size_t bsofi_dev_bsoi_group_bytes(int count) {
+  return align256(sizeof(unsigned long long) * (size_t)group_launches_max(count));
+}
+
+int bsofi_dev_bsoi_group_run(int count, const int* n, const int* L, double* const* dA,
+                             const int* ldd, void* const* dws, void* gws, void* stream_small,
+                             void* stream_large) {
+  // Instances with 2n a multiple of 128 run on 128 x 128 tiles, the others on
+  // 64 x 64 tiles (the persistent single-instance plans choose the same way);
+  // each tile shape on its own stream, kBsoiGroupMax instances per launch, the
+  // descriptors in the launch's parameters (so the launches need no host
+  // staging and can be captured into a graph).
+  static thread_local BsoiGroup grp[2];
+  g_launches = 0;
+  unsigned long long* counters = static_cast<unsigned long long*>(gws);
+  cudaStream_t sts[2] = {(cudaStream_t)stream_small, (cudaStream_t)stream_large};
+  int used = 0;
+  for (int g = 0; g < 2; g++) {
+    BsoiGroup& G = grp[g];
+    G.count = 0;
+    G.total = 0;
+    bool al = true;
+    for (int i = 0; i <= count; i++) {
+      if (i == count || G.count == kBsoiGroupMax) {
+        if (G.count > 0) {  // launch the chunk gathered so far
+          if (used >= group_launches_max(count)) return (int)cudaErrorInvalidValue;
+          G.next = counters + used++;
+          G.spin_limit = 1ll << 22;
+          CKM(cudaMemsetAsync(G.next, 0, sizeof(unsigned long long), sts[g]));
+          CK(launch_bsoi_grouped(G, g == 0, al, sts[g]));
+        }
+        G.count = 0;
+        G.total = 0;
+        al = true;
+        if (i == count) break;
+      }
+      if (((2 * n[i]) % 128 == 0 ? 1 : 0) != g) continue;
+      const Layout ly = layout(n[i], L[i], ldd[i]);
+      BsoiInst& I = G.inst[G.count++];
+      I.A = dA[i];
+      I.ld = ldd[i];
+      I.carry[0] = at<double>(dws[i], ly.C0);
+      I.carry[1] = at<double>(dws[i], ly.C1);
+      I.ldc = ldd[i];
+      I.G = at<double>(dws[i], ly.G);
+      I.n = n[i];
+      I.L = L[i];
+      I.N = n[i] * L[i];
+      I.done = at<int>(dws[i], ly.bsync);
+      I.err = at<int>(dws[i], ly.info) + 2;
+      I.tile0 = G.total;
+      G.total += bsoi_group_tiles(n[i], L[i], g == 0);
+      al = al && ((uintptr_t)I.A % 16 == 0) && ((uintptr_t)I.carry[0] % 16 == 0) &&
+           ((uintptr_t)I.carry[1] % 16 == 0) && ((uintptr_t)I.G % 16 == 0) && I.ld % 2 == 0 &&
+           I.n % 2 == 0;
+    }
+  }
+  return 0;
+}
+
 size_t bsofi_dev_ozaki_scratch_bytes(int M, int N, int K, int slices) {
   return ozaki_scratch_bytes(M, N, K, slices);
 }

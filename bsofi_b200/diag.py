@@ -240,6 +240,11 @@ def batch_timing(count, streams, precision=0, reps=2, seed=77):
 
 
 def main(argv):
+    # --grouped=0: FP64 batches run each instance's BSOI as its own launch.
+    for a in list(argv):
+        if a.startswith("--grouped="):
+            _lib.load().bsofi_device_set_batch_grouped(int(a.split("=", 1)[1]))
+            argv = [x for x in argv if x != a]
     # --factor-warps=8: 16-wide BSOF leaves factored by all eight warps.
     for a in list(argv):
         if a.startswith("--factor-warps="):

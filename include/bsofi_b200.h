@@ -250,6 +250,12 @@ unsigned long long bsofi_batch_workspace_bytes(int count, const int *n, const in
 int bsofi_device_invert_batched(int count, const int *n, const int *L, double *const *dA,
                                 const int *ldda, double *const *dtau, void *dwork, int streams,
                                 void *stream);
+/* FP64 batches run BSOF + BSTRI of each instance over the stream pool, then
+ * BSOI of all instances as one persistent launch per tile shape over one
+ * queue of every instance's tiles (at most 256 instances per launch), then
+ * each instance's last BSOI copy.  Diagnostics (no reference counterpart):
+ * on = 0 runs each instance's BSOI as its own launch instead; process-wide. */
+void bsofi_device_set_batch_grouped(int on);
 /* The same batch at a chosen precision: 0 FP64 (as above), 1 mixed (every
  * instance as bsofi_device_invert_mixed with BSOFI_MIXED_SLICES slices).  The
  * workspace query returns 0 for an unknown precision. */

@@ -83,3 +83,44 @@ def test_batch_graph_replays_match_direct(cuda_device):
             assert rel_fro(X, Xd) < inverse_tolerance(M, Xd)
             assert residual(M, X) < 1e-13
     g.close()
+
+
+def test_grouped_bsoi_matches_per_instance(cuda_device):
+    """FP64 batches run BSOI as one grouped persistent launch per tile shape
+    (64 x 64 for 2n not a multiple of 128, 128 x 128 otherwise; at most 256
+    instances per launch).  300 instances of mixed sizes (so both tile shapes
+    and two launches of the 64 x 64 shape) against the same batch with each
+    instance's BSOI launched on its own: equal within the FP64 tolerance, with
+    small residuals."""
+    import torch
+    from gpu_util import from_device_colmajor, to_device_colmajor
+    lib = api.load()
+    rng = np.random.default_rng(123)
+    specs = [(int(rng.choice([8, 12, 16, 20, 32, 64, 17])), int(rng.integers(2, 9)))
+             for _ in range(300)]
+    mats = [random_pcyclic(n, L, seed=1000 + i) for i, (n, L) in enumerate(specs)]
+    ns = [n for n, _ in specs]
+    Ls = [L for _, L in specs]
+    lds = [n * L + (i % 3) for i, (n, L) in enumerate(specs)]
+
+    def run(grouped):
+        lib.bsofi_device_set_batch_grouped(grouped)
+        try:
+            dA = [to_device_colmajor(torch, M, ld=ld, device=cuda_device)
+                  for M, ld in zip(mats, lds)]
+            dtau = [torch.zeros(n * L, dtype=torch.float64, device=cuda_device) for n, L in specs]
+            ws = torch.zeros(api.batch_workspace_bytes(ns, Ls, lds) // 8 + 1, dtype=torch.float64,
+                             device=cuda_device)
+            rc = api.device_invert_batched(ns, Ls, [t.data_ptr() for t in dA], lds,
+                                           [t.data_ptr() for t in dtau], ws.data_ptr(), streams=8)
+            torch.cuda.synchronize()
+            assert rc == 0
+            return [from_device_colmajor(A, n * L) for A, (n, L) in zip(dA, specs)]
+        finally:
+            lib.bsofi_device_set_batch_grouped(1)
+
+    Xg = run(1)
+    Xp = run(0)
+    for M, a, b in zip(mats, Xg, Xp):
+        assert rel_fro(a, b) < inverse_tolerance(M, b)
+        assert residual(M, a) < 1e-13
