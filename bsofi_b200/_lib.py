@@ -117,6 +117,17 @@ _SIGS = {
                                                      ctypes.c_double, _vp, ctypes.c_int, _vp]),
     "bsofi_device_logdet": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp,
                                            ctypes.c_int, _vp, _vp]),
+    "bsofi_shard_state_bytes": (ctypes.c_ulonglong, [ctypes.c_int] * 2),
+    "bsofi_shard_factor": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]),
+    "bsofi_shard_hubbard_factor": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp,
+                                                  ctypes.c_double, _vp, _vp]),
+    "bsofi_shard_bstri_columns": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.c_int, _vp, ctypes.c_longlong, _vp, _vp]),
+    "bsofi_shard_bsoi_rows": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_int, _vp, ctypes.c_longlong, _vp, _vp]),
+    "bsofi_shard_logdet": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
+    "bsofi_shard_info": (_vp, [_vp]),
+    "bsofi_shard_tau": (_vp, [_vp, ctypes.c_int, ctypes.c_int]),
     "bsofi_noalloc_scratch_bytes": (ctypes.c_ulonglong, []),
     "bsofi_noalloc_prepare": (ctypes.c_int, []),
     "bsofi_device_invert_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int,
@@ -143,7 +154,7 @@ def declared_symbols(header=HEADER):
     """Function names declared in include/bsofi_b200.h."""
     text = open(header).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"^\s*(?:unsigned\s+long\s+long|long\s+long|int\s*\*?|double|void|bsofi_\w+)\s*\*?\s*(\w+)\s*\(",
+    return sorted(set(re.findall(r"^\s*(?:unsigned\s+long\s+long|long\s+long|int\s*\*?|(?:const\s+)?double|void|bsofi_\w+)\s*\*?\s*(\w+)\s*\(",
                                  text, flags=re.M)))
 
 

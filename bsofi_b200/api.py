@@ -125,6 +125,51 @@ def device_bsoi_rows(n, L, dA, ldda, dtau, dwork, row0, row1, stream=0):
     return load().bsofi_device_bsoi_rows(n, L, dA, ldda, dtau, dwork, row0, row1, stream)
 
 
+def shard_state_bytes(n, L):
+    """Bytes of one rank's state for the storage-sharded inversion."""
+    return int(load().bsofi_shard_state_bytes(n, L))
+
+
+def shard_factor(n, L, dD, dS, dstate, stream=0):
+    """bsofi_shard_factor: compact factorization state from packed blocks."""
+    return load().bsofi_shard_factor(n, L, dD or None, dS, dstate, stream)
+
+
+def shard_hubbard_factor(n, L, dExpK, dh, lam, dstate, stream=0):
+    """bsofi_shard_hubbard_factor: compact state from expm(K) and the fields."""
+    return load().bsofi_shard_hubbard_factor(n, L, dExpK, dh, lam, dstate, stream)
+
+
+def shard_bstri_columns(n, L, c0, c1, dX, ldx, dstate, stream=0):
+    """bsofi_shard_bstri_columns: block columns [c0, c1) of R^{-1} into dX."""
+    return load().bsofi_shard_bstri_columns(n, L, c0, c1, dX, ldx, dstate, stream)
+
+
+def shard_bsoi_rows(n, L, row0, row1, dB, ldb, dstate, stream=0):
+    """bsofi_shard_bsoi_rows: rows [row0, row1) of M^{-1} in place in dB."""
+    return load().bsofi_shard_bsoi_rows(n, L, row0, row1, dB, ldb, dstate, stream)
+
+
+def shard_logdet(n, L, dstate, dout, stream=0):
+    """bsofi_shard_logdet: dout[0] = sign(det M), dout[1] = log|det M|."""
+    return load().bsofi_shard_logdet(n, L, dstate, dout, stream)
+
+
+def shard_info(state, n, L):
+    """The info word of a storage-sharded state (a torch uint8 device
+    tensor); synchronises with the device."""
+    import torch
+    del n, L
+    torch.cuda.synchronize()
+    ptr = load().bsofi_shard_info(state.data_ptr())
+    out = torch.empty(1, dtype=torch.int32)
+    base = state.data_ptr()
+    off = (ptr - base) // 4
+    out.copy_(state.view(torch.int32)[off:off + 1])
+    v = int(out.item())
+    return 0 if v >= 0x7f7f7f7f else v
+
+
 def device_assemble(n, L, dD, dS, dA, ldda, stream=0):
     """bsofi_device_assemble: p-cyclic input from packed blocks (dD may be 0 = identity)."""
     return load().bsofi_device_assemble(n, L, dD or None, dS, dA, ldda, stream)

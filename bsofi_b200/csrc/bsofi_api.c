@@ -1033,6 +1033,69 @@ int bsofi_device_bsoi_rows(int n, int L, double *dA, int ldda, const double *dta
   return e ? cuda_info((cudaError_t)e) : 0;
 }
 
+/* ---------------------------------------------- storage-sharded inversion */
+
+unsigned long long bsofi_shard_state_bytes(int n, int L) {
+  if (n < 1 || n > BSOFI_MAX_BLOCK || L < 2) return 0;
+  return (unsigned long long)bsofi_dev_shard_state_bytes(n, L);
+}
+
+static int shard_run(int e) { return e ? cuda_info((cudaError_t)e) : 0; }
+
+int bsofi_shard_factor(int n, int L, const double *dD, const double *dS, void *dstate,
+                       void *stream) {
+  int e;
+  if (n < 1 || n > BSOFI_MAX_BLOCK || L < 2 || dS == NULL || dstate == NULL) return -1;
+  e = bsofi_dev_prepare();
+  if (!e) e = bsofi_dev_shard_factor(n, L, dD, dS, NULL, NULL, 0.0, dstate, stream);
+  return shard_run(e);
+}
+
+int bsofi_shard_hubbard_factor(int n, int L, const double *dExpK, const double *dh,
+                               double lambda, void *dstate, void *stream) {
+  int e;
+  if (n < 1 || n > BSOFI_MAX_BLOCK || L < 2 || dExpK == NULL || dh == NULL || dstate == NULL)
+    return -1;
+  e = bsofi_dev_prepare();
+  if (!e) e = bsofi_dev_shard_factor(n, L, NULL, NULL, dExpK, dh, lambda, dstate, stream);
+  return shard_run(e);
+}
+
+int bsofi_shard_bstri_columns(int n, int L, int c0, int c1, double *dX, long long ldx,
+                              void *dstate, void *stream) {
+  int e;
+  if (n < 1 || n > BSOFI_MAX_BLOCK || L < 2 || c0 < 0 || c1 > L || c0 >= c1 || dX == NULL ||
+      dstate == NULL || ldx < (long long)c1 * n)
+    return -1;
+  e = bsofi_dev_prepare();
+  if (!e) e = bsofi_dev_shard_bstri_columns(n, L, c0, c1, dX, ldx, dstate, stream);
+  return shard_run(e);
+}
+
+int bsofi_shard_bsoi_rows(int n, int L, int row0, int row1, double *dB, long long ldb,
+                          void *dstate, void *stream) {
+  int e, N = n * L;
+  if (n < 1 || n > BSOFI_MAX_BLOCK || L < 2 || dB == NULL || dstate == NULL) return -1;
+  if (row0 < 0 || row1 > N || row0 >= row1 || row0 % 128 != 0 || (row1 % 128 != 0 && row1 != N) ||
+      ldb < row1 - row0)
+    return -1;
+  e = bsofi_dev_prepare();
+  if (!e) e = bsofi_dev_shard_bsoi_rows(n, L, row0, row1, dB, ldb, dstate, stream);
+  return shard_run(e);
+}
+
+int bsofi_shard_logdet(int n, int L, const void *dstate, double *dout, void *stream) {
+  if (n < 1 || n > BSOFI_MAX_BLOCK || L < 2 || dstate == NULL || dout == NULL) return -1;
+  return shard_run(bsofi_dev_shard_logdet(n, L, dstate, dout, stream));
+}
+
+int *bsofi_shard_info(void *dstate) { return dstate ? bsofi_dev_info_ptr(dstate) : NULL; }
+
+const double *bsofi_shard_tau(const void *dstate, int n, int L) {
+  if (dstate == NULL || n < 1 || n > BSOFI_MAX_BLOCK || L < 2) return NULL;
+  return bsofi_dev_shard_tau(dstate, n, L);
+}
+
 int bsofi_device_invert(int n, int L, double *dA, int ldda, double *dtau, void *dwork,
                         void *stream) {
   int e;

@@ -93,6 +93,35 @@ int bsofi_dev_bsoi_ex(int n, int L, double *dA, int ldd, const double *dtau, voi
 int bsofi_dev_bsoi_rows(int n, int L, double *dA, int ldd, const double *dtau, void *dws,
                         void *stream, int row0, int row1);
 
+/* Storage-sharded inversion (one inversion over several GPUs, none holding M
+ * or M^{-1} whole).  The state (bsofi_dev_shard_state_bytes) holds the
+ * compact factorization: block columns 0..L-2 with leading dimension 3n, the
+ * last block column as an N x n array, tau, and the pipeline workspace.
+ * shard_factor: compact input (packed blocks, or Hubbard when dExpK is set)
+ * -> BSOF with every Q_k^T, the diagonal inverses, Z_i and W_i.
+ * shard_bstri_columns: block columns [c0, c1) of X = R^{-1}, rows 0..c1 n - 1,
+ * into dX (leading dimension ldx >= c1 n).
+ * shard_bsoi_rows: dB holds rows [r0, r1) of X in all N columns (leading
+ * dimension ldb >= r1 - r0) and receives the same rows of M^{-1}; r0 a
+ * multiple of 128, r1 too unless it is N. */
+size_t bsofi_dev_shard_state_bytes(int n, int L);
+int bsofi_dev_shard_factor(int n, int L, const double *dD, const double *dS,
+                           const double *dExpK, const double *dh, double lambda, void *dstate,
+                           void *stream);
+int bsofi_dev_shard_bstri_columns(int n, int L, int c0, int c1, double *dX, long long ldx,
+                                  void *dstate, void *stream);
+int bsofi_dev_shard_bsoi_rows(int n, int L, int r0, int r1, double *dB, long long ldb,
+                              void *dstate, void *stream);
+/* Sign and log|det M| (dout[0], dout[1]) from the state of shard_factor. */
+int bsofi_dev_shard_logdet(int n, int L, const void *dstate, double *dout, void *stream);
+const double *bsofi_dev_shard_tau(const void *dstate, int n, int L);
+/* Compact assembly and log-determinant (kernels_dqmc.cu). */
+int bsofi_dev_assemble_compact(int n, int L, const double *dD, const double *dS,
+                               const double *dExpK, const double *dh, double lambda,
+                               double *band, size_t band_doubles, double *last, void *stream);
+int bsofi_dev_logdet_compact(int n, int L, const double *band, const double *last,
+                             const double *tau, int inverted, double *out, void *stream);
+
 /* The reflector rows of every block column and tau (what Q formation reads):
  * mode 0 packs them into ref (bsofi_dev_state_ref_doubles doubles), mode 1
  * compares them with ref and sets the device int *dflag to 1 on a difference. */

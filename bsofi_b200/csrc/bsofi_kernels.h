@@ -46,7 +46,9 @@ cudaError_t launch_wy_apply(const WyArgs& a, int batch, cudaStream_t st);
 // the launch.  G (optional): (L-1) x (2n)^2 identity matrices that become
 // Q_k^T.  [s_begin, s_end): the leaves this launch factors (-1: to the end);
 // a later launch continues with the counters the earlier one left, after
-// next_task is zeroed again.
+// next_task is zeroed again.  Al, ldl (optional): the last block column in
+// its own array (rows 0..N-1), with block columns 0..L-2 at A; without them
+// it is A's block column L-1.
 int bsof_leaf_width(int n);
 void bsof_set_factor_warps(int w);
 int bsof_tiles(int n);
@@ -54,7 +56,7 @@ cudaError_t launch_bsof_persistent(double* A, long long ld, int n, int L, double
                                    double* G, int maxleaves, int* cnt, int* factored,
                                    int* next_task, int* err, unsigned long long* timeline,
                                    int workers, cudaStream_t st, int s_begin = 0,
-                                   int s_end = -1);
+                                   int s_end = -1, double* Al = nullptr, long long ldl = 0);
 
 // Persistent BSTRI row recurrence (kernels_bstri.cu): done is (L-2) x
 // bstri_recurrence_ctmax(n, L) ints and next one int, zeroed before.

@@ -145,23 +145,16 @@ BSOFI_DEVINL long long tasks_before(const BsofGeom& g, int s) {
   return base + full * (2 * nl - 2) - full * (full - 1) / 2;
 }
 
-// Column tile (m, t) of the matrix, or of G_k for m >= L: base pointer at the
-// leaf's first row j0 of its panel, and leading dimension.
-BSOFI_DEVINL double* tile_ptr(const BsofGeom& g, double* A, long long ld, double* G, int k, int j0,
-                              int m, int t, long long& ldt) {
-  if (m >= g.L) {
-    const int kk = (m - g.L) / 2, h = (m - g.L) % 2;
-    const long long n2 = 2ll * g.n;
-    ldt = n2;
-    return G + (long long)kk * n2 * n2 + cm(j0, (long long)h * g.n + t * g.NB, n2);
-  }
-  ldt = ld;
-  return A + cm((long long)k * g.n + j0, (long long)m * g.n + t * g.NB, ld);
-}
-
 struct BsofState {
+  // Block columns 0..L-2 of the matrix at A (leading dimension ld), the last
+  // block column at Al (ldl).  The ordinary layout has Al = A + (L-1) n ld;
+  // the compact one stores block columns 0..L-2 with ld = 3n (every access
+  // of block column m stays in block rows m-1..m+1, so those windows never
+  // overlap) and the last block column as its own N x n array.
   double* A;
   long long ld;
+  double* Al;
+  long long ldl;
   double* G;  // (L-1) x (2n)^2, used when form_g
   double* tau;
   double* T;  // 256 doubles per leaf: (k * maxleaves + l) * 256
@@ -177,6 +170,31 @@ struct BsofState {
   // the leaves before s_begin, whose updates are then all done.
   int s_begin, s_end;
 };
+
+// Element (row, column col of block column m) of the matrix, and the leading
+// dimension there.
+BSOFI_DEVINL double* mat_ptr(const BsofGeom& g, const BsofState& st, long long row, int m,
+                             int col, long long& ldm) {
+  if (m == g.L - 1) {
+    ldm = st.ldl;
+    return st.Al + cm(row, col, st.ldl);
+  }
+  ldm = st.ld;
+  return st.A + cm(row, (long long)m * g.n + col, st.ld);
+}
+
+// Column tile (m, t) of the matrix, or of G_k for m >= L: base pointer at the
+// leaf's first row j0 of its panel, and leading dimension.
+BSOFI_DEVINL double* tile_ptr(const BsofGeom& g, const BsofState& st, int k, int j0, int m, int t,
+                              long long& ldt) {
+  if (m >= g.L) {
+    const int kk = (m - g.L) / 2, h = (m - g.L) % 2;
+    const long long n2 = 2ll * g.n;
+    ldt = n2;
+    return st.G + (long long)kk * n2 * n2 + cm(j0, (long long)h * g.n + t * g.NB, n2);
+  }
+  return mat_ptr(g, st, (long long)k * g.n + j0, m, t * g.NB, ldt);
+}
 
 BSOFI_DEVINL unsigned long long gtimer() {
   unsigned long long t;
@@ -692,7 +710,8 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
       if (!own && !block_wait_geq(st, st.cnt + tile_id(g, f.m, f.t), hi - lo, &sm.flag)) return;
       if (tid == 0) st.timeline[4 * s + 1] = gtimer();
       const int mrows = 2 * g.n - f.j0;
-      double* P = st.A + cm((long long)f.k * g.n + f.j0, (long long)f.m * g.n + f.t * g.NB, st.ld);
+      long long ldp;
+      double* P = mat_ptr(g, st, (long long)f.k * g.n + f.j0, f.m, f.t * g.NB, ldp);
       // Target 0 of leaf s: the tile of leaf s+1.
       const bool next = ntargets(g, f) > 0;
       int m2 = 0, t2 = 0, lo2 = 0, hi2 = 0;
@@ -702,7 +721,7 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
       }
       const int x2 = tile_id(g, m2, t2);
       long long ldc = st.ld;
-      double* C = next ? tile_ptr(g, st.A, st.ld, st.G, f.k, f.j0, m2, t2, ldc) : nullptr;
+      double* C = next ? tile_ptr(g, st, f.k, f.j0, m2, t2, ldc) : nullptr;
       const int w2 = min(g.NB, g.n - t2 * g.NB);
       for (int e = tid; e < NB * (NB + 1); e += BT) (&sm.T[0][0])[e] = 0.0;
       if (tid < 2 * NB) (&sm.gsh[0][0])[tid] = 0.0;
@@ -715,7 +734,7 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
           const int r = tid + FW * 32 * i;
 #pragma unroll
           for (int c = 0; c < NB; c++)
-            a[i][c] = (r < mrows && c < f.w) ? __ldcg(P + cm(r, c, st.ld)) : 0.0;
+            a[i][c] = (r < mrows && c < f.w) ? __ldcg(P + cm(r, c, ldp)) : 0.0;
         }
         factor_leaf<FR, NB, FW>(a, sm, mrows, f.w, st.tau + (long long)f.k * g.n + f.j0);
 #pragma unroll
@@ -724,7 +743,7 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
           if (r < mrows) {
 #pragma unroll
             for (int c = 0; c < NB; c++)
-              if (c < f.w) __stcg(P + cm(r, c, st.ld), a[i][c]);
+              if (c < f.w) __stcg(P + cm(r, c, ldp), a[i][c]);
           }
           if constexpr (NB == 16 && Pass<R>::NP == 1) {  // reflectors for the next-tile update
             if (r < Pass<R>::ROWS) {
@@ -781,9 +800,9 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
           // leaf, else re-read from L2 (just written by this CTA).
           double none[R][16];
           apply_qt_mma<R, false, Pass<R>::NP == 1, PREFETCH>(
-              sC, sC + Pass<R>::ROWS * MS, none, P, st.ld, f.w, C, ldc, mrows, w2, sm);
+              sC, sC + Pass<R>::ROWS * MS, none, P, ldp, f.w, C, ldc, mrows, w2, sm);
         } else {
-          apply_qt_mma8<R, true>(sC, sC + 8 * Stage8<R>::S8, a, P, st.ld, f.w, C, ldc, mrows, w2,
+          apply_qt_mma8<R, true>(sC, sC + 8 * Stage8<R>::S8, a, P, ldp, f.w, C, ldc, mrows, w2,
                                  sm);
         }
       }
@@ -823,19 +842,19 @@ __global__ void __launch_bounds__(BT, 1) bsof_persistent_kernel(BsofGeom g, Bsof
     const int mrows = 2 * g.n - f.j0;
     const double* T = st.T + ((long long)f.k * st.maxleaves + f.l) * 256;
     for (int e = tid; e < NB * NB; e += BT) sm.T[e % NB][e / NB] = __ldcg(T + (e % NB) + 16 * (e / NB));
-    const double* P = st.A + cm((long long)f.k * g.n + f.j0, (long long)f.m * g.n + f.t * g.NB, st.ld);
-    long long ldc;
-    double* C = tile_ptr(g, st.A, st.ld, st.G, f.k, f.j0, m2, t2, ldc);
+    long long ldp, ldc;
+    const double* P = mat_ptr(g, st, (long long)f.k * g.n + f.j0, f.m, f.t * g.NB, ldp);
+    double* C = tile_ptr(g, st, f.k, f.j0, m2, t2, ldc);
     const int w2 = min(g.NB, g.n - t2 * g.NB);
     if constexpr (NB == 16) {
       if (!block_wait_geq(st, st.cnt + x2, s - lo2, &sm.flag)) return;
       double none[R][16];
-      apply_qt_mma<R, false>(sC, sC + Pass<R>::ROWS * MS, none, P, st.ld, f.w, C, ldc, mrows, w2,
+      apply_qt_mma<R, false>(sC, sC + Pass<R>::ROWS * MS, none, P, ldp, f.w, C, ldc, mrows, w2,
                              sm);
     } else {
       if (!block_wait_geq(st, st.cnt + x2, s - lo2, &sm.flag)) return;
       double none[R][8];
-      apply_qt_mma8<R, false>(sC, sC + 8 * Stage8<R>::S8, none, P, st.ld, f.w, C, ldc, mrows, w2,
+      apply_qt_mma8<R, false>(sC, sC + 8 * Stage8<R>::S8, none, P, ldp, f.w, C, ldc, mrows, w2,
                               sm);
     }
     if (tid == 0) {
@@ -887,7 +906,8 @@ void bsof_set_factor_warps(int w) { g_factor8.store(w == 8 ? 1 : 0); }
 cudaError_t launch_bsof_persistent(double* A, long long ld, int n, int L, double* tau, double* T,
                                    double* G, int maxleaves, int* cnt, int* factored,
                                    int* next_task, int* err, unsigned long long* timeline,
-                                   int workers, cudaStream_t st, int s_begin, int s_end) {
+                                   int workers, cudaStream_t st, int s_begin, int s_end,
+                                   double* Al, long long ldl) {
   BsofGeom g;
   g.form_g = G != nullptr;
   g.n = n;
@@ -898,6 +918,8 @@ cudaError_t launch_bsof_persistent(double* A, long long ld, int n, int L, double
   BsofState s;
   s.A = A;
   s.ld = ld;
+  s.Al = Al ? Al : A + cm(0, (long long)(L - 1) * n, ld);
+  s.ldl = Al ? ldl : ld;
   s.G = G;
   s.tau = tau;
   s.T = T;

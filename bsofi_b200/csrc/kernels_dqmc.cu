@@ -15,6 +15,8 @@
 // tau_j = 0) and R triangular:
 //   sign(det M) = (-1)^{#(tau_j != 0)} prod sign(R_jj),  log|det M| = sum log|R_jj|.
 // After BSTRI the diagonal holds 1/R_jj (same sign, log negated).
+#include <climits>
+
 #include <cuda_runtime.h>
 
 #include "bsofi_common.cuh"
@@ -30,6 +32,8 @@ struct AssembleArgs {
   int n, L;
   long long ldd;
   double* A;
+  double* Al;         // the last block column (rows 0..N-1), leading dimension ldl
+  long long ldl;
   const double* D;    // L packed diagonal blocks, or nullptr = identity
   const double* S;    // L packed coupling blocks (packed mode)
   const double* E;    // expm(dtau t K), n x n (Hubbard mode)
@@ -47,7 +51,10 @@ __global__ void assemble_kernel(AssembleArgs s) {
   const bool diag = y < s.L;
   const int k = diag ? y : y - s.L;
   const int bi = diag ? k : (k + 1) % s.L, bj = k;
-  double* blk = s.A + cm((long long)bi * n, (long long)bj * n, s.ldd);
+  const bool last = bj == s.L - 1;
+  double* blk = last ? s.Al + cm((long long)bi * n, 0, s.ldl)
+                     : s.A + cm((long long)bi * n, (long long)bj * n, s.ldd);
+  const long long ld = last ? s.ldl : s.ldd;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nn;
        e += (long long)gridDim.x * blockDim.x) {
     const int r = (int)(e % n), c = (int)(e / n);
@@ -61,13 +68,20 @@ __global__ void assemble_kernel(AssembleArgs s) {
     } else {
       v = s.S[(long long)k * nn + e];
     }
-    blk[cm(r, c, s.ldd)] = v;
+    blk[cm(r, c, ld)] = v;
   }
 }
 
-cudaError_t launch_assemble(const AssembleArgs& s, cudaStream_t st) {
-  cudaError_t e = launch_zero_structural(s.A, s.ldd, s.n, s.L, st);
-  if (e != cudaSuccess) return e;
+// Into the ordinary layout (s.Al unset): the structural zero blocks the
+// factorization reads, then the p-cyclic blocks.  Into the compact one
+// (s.Al set; the caller zeroed both arrays): the p-cyclic blocks only.
+cudaError_t launch_assemble(AssembleArgs s, cudaStream_t st) {
+  if (s.Al == nullptr) {
+    cudaError_t e = launch_zero_structural(s.A, s.ldd, s.n, s.L, st);
+    if (e != cudaSuccess) return e;
+    s.Al = s.A + cm(0, (long long)(s.L - 1) * s.n, s.ldd);
+    s.ldl = s.ldd;
+  }
   const long long nn = (long long)s.n * s.n;
   const int gx = (int)((nn + 255) / 256 < 64 ? (nn + 255) / 256 : 64);
   assemble_kernel<<<dim3(gx, 2 * s.L), 256, 0, st>>>(s);
@@ -76,15 +90,18 @@ cudaError_t launch_assemble(const AssembleArgs& s, cudaStream_t st) {
 
 // One CTA: sum of log|d_j|, count of d_j < 0, of d_j == 0 (or not finite) and
 // of tau_j != 0 over the N diagonal entries.
+// Diagonal entries j < jsplit at A (leading dimension ldd), the rest at Al
+// (ldl), whose column 0 is column jsplit of the matrix (jsplit = N: all in A).
 __global__ void __launch_bounds__(1024) logdet_kernel(const double* A, long long ldd, int N,
                                                       const double* tau, int inverted,
-                                                      double* out) {
+                                                      double* out, const double* Al = nullptr,
+                                                      long long ldl = 0, int jsplit = INT_MAX) {
   __shared__ double s_log[32];
   __shared__ int s_cnt[32][3];
   double lsum = 0.0;
   int neg = 0, bad = 0, refl = 0;
   for (int j = threadIdx.x; j < N; j += blockDim.x) {
-    const double d = A[(long long)j * ldd + j];
+    const double d = j < jsplit ? A[(long long)j * ldd + j] : Al[cm(j, j - jsplit, ldl)];
     const double ad = fabs(d);
     if (d < 0.0) neg++;
     if (!(ad > 0.0) || isinf(ad)) bad++;
@@ -168,4 +185,44 @@ BSOFI_API int bsofi_device_logdet(int n, int L, const double* dA, int ldda, cons
   logdet_kernel<<<1, 1024, 0, (cudaStream_t)stream>>>(dA, ldda, n * L, dtau, inverted ? 1 : 0,
                                                       dout);
   return api_err(cudaGetLastError());
+}
+
+// Compact storage of the storage-sharded inversion: block columns 0..L-2 at
+// band (leading dimension 3n, band_doubles in all), the last block column at
+// last (N x n, leading dimension N).  Both arrays are zeroed, then the
+// p-cyclic blocks written: packed (dS, and dD or identity diagonal blocks) or
+// Hubbard (dExpK set: dh and lambda as for bsofi_device_hubbard_assemble).
+extern "C" int bsofi_dev_assemble_compact(int n, int L, const double* dD, const double* dS,
+                                          const double* dExpK, const double* dh, double lambda,
+                                          double* band, size_t band_doubles, double* last,
+                                          void* stream) {
+  const cudaStream_t st = (cudaStream_t)stream;
+  const long long N = (long long)n * L;
+  cudaError_t e = cudaMemsetAsync(band, 0, sizeof(double) * band_doubles, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(last, 0, sizeof(double) * (size_t)N * n, st);
+  if (e != cudaSuccess) return (int)e;
+  AssembleArgs s = {};
+  s.n = n;
+  s.L = L;
+  s.ldd = 3ll * n;
+  s.A = band;
+  s.Al = last;
+  s.ldl = N;
+  s.D = dD;
+  s.S = dS;
+  s.E = dExpK;
+  s.h = dh;
+  s.lambda = lambda;
+  s.hubbard = dExpK != nullptr;
+  return (int)launch_assemble(s, st);
+}
+
+// Sign and log|det M| from the compact state (as bsofi_device_logdet).
+extern "C" int bsofi_dev_logdet_compact(int n, int L, const double* band, const double* last,
+                                        const double* tau, int inverted, double* out,
+                                        void* stream) {
+  const int N = n * L;
+  logdet_kernel<<<1, 1024, 0, (cudaStream_t)stream>>>(band, 3ll * n, N, tau, inverted ? 1 : 0,
+                                                      out, last, N, (L - 1) * n);
+  return (int)cudaGetLastError();
 }

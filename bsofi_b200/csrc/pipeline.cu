@@ -230,8 +230,11 @@ __global__ void __launch_bounds__(256) build_leaf_t_kernel(const double* __restr
 
 // BSOF.  form_q: the persistent kernel also forms G_k = Q_k^T for BSOI.
 // workers: worker CTAs for 16-wide leaves (four times as many for 8-wide).
+// Al, ldl (optional): the last block column in its own array (the compact
+// layout of the storage-sharded inversion); the workspace regions used here
+// lie before the carries, so their offsets do not depend on ldd.
 int run_bsof(int n, int L, double* dA, int ldd, double* dtau, void* ws, cudaStream_t st,
-             bool form_q, int base_workers) {
+             bool form_q, int base_workers, double* Al = nullptr, long long ldl = 0) {
   Layout ly = layout(n, L, ldd);
   double* Tb = at<double>(ws, ly.T);
   double* G = at<double>(ws, ly.G);
@@ -246,7 +249,7 @@ int run_bsof(int n, int L, double* dA, int ldd, double* dtau, void* ws, cudaStre
   if (form_q) workers *= 2;
   CK(launch_bsof_persistent(dA, ldd, n, L, dtau, Tb, form_q ? G : nullptr, ly.maxleaves, sync,
                             sync + ntiles, sync + ntiles + ly.leaves, at<int>(ws, ly.info) + 1,
-                            at<unsigned long long>(ws, ly.tl), workers, st));
+                            at<unsigned long long>(ws, ly.tl), workers, st, 0, -1, Al, ldl));
   return 0;
 }
 
@@ -441,13 +444,16 @@ int w_products(int n, double* dA, int ldd, double* W, int i0, int i1, cudaStream
 }
 
 // Y_i = R_{i,L-1} X_{L-1,L-1} and Z_i = -X_ii Y_i -> A(i, L-1), i = 0..L-2.
-int yz_products(int n, int L, double* dA, int ldd, double* Y, cudaStream_t st) {
+// The last block column is at Al (leading dimension ldl): A's block column
+// L-1, or its own array in the compact layout.
+int yz_products(int n, int L, double* dA, int ldd, double* Al, long long ldl, double* Y,
+                cudaStream_t st) {
   const long long nn = (long long)n * n, diag = (long long)n * (ldd + 1);
   GemmDims d = {n, n, n};
   {
-    GemmA a = plain_a(dA + cm(0, (long long)(L - 1) * n, ldd), ldd, n);
+    GemmA a = plain_a(Al, ldl, n);
     a.ksplit = n;
-    GemmB b = {dA + cm((long long)(L - 1) * n, (long long)(L - 1) * n, ldd), ldd, 0, 0};
+    GemmB b = {Al + cm((long long)(L - 1) * n, 0, ldl), ldl, 0, 0};
     GemmC c = {};
     c.p0 = Y;
     c.ld0 = n;
@@ -463,8 +469,8 @@ int yz_products(int n, int L, double* dA, int ldd, double* Y, cudaStream_t st) {
     a.roff0 = 0;
     GemmB b = {Y, n, nn, kNoMask};
     GemmC c = {};
-    c.p0 = dA + cm(0, (long long)(L - 1) * n, ldd);
-    c.ld0 = ldd;
+    c.p0 = Al;
+    c.ld0 = ldl;
     c.bs0 = n;
     c.ld1 = 1;
     c.nsplit = n;
@@ -484,7 +490,8 @@ int run_bstri(int n, int L, double* dA, int ldd, void* ws, cudaStream_t st) {
   // X_ii = R_ii^{-1} for every diagonal block (Y, not yet used, is the
   // scratch of the recursive inversion).
   if (int e = diag_inverse(n, dA, ldd, info, Y, 0, L, st)) return e;
-  if (int e = yz_products(n, L, dA, ldd, Y, st)) return e;
+  double* last = dA + cm(0, (long long)(L - 1) * n, ldd);
+  if (int e = yz_products(n, L, dA, ldd, last, ldd, Y, st)) return e;
   if (int e = w_products(n, dA, ldd, W, 0, L - 2, st)) return e;
   // Row recurrence: X_{i, i+1:L} = W_i X_{i+1, i+1:L} (+ Z_i on the last block).
   const Plan plan = plan_for(n, L);
@@ -657,7 +664,8 @@ int run_bsoftri_overlap(int n, int L, double* dA, int ldd, double* dtau, void* w
   if (j4) return j4;
   // The rest of BSTRI.
   if (int e = diag_inverse(n, dA, ldd, info, Y, h, L, st)) return e;
-  if (int e = yz_products(n, L, dA, ldd, Y, st)) return e;
+  double* last = dA + cm(0, (long long)(L - 1) * n, ldd);
+  if (int e = yz_products(n, L, dA, ldd, last, ldd, Y, st)) return e;
   if (int e = w_products(n, dA, ldd, W, h, L - 2, st)) return e;
   if (int e = groups_seed(G, W, P, 0, tailg, st)) return e;
   if (int e = groups_rounds(G, dA, ldd, W, P, 0, tailg, kRoundP | kRoundIntra, st)) return e;
@@ -877,6 +885,153 @@ int run_bsoi(int n, int L, double* dA, int ldd, const double* dtau, void* ws, cu
       if ((e = bsoi_step(n, L, k, dA, ldd, ws, st, cfg)) != 0) return e;
   }
   return bsoi_finish(n, L, dA, ldd, ws, st);
+}
+
+// ------------------------------------------------------ storage-sharded
+// One inversion over several GPUs with no GPU holding M or M^{-1} whole.
+// The factorization's state is O(L n^2): R has three nonzero blocks per block
+// row (diagonal, superdiagonal, last column) and the reflectors fill the
+// panels, so every rank factors the whole matrix in a compact layout:
+//   band  block columns 0..L-2 with leading dimension 3n: BSOF and BSTRI's
+//         diagonal and row-multiplier products touch only block rows m-1..m+1
+//         of block column m, and with ld = 3n those windows of consecutive
+//         columns never overlap (column j's window starts 3n elements after
+//         column j-1's, and n further at a block boundary);
+//   last  the last block column, N x n (R_{i,L-1} and then Z_i for every i);
+//   tau   N doubles;
+// plus the workspace regions of the fused pipeline (G_k = Q_k^T, W_i, Y_i,
+// the BSOI carries).  BSTRI's block columns are then independent given W_i
+// and Z_i (X_{i,c} = W_i X_{i+1,c} (+ Z_i for c = L-1)), and BSOI's rows are
+// independent (X(rows, k:k+1) Q_k^T), so a rank computes the block columns it
+// owns, the ranks exchange them for row bands, and each finishes its rows.
+struct ShardLayout {
+  size_t ws, band, last, tau, total;
+  size_t band_doubles;
+};
+
+ShardLayout shard_layout(int n, int L) {
+  const size_t N = (size_t)n * L;
+  ShardLayout s;
+  s.ws = 0;
+  // Carries for a row band of up to N rows with an even leading dimension.
+  size_t off = layout(n, L, (int)N + 1).total;
+  s.band_doubles = 3 * (size_t)n * (size_t)(L - 1) * n + N;
+  s.band = off;
+  off += align256(sizeof(double) * s.band_doubles);
+  s.last = off;
+  off += align256(sizeof(double) * N * n);
+  s.tau = off;
+  off += align256(sizeof(double) * N);
+  s.total = off;
+  return s;
+}
+
+// Compact input, BSOF with every Q_k^T formed, the diagonal inverses
+// X_ii = R_ii^{-1}, Z_i (into last) and W_i: everything BSTRI's column
+// recurrence and BSOI read.
+int shard_factor(int n, int L, const double* dD, const double* dS, const double* dExpK,
+                 const double* dh, double lambda, void* state, cudaStream_t st) {
+  const ShardLayout sl = shard_layout(n, L);
+  const int N = n * L;
+  Layout ly = layout(n, L, N + 1);
+  double* band = at<double>(state, sl.band);
+  double* last = at<double>(state, sl.last);
+  double* tau = at<double>(state, sl.tau);
+  int* info = at<int>(state, ly.info);
+  double* W = at<double>(state, ly.W);
+  double* Y = at<double>(state, ly.Y);
+  const int ldb = 3 * n;
+  if (int e = bsofi_dev_assemble_compact(n, L, dD, dS, dExpK, dh, lambda, band, sl.band_doubles,
+                                         last, st))
+    return e;
+  g_launches++;
+  if (int e = run_bsof(n, L, band, ldb, tau, state, st, true, bsof_workers(n, L, 0), last, N))
+    return e;
+  CKM(cudaMemsetAsync(info, 0x7f, sizeof(int), st));
+  CKM(cudaMemsetAsync(info + 3, 0, sizeof(int), st));
+  if (int e = diag_inverse(n, band, ldb, info, Y, 0, L - 1, st)) return e;
+  CK(launch_trtri_blocks(last + cm((long long)(L - 1) * n, 0, N), N, n, 0, 1, info, Y, st,
+                         L - 1));
+  if (int e = yz_products(n, L, band, ldb, last, N, Y, st)) return e;
+  return w_products(n, band, ldb, W, 0, L - 2, st);
+}
+
+// Block columns [c0, c1) of X = R^{-1}, rows 0..c1 n - 1 (X is block upper
+// triangular), into X (leading dimension ldx >= c1 n), from the state of
+// shard_factor: the diagonal blocks and Z_i copied in, then for
+// i = min(c1-2, L-3) .. 0 one GEMM X_{i, c} = W_i X_{i+1, c} (+ Z_i for
+// c = L-1) over the owned columns c > i.
+int shard_bstri_columns(int n, int L, int c0, int c1, double* X, long long ldx, void* state,
+                        cudaStream_t st) {
+  const ShardLayout sl = shard_layout(n, L);
+  const int N = n * L;
+  Layout ly = layout(n, L, N + 1);
+  const double* band = at<double>(state, sl.band);
+  const double* last = at<double>(state, sl.last);
+  const double* W = at<double>(state, ly.W);
+  const long long nn = (long long)n * n, ldb = 3ll * n;
+  const bool has_last = c1 == L;
+  CKM(cudaMemset2DAsync(X, sizeof(double) * ldx, 0, sizeof(double) * (size_t)c1 * n,
+                        (size_t)(c1 - c0) * n, st));
+  for (int c = c0; c < c1 && c < L - 1; c++)
+    CK(launch_copy_masked(X + cm((long long)c * n, (long long)(c - c0) * n, ldx), ldx,
+                          band + cm((long long)c * n, (long long)c * n, ldb), ldb, n, n, 0, st));
+  if (has_last)
+    CK(launch_copy_masked(X + cm(0, (long long)(L - 1 - c0) * n, ldx), ldx, last, N, N, n,
+                          (L - 1) * n, st));
+  for (int i = min(c1 - 2, L - 3); i >= 0; i--) {
+    const int cs = max(i + 1, c0);
+    if (cs >= c1) continue;
+    const int ncol = (c1 - cs) * n;
+    GemmDims d = {n, ncol, n};
+    GemmA a = plain_a(W + (size_t)i * nn, n, 0);
+    a.ksplit = n;
+    GemmB b = {X + cm((long long)(i + 1) * n, (long long)(cs - c0) * n, ldx), ldx, 0, kNoMask};
+    GemmC c = {};
+    c.p0 = X + cm((long long)i * n, (long long)(cs - c0) * n, ldx);
+    c.ld0 = ldx;
+    c.alpha = 1.0;
+    c.beta0 = 0.0;
+    if (has_last) {
+      c.p1 = X + cm((long long)i * n, (long long)(L - 1 - c0) * n, ldx);
+      c.ld1 = ldx;
+      c.nsplit = ncol - n;
+      c.beta1 = 1.0;
+    } else {
+      c.p1 = c.p0;
+      c.ld1 = ldx;
+      c.nsplit = ncol;
+    }
+    CK(launch_gemm(d, a, b, c, 1, 0, st));
+  }
+  return 0;
+}
+
+// Rows [r0, r1) of M^{-1} from the same rows of X in every column, in place
+// in B (leading dimension ldb >= r1 - r0): BSOI's persistent launch over
+// that row range, with B and the carries addressed by global row (shifted
+// base pointers; every access stays inside [r0, r1)).
+int shard_bsoi_rows(int n, int L, int r0, int r1, double* B, long long ldb, void* state,
+                    cudaStream_t st) {
+  const int N = n * L;
+  Layout ly = layout(n, L, N + 1);
+  const int rows = r1 - r0;
+  const long long ldc = (rows + 1) & ~1;
+  double* Bs = B - r0;
+  double* C[2] = {at<double>(state, ly.C0) - r0, at<double>(state, ly.C1) - r0};
+  const double* G = at<double>(state, ly.G);
+  int* info = at<int>(state, ly.info);
+  CK(launch_copy_masked(C[0] + r0, ldc, Bs + cm(r0, (long long)(L - 1) * n, ldb), ldb, rows, n,
+                        (L - 1) * n - r0, st));
+  CKM(cudaMemsetAsync(info + 2, 0, sizeof(int), st));
+  const Plan plan = plan_for(n, L);
+  int* bs = at<int>(state, ly.bsync);
+  CKM(cudaMemsetAsync(bs, 0, sizeof(int) * ly.bsync_ints, st));
+  CK(launch_bsoi_persistent(Bs, ldb, C[0], C[1], ldc, G, n, L, bs, bs + ly.bsync_ints - 2,
+                            info + 2, plan.bsoi != 0, st, r0, r1));
+  const int cur = (L - 1) & 1;  // carry buffer written by step 0
+  CK(launch_copy_masked(B, ldb, C[cur] + r0, ldc, rows, n, kNoMask, st, info));
+  return 0;
 }
 
 }  // namespace
@@ -1115,6 +1270,39 @@ int bsofi_dev_bsoi_step(int n, int L, int k, double* dA, int ldd, void* dws, voi
 
 int bsofi_dev_bsoi_finish(int n, int L, double* dA, int ldd, void* dws, void* stream) {
   return bsoi_finish(n, L, dA, ldd, dws, (cudaStream_t)stream);
+}
+
+size_t bsofi_dev_shard_state_bytes(int n, int L) { return shard_layout(n, L).total; }
+
+int bsofi_dev_shard_factor(int n, int L, const double* dD, const double* dS,
+                           const double* dExpK, const double* dh, double lambda, void* dstate,
+                           void* stream) {
+  g_launches = 0;
+  return shard_factor(n, L, dD, dS, dExpK, dh, lambda, dstate, (cudaStream_t)stream);
+}
+
+int bsofi_dev_shard_bstri_columns(int n, int L, int c0, int c1, double* dX, long long ldx,
+                                  void* dstate, void* stream) {
+  g_launches = 0;
+  return shard_bstri_columns(n, L, c0, c1, dX, ldx, dstate, (cudaStream_t)stream);
+}
+
+int bsofi_dev_shard_bsoi_rows(int n, int L, int r0, int r1, double* dB, long long ldb,
+                              void* dstate, void* stream) {
+  g_launches = 0;
+  return shard_bsoi_rows(n, L, r0, r1, dB, ldb, dstate, (cudaStream_t)stream);
+}
+
+int bsofi_dev_shard_logdet(int n, int L, const void* dstate, double* dout, void* stream) {
+  const ShardLayout sl = shard_layout(n, L);
+  void* s = const_cast<void*>(dstate);
+  // After shard_factor the diagonal blocks hold R_ii^{-1}.
+  return bsofi_dev_logdet_compact(n, L, at<double>(s, sl.band), at<double>(s, sl.last),
+                                  at<double>(s, sl.tau), 1, dout, stream);
+}
+
+const double* bsofi_dev_shard_tau(const void* dstate, int n, int L) {
+  return at<double>(const_cast<void*>(dstate), shard_layout(n, L).tau);
 }
 
 int bsofi_dev_invert(int n, int L, double* dA, int ldd, double* dtau, void* dws, void* stream) {

@@ -183,6 +183,54 @@ int bsofi_device_bsoi_rows(int n, int L, double *dA, int ldda, const double *dta
                            int row0, int row1, void *stream);
 int *bsofi_device_info(void *dwork);
 
+/* Storage-sharded inversion: one inversion over several GPUs with no GPU
+ * holding M or M^{-1} whole, for N beyond one GPU's memory (no reference
+ * counterpart; the reference inverts on one device, src/bsofi_callback.c:
+ * 130-157).  The split follows the algorithm's structure:
+ *   - BSOF's state is small: R has three nonzero blocks per block row and the
+ *     reflectors fill the 2n x n panels (src/bsofi_cpu.c:86-118), so every
+ *     rank factors the whole matrix in a compact layout (3 L n^2 + N n
+ *     doubles instead of N^2) and holds the same state;
+ *   - BSTRI's block columns are independent once the diagonal inverses
+ *     X_ii = R_ii^{-1}, the row multipliers W_i = -X_ii R_{i,i+1} and
+ *     Z_i = -X_ii R_{i,L-1} X_{L-1,L-1} are known (the row recurrence of
+ *     src/bsofi_cpu.c:146-177 read by columns: X_{i,c} = W_i X_{i+1,c}, plus
+ *     Z_i in the last column), so each rank computes the block columns it owns;
+ *   - BSOI's rows are independent (X(:,k:k+1) Q_k^T, src/bsofi_cpu.c:211-248),
+ *     so after the ranks exchange their columns for row bands each finishes
+ *     its rows of M^{-1}.
+ * Per rank: bsofi_shard_state_bytes(n, L) of device state, the owned block
+ * columns (c1 n x (c1 - c0) n doubles) and the row band ((r1 - r0) x N).
+ *
+ * bsofi_shard_factor: the state from the packed p-cyclic blocks (dD, dS as
+ * bsofi_device_assemble takes them); bsofi_shard_hubbard_factor from expm(K)
+ * and the fields (as bsofi_device_hubbard_assemble).
+ * bsofi_shard_bstri_columns: block columns [c0, c1) of X = R^{-1}, rows
+ * 0 .. c1 n - 1 (the rest of those columns is zero), into dX (column-major,
+ * leading dimension ldx >= c1 n).
+ * bsofi_shard_bsoi_rows: dB holds rows [row0, row1) of X in all N columns
+ * (column-major, leading dimension ldb >= row1 - row0) and is overwritten
+ * with the same rows of M^{-1}; row0 a multiple of 128, row1 too unless it
+ * is N.  Calls on one state run in order (they share its workspace).
+ * bsofi_shard_logdet: sign and log|det M| as bsofi_device_logdet, from the
+ * state.  bsofi_shard_info: the state's info word (as bsofi_device_info);
+ * bsofi_shard_tau: the N reflector scalars inside the state.
+ * All enqueue on `stream` and return 0, -1 for an illegal argument, or
+ * BSOFI_INFO_CUDA - cudaError_t.  bsofi_b200/shard.py drives them over a
+ * torch.distributed group (all-to-all of columns into row bands). */
+unsigned long long bsofi_shard_state_bytes(int n, int L);
+int bsofi_shard_factor(int n, int L, const double *dD, const double *dS, void *dstate,
+                       void *stream);
+int bsofi_shard_hubbard_factor(int n, int L, const double *dExpK, const double *dh,
+                               double lambda, void *dstate, void *stream);
+int bsofi_shard_bstri_columns(int n, int L, int c0, int c1, double *dX, long long ldx,
+                              void *dstate, void *stream);
+int bsofi_shard_bsoi_rows(int n, int L, int row0, int row1, double *dB, long long ldb,
+                          void *dstate, void *stream);
+int bsofi_shard_logdet(int n, int L, const void *dstate, double *dout, void *stream);
+int *bsofi_shard_info(void *dstate);
+const double *bsofi_shard_tau(const void *dstate, int n, int L);
+
 /* Mixed-precision inversion (no reference counterpart; the reference's
  * BSOI products are FP64 LAPACK/MAGMA calls, src/bsofi_cpu.c:234-245 and
  * src/bsofi_gpu.c:397-411).  The factorization (BSOF), the triangular

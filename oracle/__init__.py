@@ -123,6 +123,22 @@ def ref_bsoftri(A, n, L, inplace=False):
     return A, tau, info.value
 
 
+def ref_bsof(A, n, L):
+    """lapackXbsof (src/bsofi_cpu.c:86-118) on a copy of A: the factorization
+    alone, R in the block upper part and the reflectors below.  Returns
+    (A_out, tau, info)."""
+    lib = _lib("ref")
+    A = _check(A, n, L)
+    N = n * L
+    lw = int(lib.lapackXbsofiLWork(ctypes.c_int(n), ctypes.c_int(L), ctypes.c_int(N)))
+    work = np.zeros(max(lw, 1))
+    tau = np.zeros(N)
+    info = ctypes.c_int(0)
+    lib.lapackXbsof(ctypes.c_int(n), ctypes.c_int(L), _p(A), ctypes.c_int(N), _p(tau), _p(work),
+                    ctypes.c_int(lw), ctypes.byref(info))
+    return A, tau, info.value
+
+
 def ref_bsoi(A, tau, n, L, inplace=False):
     """hybridxbsoih_ on a copy of the BSOFTRI state (on A and tau themselves
     with inplace=True).  Returns (A_out, info)."""
