@@ -240,7 +240,8 @@ def batch_timing(count, streams, precision=0, reps=2, seed=77):
 
 
 def main(argv):
-    # --grouped=0: FP64 batches run each instance's BSOI as its own launch.
+    # --grouped=1: FP64 batches run BSOI as one grouped launch per tile shape
+    # (the default, 0, launches each instance's BSOI on its own stream).
     for a in list(argv):
         if a.startswith("--grouped="):
             _lib.load().bsofi_device_set_batch_grouped(int(a.split("=", 1)[1]))

@@ -298,11 +298,15 @@ unsigned long long bsofi_batch_workspace_bytes(int count, const int *n, const in
 int bsofi_device_invert_batched(int count, const int *n, const int *L, double *const *dA,
                                 const int *ldda, double *const *dtau, void *dwork, int streams,
                                 void *stream);
-/* FP64 batches run BSOF + BSTRI of each instance over the stream pool, then
- * BSOI of all instances as one persistent launch per tile shape over one
- * queue of every instance's tiles (at most 256 instances per launch), then
- * each instance's last BSOI copy.  Diagnostics (no reference counterpart):
- * on = 0 runs each instance's BSOI as its own launch instead; process-wide. */
+/* How FP64 batches run BSOI (no reference counterpart; process-wide).
+ * on = 0, the default: each instance's BSOI is its own persistent launch on
+ * the instance's stream, overlapping the other instances' factorizations.
+ * on = 1: BSOF + BSTRI of every instance over the stream pool first, then BSOI
+ * of all instances as one persistent launch per tile shape over one queue of
+ * every instance's tiles (at most 256 instances per launch), then each
+ * instance's last BSOI copy: no wave tails between instances, but the
+ * latency-bound factorizations no longer overlap the GEMM work (measured
+ * slower on a 256-instance batch of mixed sizes). */
 void bsofi_device_set_batch_grouped(int on);
 /* The same batch at a chosen precision: 0 FP64 (as above), 1 mixed (every
  * instance as bsofi_device_invert_mixed with BSOFI_MIXED_SLICES slices).  The

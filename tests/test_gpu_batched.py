@@ -86,12 +86,13 @@ def test_batch_graph_replays_match_direct(cuda_device):
 
 
 def test_grouped_bsoi_matches_per_instance(cuda_device):
-    """FP64 batches run BSOI as one grouped persistent launch per tile shape
-    (64 x 64 for 2n not a multiple of 128, 128 x 128 otherwise; at most 256
-    instances per launch).  300 instances of mixed sizes (so both tile shapes
-    and two launches of the 64 x 64 shape) against the same batch with each
-    instance's BSOI launched on its own: equal within the FP64 tolerance, with
-    small residuals."""
+    """With bsofi_device_set_batch_grouped(1) FP64 batches run BSOI as one
+    grouped persistent launch per tile shape (64 x 64 for 2n not a multiple
+    of 128, 128 x 128 otherwise; at most 256 instances per launch).  300
+    instances of mixed sizes (so both tile shapes and two launches of the
+    64 x 64 shape) against the same batch with each instance's BSOI launched
+    on its own (the default): equal within the FP64 tolerance, with small
+    residuals."""
     import torch
     from gpu_util import from_device_colmajor, to_device_colmajor
     lib = api.load()
@@ -117,7 +118,7 @@ def test_grouped_bsoi_matches_per_instance(cuda_device):
             assert rc == 0
             return [from_device_colmajor(A, n * L) for A, (n, L) in zip(dA, specs)]
         finally:
-            lib.bsofi_device_set_batch_grouped(1)
+            lib.bsofi_device_set_batch_grouped(0)
 
     Xg = run(1)
     Xp = run(0)
