@@ -137,6 +137,8 @@ _SIGS = {
     "bsofi_device_set_bsof_workers": (None, [ctypes.c_int]),
     "bsofi_device_set_bsof_factor_warps": (None, [ctypes.c_int]),
     "bsofi_device_set_batch_grouped": (None, [ctypes.c_int]),
+    "bsofi_device_set_batch_chains": (None, [ctypes.c_int]),
+    "bsofi_device_set_batch_pipelined": (None, [ctypes.c_int]),
     "bsofi_device_set_wait_test": (None, [ctypes.c_int]),
     "bsofi_device_set_bstri_overlap": (None, [ctypes.c_int]),
     "bsofi_device_timing": (None, [ctypes.c_int]),

@@ -21,10 +21,15 @@
 
 #define MAX_STREAMS 32
 
+/* Ring of events bounding the factorization chains in flight. */
+#define MAX_GATE 32
+
 typedef struct {
-  int ready, count, device;
+  int ready, count, device, gates, hi_count;
   cudaStream_t s[MAX_STREAMS];
+  cudaStream_t hi[MAX_STREAMS];  /* highest priority: factorization chains */
   cudaEvent_t ev[MAX_STREAMS + 1];
+  cudaEvent_t gate[MAX_GATE];
 } stream_pool;
 
 static __thread stream_pool t_pool;
@@ -39,8 +44,12 @@ static cudaError_t pool_get(int want, stream_pool **out) {
   if (p->ready && p->device != dev) {
     for (i = 0; i < p->count; i++) cudaStreamDestroy(p->s[i]);
     for (i = 0; i <= p->count; i++) cudaEventDestroy(p->ev[i]);
+    for (i = 0; i < p->gates; i++) cudaEventDestroy(p->gate[i]);
+    for (i = 0; i < p->hi_count; i++) cudaStreamDestroy(p->hi[i]);
     p->ready = 0;
     p->count = 0;
+    p->gates = 0;
+    p->hi_count = 0;
   }
   if (!p->ready) {
     if ((e = cudaEventCreateWithFlags(&p->ev[0], cudaEventDisableTiming)) != cudaSuccess) return e;
@@ -53,6 +62,21 @@ static cudaError_t pool_get(int want, stream_pool **out) {
     if ((e = cudaEventCreateWithFlags(&p->ev[p->count + 1], cudaEventDisableTiming)) != cudaSuccess)
       return e;
     p->count++;
+  }
+  while (p->gates < MAX_GATE) {
+    if ((e = cudaEventCreateWithFlags(&p->gate[p->gates], cudaEventDisableTiming)) != cudaSuccess)
+      return e;
+    p->gates++;
+  }
+  if (p->hi_count < p->count) {
+    int least = 0, greatest = 0;
+    if ((e = cudaDeviceGetStreamPriorityRange(&least, &greatest)) != cudaSuccess) return e;
+    while (p->hi_count < p->count) {
+      if ((e = cudaStreamCreateWithPriority(&p->hi[p->hi_count], cudaStreamNonBlocking,
+                                            greatest)) != cudaSuccess)
+        return e;
+      p->hi_count++;
+    }
   }
   *out = p;
   return cudaSuccess;
@@ -74,6 +98,24 @@ static size_t inst_ws(int n, int L, int ldda, int precision) {
  * sizes, 227.8 against 248.5 inversions/s). */
 static int g_grouped = 0;
 void bsofi_device_set_batch_grouped(int on) { g_grouped = on ? 1 : 0; }
+
+/* At most this many instances' factorization chains run at once (0: as many
+ * as there are streams).  A BSOF launch holds its SMs (one CTA each) for the
+ * whole latency-bound chain, so chains beyond a few only take SMs from the
+ * other instances' GEMM phases. */
+static int g_chains = 0;
+void bsofi_device_set_batch_chains(int k) {
+  g_chains = k < 0 ? 0 : (k > MAX_GATE ? MAX_GATE : k);
+}
+
+/* Pipelined batches (1): each instance's factorization chain runs on a
+ * highest-priority stream, chains of the instances dealt to one slot back to
+ * back, and hands over by an event to the slot's ordinary stream for BSTRI
+ * and BSOI, launched without persistent kernels (per-step GEMMs, whose CTAs
+ * retire tile by tile, so that the next chains' cooperative launches find
+ * SMs).  0: each instance's whole pipeline on one stream. */
+static int g_pipelined = 0;
+void bsofi_device_set_batch_pipelined(int on) { g_pipelined = on ? 1 : 0; }
 
 unsigned long long bsofi_batch_workspace_bytes_ex(int count, const int *n, const int *L,
                                                   const int *ldda, int precision) {
@@ -214,11 +256,38 @@ int bsofi_device_invert_batched_ex(int count, const int *n, const int *L, double
       goto fail;
     }
   }
-  for (i = 0; i < count && !(precision == 0 && g_grouped); i++) {
+  if (g_pipelined && !(precision == 0 && g_grouped)) {
+    for (i = 0; i < used; i++)
+      if ((e = cudaStreamWaitEvent(p->hi[i], p->ev[0], 0)) != cudaSuccess) goto fail;
+    bsofi_dev_set_nonpersistent(1);
+    for (i = 0; i < count && !r; i++) {
+      const int k = ord[i].i, slot = i % used;
+      const int workers = n[k] <= 256 ? 6 : 24;
+      r = bsofi_dev_invert_two_streams(n[k], L[k], dA[k], ldda[k], dtau[k],
+                                       (char *)dwork + off[k], p->hi[slot], p->s[slot],
+                                       p->gate[slot], workers,
+                                       precision == 1 ? BSOFI_MIXED_SLICES : 0);
+      launches += bsofi_dev_launch_count();
+    }
+    bsofi_dev_set_nonpersistent(0);
+    if (r) {
+      e = (cudaError_t)r;
+      goto fail;
+    }
+  }
+  for (i = 0; i < count && !(precision == 0 && g_grouped) && !g_pipelined; i++) {
     const int k = ord[i].i;
     /* Few BSOF workers per instance: the batch supplies the parallelism. */
     const int workers = n[k] <= 256 ? 6 : 24;
-    if (precision == 1)
+    /* Gate: instance i waits for the chain of instance i - K (ring slot
+     * i % K, recorded by that instance after its BSOF) and records the slot
+     * after its own; the host issues them in that order. */
+    const int K = (g_chains > 0 && g_chains < used) ? g_chains : 0;
+    if (K > 0)
+      r = bsofi_dev_invert_gated(n[k], L[k], dA[k], ldda[k], dtau[k], (char *)dwork + off[k],
+                                 p->s[i % used], workers, precision == 1 ? BSOFI_MIXED_SLICES : 0,
+                                 i >= K ? (void *)p->gate[i % K] : NULL, (void *)p->gate[i % K]);
+    else if (precision == 1)
       r = bsofi_dev_invert_mixed(n[k], L[k], dA[k], ldda[k], dtau[k], (char *)dwork + off[k],
                                  p->s[i % used], workers, BSOFI_MIXED_SLICES);
     else
@@ -233,6 +302,14 @@ int bsofi_device_invert_batched_ex(int count, const int *n, const int *L, double
   for (i = 0; i < used; i++) {
     if ((e = cudaEventRecord(p->ev[i + 1], p->s[i])) != cudaSuccess) goto fail;
     if ((e = cudaStreamWaitEvent((cudaStream_t)stream, p->ev[i + 1], 0)) != cudaSuccess) goto fail;
+    /* The chain streams too (their last work is already ordered before the
+     * ordinary streams' by the hand-over events; joining them as well keeps
+     * a stream capture of the batch complete). */
+    if (g_pipelined && !(precision == 0 && g_grouped)) {
+      if ((e = cudaEventRecord(p->gate[i], p->hi[i])) != cudaSuccess) goto fail;
+      if ((e = cudaStreamWaitEvent((cudaStream_t)stream, p->gate[i], 0)) != cudaSuccess)
+        goto fail;
+    }
   }
   free(ord);
   free(off);

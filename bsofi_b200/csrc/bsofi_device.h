@@ -93,6 +93,24 @@ int bsofi_dev_bsoi_ex(int n, int L, double *dA, int ldd, const double *dtau, voi
 int bsofi_dev_bsoi_rows(int n, int L, double *dA, int ldd, const double *dtau, void *dws,
                         void *stream, int row0, int row1);
 
+/* One inversion (FP64 when slices = 0, else the mixed path with that many
+ * slices) whose factorization chain is gated: the stream waits for wait_ev
+ * (optional) before BSOF and records done_ev (optional) right after it, so
+ * that a batch can bound how many chains run at once.  Ordered phases, every
+ * Q_k^T formed by the BSOF workers; workers as for bsofi_dev_invert_ex. */
+int bsofi_dev_invert_gated(int n, int L, double *dA, int ldd, double *dtau, void *dws,
+                           void *stream, int workers, int slices, void *wait_ev, void *done_ev);
+
+/* One inversion split over two streams: BSOF (every Q_k^T formed) on
+ * chain_stream, then `handoff` recorded there and waited for on gemm_stream,
+ * which runs BSTRI and BSOI (FP64, or the mixed path when slices != 0). */
+int bsofi_dev_invert_two_streams(int n, int L, double *dA, int ldd, double *dtau, void *dws,
+                                 void *chain_stream, void *gemm_stream, void *handoff,
+                                 int workers, int slices);
+/* Launch plans of the calling thread without persistent GEMM kernels (BSOI
+ * and the BSTRI recurrence as per-step launches) while on != 0. */
+void bsofi_dev_set_nonpersistent(int on);
+
 /* Storage-sharded inversion (one inversion over several GPUs, none holding M
  * or M^{-1} whole).  The state (bsofi_dev_shard_state_bytes) holds the
  * compact factorization: block columns 0..L-2 with leading dimension 3n, the

@@ -93,10 +93,24 @@ Plan default_plan(int n, int L) {
   return Plan{bsoi, rec, 32, group};
 }
 
+// Plans of this thread's launches without persistent GEMM kernels (set by
+// pipelined batches): a persistent launch keeps every SM until it ends, so
+// another instance's cooperative BSOF launch could not start meanwhile.
+thread_local bool g_nonpersistent = false;
+
 Plan plan_for(int n, int L) {
-  std::lock_guard<std::mutex> lk(g_plan_mu);
-  auto it = g_plans.find({n, L});
-  return it == g_plans.end() ? default_plan(n, L) : it->second;
+  Plan p;
+  {
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    auto it = g_plans.find({n, L});
+    p = it == g_plans.end() ? default_plan(n, L) : it->second;
+  }
+  if (g_nonpersistent) {
+    if (p.bsoi == 0) p.bsoi = 3;  // per-step 128 x 128 (K stage 32)
+    if (p.bsoi == 5) p.bsoi = 2;  // per-step 64 x 64
+    if (p.bstri_cfg == 4) p.bstri_cfg = 0;  // per-step (or per-group) launches
+  }
+  return p;
 }
 
 // Diagnostics override of the BSOF worker count (0 = the plan's).
@@ -1055,6 +1069,43 @@ int bsofi_dev_invert_mixed(int n, int L, double* dA, int ldd, double* dtau, void
   void* oz = at<char>(dws, layout(n, L, ldd).total);
   return run_bsoi_mixed(n, L, dA, ldd, dws, oz, slices, (cudaStream_t)stream);
 }
+
+int bsofi_dev_invert_gated(int n, int L, double* dA, int ldd, double* dtau, void* dws,
+                           void* stream, int workers, int slices, void* wait_ev, void* done_ev) {
+  g_launches = 0;
+  const cudaStream_t st = (cudaStream_t)stream;
+  if (slices != 0 &&
+      (slices < kOzakiMinSlices || slices > kOzakiMaxSlices || 2 * n > kOzakiMaxK))
+    return (int)cudaErrorInvalidValue;
+  if (wait_ev) CKM(cudaStreamWaitEvent(st, (cudaEvent_t)wait_ev, 0));
+  int e = run_bsof(n, L, dA, ldd, dtau, dws, st, true, bsof_workers(n, L, workers));
+  if (e) return e;
+  if (done_ev) CKM(cudaEventRecord((cudaEvent_t)done_ev, st));
+  if ((e = run_bstri(n, L, dA, ldd, dws, st)) != 0) return e;
+  if (slices != 0)
+    return run_bsoi_mixed(n, L, dA, ldd, dws, at<char>(dws, layout(n, L, ldd).total), slices, st);
+  return run_bsoi(n, L, dA, ldd, dtau, dws, st, true);
+}
+
+int bsofi_dev_invert_two_streams(int n, int L, double* dA, int ldd, double* dtau, void* dws,
+                                 void* chain_stream, void* gemm_stream, void* handoff,
+                                 int workers, int slices) {
+  g_launches = 0;
+  const cudaStream_t hs = (cudaStream_t)chain_stream, gs = (cudaStream_t)gemm_stream;
+  if (slices != 0 &&
+      (slices < kOzakiMinSlices || slices > kOzakiMaxSlices || 2 * n > kOzakiMaxK))
+    return (int)cudaErrorInvalidValue;
+  int e = run_bsof(n, L, dA, ldd, dtau, dws, hs, true, bsof_workers(n, L, workers));
+  if (e) return e;
+  CKM(cudaEventRecord((cudaEvent_t)handoff, hs));
+  CKM(cudaStreamWaitEvent(gs, (cudaEvent_t)handoff, 0));
+  if ((e = run_bstri(n, L, dA, ldd, dws, gs)) != 0) return e;
+  if (slices != 0)
+    return run_bsoi_mixed(n, L, dA, ldd, dws, at<char>(dws, layout(n, L, ldd).total), slices, gs);
+  return run_bsoi(n, L, dA, ldd, dtau, dws, gs, true);
+}
+
+void bsofi_dev_set_nonpersistent(int on) { g_nonpersistent = on != 0; }
 
 int bsofi_dev_bsoftri_q_ex(int n, int L, double* dA, int ldd, double* dtau, void* dws,
                            void* stream, int workers) {

@@ -4,7 +4,8 @@
     python -m bsofi_b200.diag invert N_BLOCK L [REPS] [U]
     python -m bsofi_b200.diag invert-mixed N_BLOCK L [REPS] [SLICES]
     python -m bsofi_b200.diag split-phases N_BLOCK L [REPS]
-    python -m bsofi_b200.diag batch COUNT STREAMS [PRECISION]
+    python -m bsofi_b200.diag batch COUNT STREAMS [PRECISION [SIDE P]]
+    python -m bsofi_b200.diag shard-storage N_BLOCK L WORLD [U]
 
 bsof-timeline inverts a seeded Hubbard matrix (a random p-cyclic one when n is
 not a square) with bsofi_device_invert and prints, for the last run, the BSOF
@@ -20,7 +21,7 @@ import sys
 import numpy as np
 
 from . import _lib, api
-from .hubbard import hubbard_matrix, random_pcyclic
+from .hubbard import hubbard_blocks, hubbard_matrix, random_pcyclic
 
 
 def bsof_leaves(n, L):
@@ -156,6 +157,75 @@ def invert_mixed_timing(n, L, reps=3, U=4.0, slices=0):
             "bsoi_tflops": flops_bsoi(n, L) / bsoi / 1e9, "residual": res}
 
 
+def shard_storage_timing(n, L, world, U=4.0):
+    """The storage-sharded inversion's phases for `world` ranks, each rank's
+    share timed on its own on this GPU (CUDA events): the compact
+    factorization (every rank runs it), each rank's block columns of R^{-1},
+    each rank's BSOI rows, and the bytes each rank sends in the all-to-all.
+    Returns a dict; a rank's device time is factor + columns + rows."""
+    import torch
+    from . import shard
+    side = int(round(n ** 0.5))
+    N = n * L
+    # The packed blocks only (no dense N x N host matrix): the Hubbard chain
+    # (identity diagonal, -B_k below, +B_p in the corner) or random blocks.
+    if side * side == n:
+        B = hubbard_blocks(side, L, U, seed=1)
+        diag = np.broadcast_to(np.eye(n), (L, n, n))
+        sub = -B
+        sub[L - 1] = B[L - 1]
+    else:
+        rng = np.random.default_rng(1)
+        diag = rng.standard_normal((L, n, n)) + np.eye(n)[None]
+        sub = rng.standard_normal((L, n, n))
+    dev = torch.device("cuda:0")
+    st = torch.cuda.current_stream()
+    dD = torch.from_numpy(np.ascontiguousarray(np.transpose(diag, (0, 2, 1)))).to(dev)
+    dS = torch.from_numpy(np.ascontiguousarray(np.transpose(sub, (0, 2, 1)))).to(dev)
+    state = torch.empty(api.shard_state_bytes(n, L), dtype=torch.uint8, device=dev)
+
+    def timed(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        rc = fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        if rc != 0:
+            raise RuntimeError("shard phase failed (%d)" % rc)
+        return e0.elapsed_time(e1)
+
+    def factor():
+        return api.shard_factor(n, L, dD.data_ptr(), dS.data_ptr(), state.data_ptr(),
+                                st.cuda_stream)
+
+    timed(factor)  # warm-up
+    t_factor = timed(factor)
+    cols = shard.column_slabs(L, world)
+    bands = shard.bsoi_row_bands(n, L, world)
+    t_cols, sent, sends = [], [], []
+    for r, (c0, c1) in enumerate(cols):
+        slab = torch.empty(((c1 - c0) * n, max(c1 * n, 1)), dtype=torch.float64, device=dev)
+        t_cols.append(timed(lambda: api.shard_bstri_columns(
+            n, L, c0, c1, slab.data_ptr(), slab.shape[1], state.data_ptr(), st.cuda_stream))
+            if c1 > c0 else 0.0)
+        blocks = shard._send_blocks(slab, n, c0, c1, bands)
+        sent.append(8 * sum(b.numel() for q, b in enumerate(blocks) if q != r))
+        sends.append(blocks)
+        del slab
+    t_rows = []
+    for q, (r0, r1) in enumerate(bands):
+        band = torch.zeros((N, r1 - r0), dtype=torch.float64, device=dev)
+        shard._place(torch, band, n, cols, (r0, r1), [sends[r][q] for r in range(world)])
+        t_rows.append(timed(lambda: api.shard_bsoi_rows(
+            n, L, r0, r1, band.data_ptr(), r1 - r0, state.data_ptr(), st.cuda_stream))
+            if r1 > r0 else 0.0)
+        del band
+    return {"factor_ms": t_factor, "columns_ms": t_cols, "rows_ms": t_rows,
+            "sent_bytes": sent, "state_bytes": api.shard_state_bytes(n, L),
+            "cols": cols, "bands": bands}
+
+
 def split_phases_timing(n, L, reps=2):
     """bsofi_device_bsoftri then bsofi_device_bsoi as separate calls: BSOI then
     forms every Q_k^T from the stored reflectors and tau (build_leaf_t_kernel,
@@ -191,16 +261,20 @@ def split_phases_timing(n, L, reps=2):
     return best
 
 
-def batch_timing(count, streams, precision=0, reps=2, seed=77):
+def batch_timing(count, streams, precision=0, reps=2, seed=77, fixed=None):
     """The batched configuration (side in {8,..,16}, p in [8, 64], U in [2, 6]),
-    `count` instances per call with `streams` internal streams; inputs are
-    re-assembled from packed blocks before each timed call.  Returns the best
-    call's time in ms and the rate."""
+    or `count` instances of one size when fixed = (side, p) (U = 4), per call
+    with `streams` internal streams; inputs are re-assembled from packed
+    blocks before each timed call.  Returns the best call's time in ms and
+    the rate."""
     import torch
     from .hubbard import hubbard_blocks
     rng = np.random.default_rng(seed)
-    specs = [(int(rng.choice([8, 10, 12, 14, 16])), int(rng.integers(8, 65)),
-              float(rng.uniform(2.0, 6.0)), 9000 + i) for i in range(count)]
+    if fixed:
+        specs = [(fixed[0], fixed[1], 4.0, 9000 + i) for i in range(count)]
+    else:
+        specs = [(int(rng.choice([8, 10, 12, 14, 16])), int(rng.integers(8, 65)),
+                  float(rng.uniform(2.0, 6.0)), 9000 + i) for i in range(count)]
     dev = torch.device("cuda:0")
     ns, Ls, lds, bufs, packs, taus = [], [], [], [], [], []
     for side, L, U, sd in specs:
@@ -246,6 +320,17 @@ def main(argv):
         if a.startswith("--grouped="):
             _lib.load().bsofi_device_set_batch_grouped(int(a.split("=", 1)[1]))
             argv = [x for x in argv if x != a]
+    # --pipelined=1: batches with chains on high-priority streams and
+    # non-persistent GEMM phases.
+    for a in list(argv):
+        if a.startswith("--pipelined="):
+            _lib.load().bsofi_device_set_batch_pipelined(int(a.split("=", 1)[1]))
+            argv = [x for x in argv if x != a]
+    # --chains=K: at most K factorization chains of a batch in flight.
+    for a in list(argv):
+        if a.startswith("--chains="):
+            _lib.load().bsofi_device_set_batch_chains(int(a.split("=", 1)[1]))
+            argv = [x for x in argv if x != a]
     # --factor-warps=8: 16-wide BSOF leaves factored by all eight warps.
     for a in list(argv):
         if a.startswith("--factor-warps="):
@@ -283,9 +368,22 @@ def main(argv):
     if len(argv) >= 3 and argv[0] == "batch":
         count, streams = int(argv[1]), int(argv[2])
         precision = int(argv[3]) if len(argv) > 3 else 0
-        ms, rate = batch_timing(count, streams, precision)
-        print("batch of %d (streams %d, precision %d): %.1f ms = %.1f inversions/s"
-              % (count, streams, precision, ms, rate))
+        fixed = (int(argv[4]), int(argv[5])) if len(argv) > 5 else None
+        ms, rate = batch_timing(count, streams, precision, fixed=fixed)
+        print("batch of %d%s (streams %d, precision %d): %.1f ms = %.1f inversions/s"
+              % (count, " x side %d p %d" % fixed if fixed else "", streams, precision, ms, rate))
+        return 0
+    if len(argv) >= 4 and argv[0] == "shard-storage":
+        n, L, world = int(argv[1]), int(argv[2]), int(argv[3])
+        U = float(argv[4]) if len(argv) > 4 else 4.0
+        r = shard_storage_timing(n, L, world, U)
+        per_rank = [r["factor_ms"] + c + w for c, w in zip(r["columns_ms"], r["rows_ms"])]
+        print("n %d L %d over %d ranks: factor %.3f ms (every rank); columns %s ms; rows %s ms;"
+              " device time per rank %s ms (max %.3f); sent %s MB; state %.1f MB"
+              % (n, L, world, r["factor_ms"], ["%.3f" % x for x in r["columns_ms"]],
+                 ["%.3f" % x for x in r["rows_ms"]], ["%.2f" % x for x in per_rank],
+                 max(per_rank), ["%.0f" % (b / 1e6) for b in r["sent_bytes"]],
+                 r["state_bytes"] / 1e6))
         return 0
     if len(argv) >= 3 and argv[0] == "split-phases":
         n, L = int(argv[1]), int(argv[2])

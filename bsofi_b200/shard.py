@@ -23,7 +23,8 @@ whole, so N can exceed one GPU's memory:
      the column ranges balanced by the area of the block upper triangle;
   3. one all-to-all turns the column slabs into row bands (rows below c1 n
      of a slab are zero and are not sent);
-  4. rank r finishes rows bands[r] of M^{-1} with bsofi_shard_bsoi_rows.
+  4. rank r finishes rows bands[r] of M^{-1} with bsofi_shard_bsoi_rows,
+     the bands balanced by BSOI's work (the top rows cost twice the bottom).
 Per rank the device holds the state, its slab (about N^2 / (2 P) doubles)
 and its band (N^2 / P), plus the exchange buffers of the same sizes.
 """
@@ -48,6 +49,33 @@ def row_bands(N, world, align=128):
         u += cnt
         bands.append((r0, min(u * align, N)))
     return bands
+
+
+def bsoi_row_bands(n, L, world, align=128):
+    """Row bands [r0, r1) as row_bands gives them, but balanced by BSOI's
+    work instead of the row count: a row of block row b takes the 2n-deep
+    product in the L-1-b steps whose X(:,k) reaches it and only the n-deep
+    carry product in the other b (the orgqr zero structure), so its work is
+    proportional to 2L - 2 - b: the top rows cost about twice the bottom
+    ones."""
+    N = n * L
+    if N < 0 or world < 1 or align < 1:
+        raise ValueError("bsoi_row_bands: N >= 0, world >= 1, align >= 1")
+    units = (N + align - 1) // align
+    w = []
+    for u in range(units):
+        a, b = u * align, min((u + 1) * align, N)
+        w.append(sum(2 * L - 2 - i // n for i in range(a, b)))
+    total = float(sum(w))
+    cuts, acc, u = [0], 0.0, 0
+    for r in range(1, world):
+        target = total * r / world
+        while u < units and acc + w[u] / 2.0 <= target:
+            acc += w[u]
+            u += 1
+        cuts.append(u)
+    cuts.append(units)
+    return [(min(cuts[r] * align, N), min(cuts[r + 1] * align, N)) for r in range(world)]
 
 
 def gather_rows(torch, dist, Xc, N, bands, group=None):
@@ -212,7 +240,7 @@ def storage_sharded_invert(n, L, dD, dS, group=None, align=128):
     state = torch.empty(api.shard_state_bytes(n, L), dtype=torch.uint8, device=dev)
     rc = api.shard_factor(n, L, dD, dS, state.data_ptr(), stream)
     cols = column_slabs(L, world)
-    bands = row_bands(N, world, align)
+    bands = bsoi_row_bands(n, L, world, align)
     c0, c1 = cols[rank]
     slab = _new_slab(torch, n, c0, c1, dev)
     if rc == 0 and c1 > c0:
@@ -243,7 +271,7 @@ def storage_sharded_local(n, L, dD, dS, world, align=128):
     state = torch.empty(api.shard_state_bytes(n, L), dtype=torch.uint8, device=dev)
     rc = api.shard_factor(n, L, dD, dS, state.data_ptr(), stream)
     cols = column_slabs(L, world)
-    bands = row_bands(N, world, align)
+    bands = bsoi_row_bands(n, L, world, align)
     sends = []
     for c0, c1 in cols:
         slab = _new_slab(torch, n, c0, c1, dev)

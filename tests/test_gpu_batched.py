@@ -125,3 +125,113 @@ def test_grouped_bsoi_matches_per_instance(cuda_device):
     for M, a, b in zip(mats, Xg, Xp):
         assert rel_fro(a, b) < inverse_tolerance(M, b)
         assert residual(M, a) < 1e-13
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_chain_gate_gives_the_same_results(cuda_device, precision):
+    """bsofi_device_set_batch_chains(k) only orders the instances'
+    factorization chains (event waits between instances): the same kernels
+    run on the same data, so the results are bitwise those of the ungated
+    batch."""
+    import torch
+    from gpu_util import to_device_colmajor
+    lib = api.load()
+    rng = np.random.default_rng(321)
+    specs = [(int(rng.choice([16, 36, 64, 100, 144])), int(rng.integers(3, 12))) for _ in range(40)]
+    mats = [random_pcyclic(n, L, seed=2000 + i) for i, (n, L) in enumerate(specs)]
+    ns = [n for n, _ in specs]
+    Ls = [L for _, L in specs]
+    lds = [n * L for n, L in specs]
+
+    def run(chains):
+        lib.bsofi_device_set_batch_chains(chains)
+        try:
+            dA = [to_device_colmajor(torch, M, device=cuda_device) for M in mats]
+            dtau = [torch.zeros(n * L, dtype=torch.float64, device=cuda_device) for n, L in specs]
+            nb = api.batch_workspace_bytes(ns, Ls, lds, precision=precision)
+            ws = torch.zeros(nb // 8 + 1, dtype=torch.float64, device=cuda_device)
+            rc = api.device_invert_batched(ns, Ls, [t.data_ptr() for t in dA], lds,
+                                           [t.data_ptr() for t in dtau], ws.data_ptr(),
+                                           streams=8, precision=precision)
+            torch.cuda.synchronize()
+            assert rc == 0
+            return dA, dtau
+        finally:
+            lib.bsofi_device_set_batch_chains(0)
+
+    Ag, tg = run(3)
+    Au, tu = run(0)
+    for a, b in zip(Ag, Au):
+        assert torch.equal(a, b)
+    for a, b in zip(tg, tu):
+        assert torch.equal(a, b)
+    for M, A, (n, L) in zip(mats[:5], Ag[:5], specs[:5]):
+        X = A[:, :n * L].T.cpu().numpy()
+        assert residual(M, X) < (1e-13 if precision == 0 else 1e-12)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_pipelined_batch_matches_default(cuda_device, precision):
+    """bsofi_device_set_batch_pipelined(1) runs the chains on high-priority
+    streams and BSTRI/BSOI as per-step launches: each instance's inverse
+    matches the default batch's within the FP64 tolerance (the per-step and
+    persistent GEMMs may differ in rounding), tau bitwise (the same BSOF);
+    and the pipelined batch captured into a CUDA graph replays to the same
+    results."""
+    import torch
+    from gpu_util import from_device_colmajor, to_device_colmajor
+    lib = api.load()
+    rng = np.random.default_rng(654)
+    specs = [(int(rng.choice([16, 36, 64, 100, 144, 256])), int(rng.integers(3, 14)))
+             for _ in range(30)]
+    mats = [random_pcyclic(n, L, seed=3000 + i) for i, (n, L) in enumerate(specs)]
+    ns = [n for n, _ in specs]
+    Ls = [L for _, L in specs]
+    lds = [n * L for n, L in specs]
+
+    def buffers():
+        dA = [to_device_colmajor(torch, M, device=cuda_device) for M in mats]
+        dtau = [torch.zeros(n * L, dtype=torch.float64, device=cuda_device) for n, L in specs]
+        nb = api.batch_workspace_bytes(ns, Ls, lds, precision=precision)
+        ws = torch.zeros(nb // 8 + 1, dtype=torch.float64, device=cuda_device)
+        return dA, dtau, ws
+
+    def run(pipelined):
+        lib.bsofi_device_set_batch_pipelined(pipelined)
+        try:
+            dA, dtau, ws = buffers()
+            rc = api.device_invert_batched(ns, Ls, [t.data_ptr() for t in dA], lds,
+                                           [t.data_ptr() for t in dtau], ws.data_ptr(),
+                                           streams=8, precision=precision)
+            torch.cuda.synchronize()
+            assert rc == 0
+            return dA, dtau
+        finally:
+            lib.bsofi_device_set_batch_pipelined(0)
+
+    Ap, tp = run(1)
+    Ad, td = run(0)
+    for M, a, b, (n, L) in zip(mats, Ap, Ad, specs):
+        Xa = from_device_colmajor(a, n * L)
+        Xb = from_device_colmajor(b, n * L)
+        assert rel_fro(Xa, Xb) < max(inverse_tolerance(M, Xb), 1e-13 if precision == 0 else 1e-12)
+    for a, b in zip(tp, td):
+        assert torch.equal(a, b)
+    if precision == 0:
+        lib.bsofi_device_set_batch_pipelined(1)
+        try:
+            pristine = [to_device_colmajor(torch, M, device=cuda_device) for M in mats]
+            dA, dtau, ws = buffers()
+            g = api.BatchGraph(ns, Ls, [t.data_ptr() for t in dA], lds,
+                               [t.data_ptr() for t in dtau], ws.data_ptr(), streams=8)
+        finally:
+            lib.bsofi_device_set_batch_pipelined(0)
+        stream = torch.cuda.Stream()
+        for w, p0 in zip(dA, pristine):
+            w.copy_(p0)
+        torch.cuda.synchronize()
+        assert g.launch(stream.cuda_stream) == 0
+        stream.synchronize()
+        for a, b in zip(dA, Ap):
+            assert torch.equal(a, b)
+        g.close()

@@ -63,7 +63,7 @@ def test_storage_sharded_matches_single_gpu(cuda_device, n, L, world, kind):
     assert rc == 0 and info == 0
     torch.cuda.synchronize()
     covered = sorted((r0, r1) for r0, r1, _ in bands)
-    assert covered == shard.row_bands(N, world)
+    assert covered == shard.bsoi_row_bands(n, L, world)
     Xc = _compose(torch, bands, N, cuda_device)
     assert not torch.isnan(Xc).any()
     dA = to_device_colmajor(torch, M, device=cuda_device)

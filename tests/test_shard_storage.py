@@ -39,6 +39,28 @@ def test_column_slabs_cover_once(L, world):
         assert worst <= 0.8 * L * L / world
 
 
+@pytest.mark.parametrize("n,L,world", [(256, 32, 4), (400, 64, 8), (576, 80, 8), (8, 5, 4),
+                                       (100, 10, 1), (64, 16, 3)])
+def test_bsoi_row_bands_cover_once_balanced(n, L, world):
+    """Work-balanced BSOI bands: every row once, 128-aligned starts, and
+    (with a few tiles per rank) each band's work, sum over its rows of
+    2L - 2 - block row, within one tile's work of an equal share."""
+    N = n * L
+    bands = shard.bsoi_row_bands(n, L, world)
+    covered = []
+    for r0, r1 in bands:
+        assert 0 <= r0 <= r1 <= N
+        assert r0 % 128 == 0 or r0 == N
+        assert r1 % 128 == 0 or r1 == N
+        covered.extend(range(r0, r1))
+    assert covered == list(range(N))
+    work = [sum(2 * L - 2 - i // n for i in range(r0, r1)) for r0, r1 in bands]
+    tile = 128 * (2 * L - 2)
+    if N >= 4 * 128 * world:
+        share = sum(work) / world
+        assert max(abs(w - share) for w in work) <= tile
+
+
 def _state(n, L, kind, seed):
     M = hubbard_matrix(int(round(n ** 0.5)), L, 4.0, seed=seed) if kind == "hub" else \
         random_pcyclic(n, L, seed=seed)
