@@ -65,6 +65,8 @@ def parse():
                    help="timed mixed-precision inversions at the headline size (0 = skip)")
     p.add_argument("--c4-steps", type=int, default=4,
                    help="timed inversions at n=400, p=64, U=6 for the c4 key (0 = skip)")
+    p.add_argument("--shard-ranks", type=int, default=4,
+                   help="storage-sharded C4 emulated over this many ranks on one GPU (0: skip)")
     p.add_argument("--serve", type=int, default=1000,
                    help="requests in the served Poisson stream (0 = skip; 10000 = the full "
                         "serving configuration)")
@@ -426,6 +428,10 @@ def main():
             batched_mixed_mp["ratio_to_fp64_batched"] = (batched_mixed_mp["value"] /
                                                          batched_mixed["value"])
 
+    sharded = None
+    if args.shard_ranks > 0 and world == 1:
+        sharded = run_storage_sharded(args.shard_ranks, c4)
+
     served = None
     if args.serve > 0:
         served = run_serving(api, torch, dev, args.serve, args.serve_rate, 31 + rank,
@@ -461,6 +467,7 @@ def main():
                 "cpu_baseline": cpu, "e2e": e2e, "e2e_pageable": e2e_pageable,
                 "e2e_fp32": e2e_fp32,
                 "batched": batched, "batched_mixed_sizes": batched_mixed, "served": served,
+                "storage_sharded": sharded,
                 "mixed": mixed, "batched_mixed_precision": batched_mp,
                 "batched_mixed_sizes_mixed_precision": batched_mixed_mp,
                 "gpu_launches": launches_per_step * args.steps,
@@ -517,6 +524,28 @@ def run_c4(api, torch, dev, stream, steps, warmup, peak, rank):
             "frac": tf / peak if peak else None,
             "peak": peak, "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
             "residual": resid, "plan": plan}
+
+
+def run_storage_sharded(ranks, c4):
+    """The storage-sharded inversion at C4 (n = 400, p = 64, U = 6) for
+    `ranks` ranks, each rank's share (the replicated compact factorization,
+    its block columns of R^{-1}, its BSOI row band) timed in turn on this GPU
+    with CUDA events.  The all-to-all between ranks is not timed (one GPU):
+    its bytes per rank are reported."""
+    from bsofi_b200.diag import shard_storage_timing
+    r = shard_storage_timing(400, 64, ranks, 6.0)
+    per_rank = [r["factor_ms"] + c + w for c, w in zip(r["columns_ms"], r["rows_ms"])]
+    out = {"workload": "C4 (n=400, p=64, U=6, N=25600) split over %d ranks with no rank "
+                       "holding M or M^-1 whole; each rank's kernels run in turn on this GPU"
+                       % ranks,
+           "factor_ms": r["factor_ms"], "columns_ms": r["columns_ms"], "rows_ms": r["rows_ms"],
+           "device_ms_per_rank": per_rank, "max_device_ms": max(per_rank),
+           "sent_bytes_per_rank": r["sent_bytes"], "state_bytes": r["state_bytes"],
+           "not_timed": "the all-to-all of column slabs into row bands (one GPU here)"}
+    if c4 and c4.get("ms_per_inversion"):
+        out["single_gpu_ms"] = c4["ms_per_inversion"]
+        out["speedup_device_time"] = c4["ms_per_inversion"] / max(per_rank)
+    return out
 
 
 def run_mixed_single(api, torch, dev, stream, side, L, U, steps, warmup, rank, fp64_value):
