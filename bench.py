@@ -649,7 +649,7 @@ def run_batched_packed(api, torch, dev, specs, steps, stream, precision=0):
         with torch.cuda.stream(stream):
             e0.record(stream)
             rc = api.device_invert_batched(ns, Ls, [b.data_ptr() for b in bufs], lds,
-                                           [t.data_ptr() for t in taus], ws.data_ptr(), 8, sp,
+                                           [t.data_ptr() for t in taus], ws.data_ptr(), 16, sp,
                                            precision)
             e1.record(stream)
         torch.cuda.synchronize()

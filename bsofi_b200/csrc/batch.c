@@ -108,13 +108,15 @@ void bsofi_device_set_batch_chains(int k) {
   g_chains = k < 0 ? 0 : (k > MAX_GATE ? MAX_GATE : k);
 }
 
-/* Pipelined batches (1): each instance's factorization chain runs on a
- * highest-priority stream, chains of the instances dealt to one slot back to
- * back, and hands over by an event to the slot's ordinary stream for BSTRI
- * and BSOI, launched without persistent kernels (per-step GEMMs, whose CTAs
- * retire tile by tile, so that the next chains' cooperative launches find
- * SMs).  0: each instance's whole pipeline on one stream. */
-static int g_pipelined = 0;
+/* Pipelined batches (1, the default): each instance's factorization chain
+ * runs on a highest-priority stream, chains of the instances dealt to one
+ * slot back to back, and hands over by an event to the slot's ordinary
+ * stream for BSTRI and BSOI, launched without persistent kernels (per-step
+ * GEMMs, whose CTAs retire tile by tile, so that the next chains' cooperative
+ * launches find SMs).  Measured on the 256-instance batch of mixed sizes:
+ * 265.4 against 249.5 inversions/s (16 streams); 16 instances of one size
+ * unchanged.  0: each instance's whole pipeline on one stream. */
+static int g_pipelined = 1;
 void bsofi_device_set_batch_pipelined(int on) { g_pipelined = on ? 1 : 0; }
 
 unsigned long long bsofi_batch_workspace_bytes_ex(int count, const int *n, const int *L,

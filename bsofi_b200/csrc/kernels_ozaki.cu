@@ -20,8 +20,9 @@
 // of the same arithmetic matches exactly).  With S = 8 the inverse's
 // residual matches the FP64 path's order; S = 7 reaches about 1e-12.
 //
-// Kernels: ozaki_split_kernel writes the slices and exponents of both
-// operands (one launch); ozaki_gemm_kernel is a warp-specialised tcgen05
+// Kernels: ozaki_rowmax_kernel finds A's row maxima, ozaki_split_kernel
+// writes the slices and exponents of both operands; ozaki_gemm_kernel is a
+// warp-specialised tcgen05
 // kernel: warp 0 issues TMA tile loads (32-byte swizzle, K-major) into a
 // 4-stage mbarrier ring, each stage holding all S slices of A and B for 32 K
 // bytes; warp 1 issues the S(S+1)/2 MMAs of each 32-deep K step into S int32
@@ -56,6 +57,9 @@ struct OzSplitArgs {
   int8_t* a_out;       // S slices of M x Kp (row i of slice s at a_out + s*a_slice + i*Kp)
   long long a_slice;
   int* a_exp;          // M
+  // Row maxima of |A| as the bits of non-negative doubles (zeroed before
+  // the row-max kernel; bits >= those of +Inf flag a non-finite row).
+  unsigned long long* a_max;
   // B: K x N column-major; column j becomes row j of the B slices.
   const double* b;
   long long ldb;
@@ -64,7 +68,8 @@ struct OzSplitArgs {
   long long b_slice;
   int* b_exp;          // N
   int S;
-  int a_blocks;        // blocks [0, a_blocks) split A rows (32 each), the rest B columns (8 each)
+  int a_blocks;        // slice kernel: blocks [0, a_blocks) cut A tiles, the rest B columns
+  int a_chunks;        // 128-column chunks of Kp per 32-row A block
 };
 
 __device__ __forceinline__ double oz_a(const OzSplitArgs& s, int i, int k) {
@@ -102,58 +107,65 @@ __device__ __forceinline__ double pow2_neg(int e, bool& exact) {
   return exact ? ldexp(1.0, -e) : 1.0;
 }
 
-// A rows: a CTA of 256 threads takes 32 consecutive rows.  Pass 1, the row
-// maxima: warp w reads columns w, w+8, ... with lane = row (coalesced).
-// Pass 2, per chunk of 128 columns: the 32 x 128 block is staged in shared
-// memory by the same coalesced column reads, then warp w cuts rows
-// 4w..4w+3 with lane l on columns 4l..4l+3 (two 16-byte shared loads), and
-// writes one packed 4-byte word per slice: 128 contiguous bytes per warp.
-// B columns: one warp per column (K contiguous), eight per CTA.
+// A: two kernels over a 2-D grid of 32-row blocks, so that every SM has many
+// independent tiles in flight (the operand is read at close to HBM rate).
+// Row maxima: a CTA of 256 threads takes 32 rows x 64 columns, warp w the
+// columns w, w+8, ... with lane = row (coalesced, eight loads in flight),
+// and folds its maxima into a_max[row] with one atomicMax per row (the bits
+// of non-negative doubles order as the values; NaN and Inf, whose bits lie
+// at or above +Inf's, mark the row non-finite).  Slices: a CTA takes 32 rows
+// x 128 columns; the block is staged in shared memory by the same coalesced
+// column reads, then warp w cuts rows 4w..4w+3 with lane l on columns
+// 4l..4l+3 (two 16-byte shared loads) and writes one packed 4-byte word per
+// slice: 128 contiguous bytes per warp.  B columns: one warp per column
+// (K contiguous), eight per CTA, maximum and slices in the same warp.
 constexpr int OZ_SPLIT_ROWS = 32, OZ_SPLIT_THREADS = 256, OZ_SPLIT_CHUNK = 128;
+constexpr int OZ_MAX_COLS = 64;
 constexpr int OZ_SPLIT_LD = OZ_SPLIT_CHUNK + 2;  // row stride of the staged block (16-byte rows)
+constexpr unsigned long long OZ_INF_BITS = 0x7ff0000000000000ull;
+
+__global__ void __launch_bounds__(OZ_SPLIT_THREADS) ozaki_rowmax_kernel(OzSplitArgs s) {
+  __shared__ unsigned long long s_max[8][OZ_SPLIT_ROWS];
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int r0 = blockIdx.x * OZ_SPLIT_ROWS, k0 = blockIdx.y * OZ_MAX_COLS;
+  const int i = r0 + lane;
+  unsigned long long mx = 0;
+  if (i < s.M) {
+    double v[OZ_MAX_COLS / 8];
+#pragma unroll
+    for (int j = 0; j < OZ_MAX_COLS / 8; j++) {
+      const int k = k0 + warp + 8 * j;
+      v[j] = k < s.K ? oz_a(s, i, k) : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < OZ_MAX_COLS / 8; j++) {
+      const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(v[j]));
+      mx = b > mx ? b : mx;
+    }
+  }
+  s_max[warp][lane] = mx;
+  __syncthreads();
+  if (threadIdx.x < OZ_SPLIT_ROWS && r0 + (int)threadIdx.x < s.M) {
+    unsigned long long m = 0;
+#pragma unroll
+    for (int w = 0; w < 8; w++) m = s_max[w][threadIdx.x] > m ? s_max[w][threadIdx.x] : m;
+    if (m != 0) atomicMax(s.a_max + r0 + threadIdx.x, m);
+  }
+}
 
 __global__ void __launch_bounds__(OZ_SPLIT_THREADS) ozaki_split_kernel(OzSplitArgs s) {
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   if ((int)blockIdx.x < s.a_blocks) {
-    __shared__ double s_max[8][OZ_SPLIT_ROWS];
-    __shared__ int s_bad[8][OZ_SPLIT_ROWS];
     __shared__ __align__(16) double s_blk[OZ_SPLIT_ROWS][OZ_SPLIT_LD];
     __shared__ double s_sc[OZ_SPLIT_ROWS];
     __shared__ int s_e[OZ_SPLIT_ROWS];
-    const int r0 = blockIdx.x * OZ_SPLIT_ROWS;
-    {
-      const int i = r0 + lane;
-      double mx = 0.0;
-      bool bad = false;  // fmax drops NaN, so non-finite values are tracked apart
-      if (i < s.M) {
-        // Eight independent loads in flight per iteration (columns k, k+8, ...).
-        for (int k0 = warp; k0 < s.K; k0 += 64) {
-          double v[8];
-#pragma unroll
-          for (int j = 0; j < 8; j++) {
-            const int k = k0 + 8 * j;
-            v[j] = k < s.K ? oz_a(s, i, k) : 0.0;
-          }
-#pragma unroll
-          for (int j = 0; j < 8; j++) {
-            bad |= !isfinite(v[j]);
-            mx = fmax(mx, fabs(v[j]));
-          }
-        }
-      }
-      s_max[warp][lane] = mx;
-      s_bad[warp][lane] = bad;
-    }
-    __syncthreads();
+    const int r0 = ((int)blockIdx.x / s.a_chunks) * OZ_SPLIT_ROWS;
+    const int k0 = ((int)blockIdx.x % s.a_chunks) * OZ_SPLIT_CHUNK;
     if (threadIdx.x < OZ_SPLIT_ROWS) {
       const int lr = threadIdx.x, i = r0 + lr;
-      double mx = 0.0;
-      bool bad = false;
-#pragma unroll
-      for (int w = 0; w < 8; w++) {
-        mx = fmax(mx, s_max[w][lr]);
-        bad |= s_bad[w][lr] != 0;
-      }
+      const unsigned long long bits = i < s.M ? s.a_max[i] : 0ull;
+      const bool bad = bits >= OZ_INF_BITS;
+      const double mx = bad ? 0.0 : __longlong_as_double((long long)bits);
       int e = 0;
       if (!bad) frexp(mx, &e);
       // Scale 0 makes every slice of a zero or non-finite row zero.
@@ -161,48 +173,45 @@ __global__ void __launch_bounds__(OZ_SPLIT_THREADS) ozaki_split_kernel(OzSplitAr
       const double sc = pow2_neg(e, exact);
       s_sc[lr] = (bad || !(mx > 0.0)) ? 0.0 : (exact ? sc : -1.0);  // -1: ldexp per element
       s_e[lr] = e;
-      if (i < s.M) s.a_exp[i] = bad ? OZ_EXP_NONFINITE : e;
+      if (k0 == 0 && i < s.M) s.a_exp[i] = bad ? OZ_EXP_NONFINITE : e;
     }
-    for (int k0 = 0; k0 < s.Kp; k0 += OZ_SPLIT_CHUNK) {
-      __syncthreads();  // s_sc ready / the previous chunk consumed
-      {
-        const int i = r0 + lane;
-        double v[OZ_SPLIT_CHUNK / 8];  // all 16 loads of this warp in flight at once
+    {
+      const int i = r0 + lane;
+      double v[OZ_SPLIT_CHUNK / 8];  // all 16 loads of this warp in flight at once
 #pragma unroll
-        for (int j = 0; j < OZ_SPLIT_CHUNK / 8; j++) {
-          const int k = k0 + warp + 8 * j;
-          v[j] = (i < s.M && k < s.K) ? oz_a(s, i, k) : 0.0;
-        }
-#pragma unroll
-        for (int j = 0; j < OZ_SPLIT_CHUNK / 8; j++) s_blk[lane][warp + 8 * j] = v[j];
+      for (int j = 0; j < OZ_SPLIT_CHUNK / 8; j++) {
+        const int k = k0 + warp + 8 * j;
+        v[j] = (i < s.M && k < s.K) ? oz_a(s, i, k) : 0.0;
       }
-      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < OZ_SPLIT_CHUNK / 8; j++) s_blk[lane][warp + 8 * j] = v[j];
+    }
+    __syncthreads();
 #pragma unroll 1
-      for (int rr = 0; rr < 4; rr++) {
-        const int lr = 4 * warp + rr, i = r0 + lr;
-        if (i >= s.M) break;  // warp-uniform
-        // Kp is a multiple of 32 (4-column groups never straddle it); the last
-        // chunk may end before 128 columns.
-        if (k0 + 4 * lane >= s.Kp) continue;
-        const double sc = s_sc[lr];
-        const double2 p0 = *reinterpret_cast<const double2*>(&s_blk[lr][4 * lane]);
-        const double2 p1 = *reinterpret_cast<const double2*>(&s_blk[lr][4 * lane + 2]);
-        double r[4] = {p0.x, p0.y, p1.x, p1.y};
+    for (int rr = 0; rr < 4; rr++) {
+      const int lr = 4 * warp + rr, i = r0 + lr;
+      if (i >= s.M) break;  // warp-uniform
+      // Kp is a multiple of 32 (4-column groups never straddle it); the last
+      // chunk may end before 128 columns.
+      if (k0 + 4 * lane >= s.Kp) continue;
+      const double sc = s_sc[lr];
+      const double2 p0 = *reinterpret_cast<const double2*>(&s_blk[lr][4 * lane]);
+      const double2 p1 = *reinterpret_cast<const double2*>(&s_blk[lr][4 * lane + 2]);
+      double r[4] = {p0.x, p0.y, p1.x, p1.y};
 #pragma unroll
-        for (int q = 0; q < 4; q++)
-          r[q] = sc == 0.0 ? 0.0 : (sc > 0.0 ? r[q] * sc : ldexp(r[q], -s_e[lr]));
-        int8_t* dst = s.a_out + (long long)i * s.Kp + k0 + 4 * lane;
-        for (int sl = 0; sl < s.S; sl++) {
-          uint32_t word = 0;
+      for (int q = 0; q < 4; q++)
+        r[q] = sc == 0.0 ? 0.0 : (sc > 0.0 ? r[q] * sc : ldexp(r[q], -s_e[lr]));
+      int8_t* dst = s.a_out + (long long)i * s.Kp + k0 + 4 * lane;
+      for (int sl = 0; sl < s.S; sl++) {
+        uint32_t word = 0;
 #pragma unroll
-          for (int q = 0; q < 4; q++) {
-            const double t = r[q] * 128.0;
-            const double v = trunc(t);
-            r[q] = t - v;  // exact
-            word |= ((uint32_t)(int)v & 0xffu) << (8 * q);
-          }
-          *reinterpret_cast<uint32_t*>(dst + (long long)sl * s.a_slice) = word;
+        for (int q = 0; q < 4; q++) {
+          const double t = r[q] * 128.0;
+          const double v = trunc(t);
+          r[q] = t - v;  // exact
+          word |= ((uint32_t)(int)v & 0xffu) << (8 * q);
         }
+        *reinterpret_cast<uint32_t*>(dst + (long long)sl * s.a_slice) = word;
       }
     }
     return;
@@ -455,6 +464,7 @@ struct OzScratch {
   int8_t* b;
   int* ea;
   int* eb;
+  unsigned long long* amax;
 };
 
 OzScratch carve(void* base, int M, int N, int K, int S) {
@@ -468,6 +478,8 @@ OzScratch carve(void* base, int M, int N, int K, int S) {
   o.ea = reinterpret_cast<int*>(p);
   p += al256(sizeof(int) * (size_t)M);
   o.eb = reinterpret_cast<int*>(p);
+  p += al256(sizeof(int) * (size_t)N);
+  o.amax = reinterpret_cast<unsigned long long*>(p);
   return o;
 }
 
@@ -493,7 +505,7 @@ cudaError_t gemm_s(const CUtensorMap& ma, const CUtensorMap& mb, const OzGemmArg
 size_t ozaki_scratch_bytes(int M, int N, int K, int S) {
   const size_t Kp = (size_t)kpad(K);
   return al256((size_t)S * M * Kp) + al256((size_t)S * N * Kp) + al256(sizeof(int) * (size_t)M) +
-         al256(sizeof(int) * (size_t)N);
+         al256(sizeof(int) * (size_t)N) + al256(sizeof(unsigned long long) * (size_t)M);
 }
 
 cudaError_t launch_ozaki_product(const OzProduct& p, cudaStream_t st) {
@@ -523,11 +535,18 @@ cudaError_t launch_ozaki_product(const OzProduct& p, cudaStream_t st) {
   sa.b_slice = (long long)p.N * Kp;
   sa.b_exp = o.eb;
   sa.S = p.S;
-  sa.a_blocks = (p.M + OZ_SPLIT_ROWS - 1) / OZ_SPLIT_ROWS;
+  sa.a_max = o.amax;
+  const int row_blocks = (p.M + OZ_SPLIT_ROWS - 1) / OZ_SPLIT_ROWS;
+  sa.a_chunks = (Kp + OZ_SPLIT_CHUNK - 1) / OZ_SPLIT_CHUNK;
+  sa.a_blocks = row_blocks * sa.a_chunks;
   const int b_blocks = (p.N + 7) / 8;
-  ozaki_split_kernel<<<sa.a_blocks + b_blocks, OZ_SPLIT_THREADS, 0, st>>>(sa);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = cudaMemsetAsync(o.amax, 0, sizeof(unsigned long long) * (size_t)p.M, st);
   if (e != cudaSuccess) return e;
+  ozaki_rowmax_kernel<<<dim3(row_blocks, (p.K + OZ_MAX_COLS - 1) / OZ_MAX_COLS), OZ_SPLIT_THREADS,
+                        0, st>>>(sa);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  ozaki_split_kernel<<<sa.a_blocks + b_blocks, OZ_SPLIT_THREADS, 0, st>>>(sa);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
   CUtensorMap ma, mb;
   if ((e = slice_map(&ma, o.a, Kp, p.M, p.S, OZ_BM)) != cudaSuccess) return e;
   if ((e = slice_map(&mb, o.b, Kp, p.N, p.S, OZ_BN)) != cudaSuccess) return e;
@@ -556,6 +575,7 @@ cudaError_t launch_ozaki_product(const OzProduct& p, cudaStream_t st) {
 
 cudaError_t preload_ozaki(size_t* local) {
   cudaError_t e;
+  if ((e = preload_one(ozaki_rowmax_kernel, local)) != cudaSuccess) return e;
   if ((e = preload_one(ozaki_split_kernel, local)) != cudaSuccess) return e;
   if ((e = preload_one(ozaki_gemm_kernel<3>, local)) != cudaSuccess) return e;
   if ((e = preload_one(ozaki_gemm_kernel<4>, local)) != cudaSuccess) return e;

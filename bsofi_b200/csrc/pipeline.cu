@@ -863,7 +863,7 @@ int run_bsoi_mixed(int n, int L, double* dA, int ldd, void* ws, void* oz, int S,
     p.err = at<int>(ws, ly.info) + 2;
     if (g_timer.on) CKM(g_timer.mark(st));
     CKM(launch_ozaki_product(p, st));
-    g_launches += 2;  // the split and the product
+    g_launches += 3;  // the row maxima, the split and the product
     if (g_timer.on) CKM(g_timer.mark(st));
   }
   return bsoi_finish(n, L, dA, ldd, ws, st);
@@ -1219,7 +1219,7 @@ int bsofi_dev_selftest_ozaki(int M, int N, int K, const double* dA, int lda, con
   p.S = slices;
   p.scratch = scratch;
   p.err = derr;
-  g_launches = 2;
+  g_launches = 3;
   return (int)launch_ozaki_product(p, (cudaStream_t)stream);
 }
 

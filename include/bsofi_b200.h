@@ -309,20 +309,19 @@ int bsofi_device_invert_batched(int count, const int *n, const int *L, double *c
  * slower on a 256-instance batch of mixed sizes). */
 void bsofi_device_set_batch_grouped(int on);
 /* At most k instances' factorization chains (BSOF) of a batch in flight at
- * once (0: no bound beyond the stream count; at most 32); process-wide, no
- * reference counterpart.  A chain holds its SMs while it waits on its own
- * serial column steps, so bounding them leaves the other SMs to the GEMM
- * phases of instances whose chains are done.  Results are unchanged. */
+ * once (0, the default: no bound beyond the stream count; at most 32), for
+ * batches with bsofi_device_set_batch_pipelined(0); process-wide, no
+ * reference counterpart.  Results are unchanged.  (Measured: every bound
+ * slowed the batch; the chains' latency, not their SMs, limits it.) */
 void bsofi_device_set_batch_chains(int k);
-/* Pipelined batches (on = 1; process-wide, no reference counterpart): each
- * instance's factorization chain runs on a highest-priority stream of the
- * pool, the chains dealt to one stream back to back, and hands over by an
- * event to an ordinary stream for BSTRI and BSOI, which then run as per-step
- * launches instead of persistent kernels (a persistent kernel holds every SM
- * until it ends, so the next chains could not start).  on = 0, the default:
- * each instance's whole pipeline on one stream.  Results are unchanged up to
- * the launch plans' rounding (per-step and persistent BSOI compute the same
- * tiles). */
+/* Pipelined batches (on = 1, the default; process-wide, no reference
+ * counterpart): each instance's factorization chain runs on a
+ * highest-priority stream of the pool, the chains dealt to one stream back
+ * to back, and hands over by an event to an ordinary stream for BSTRI and
+ * BSOI, which then run as per-step launches instead of persistent kernels (a
+ * persistent kernel holds every SM until it ends, so the next chains could
+ * not start).  on = 0: each instance's whole pipeline on one stream.  The two
+ * agree to the launch plans' rounding (tau bitwise). */
 void bsofi_device_set_batch_pipelined(int on);
 /* The same batch at a chosen precision: 0 FP64 (as above), 1 mixed (every
  * instance as bsofi_device_invert_mixed with BSOFI_MIXED_SLICES slices).  The

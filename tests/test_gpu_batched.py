@@ -144,6 +144,7 @@ def test_chain_gate_gives_the_same_results(cuda_device, precision):
     lds = [n * L for n, L in specs]
 
     def run(chains):
+        lib.bsofi_device_set_batch_pipelined(0)  # the gate orders the one-stream pipelines
         lib.bsofi_device_set_batch_chains(chains)
         try:
             dA = [to_device_colmajor(torch, M, device=cuda_device) for M in mats]
@@ -158,6 +159,7 @@ def test_chain_gate_gives_the_same_results(cuda_device, precision):
             return dA, dtau
         finally:
             lib.bsofi_device_set_batch_chains(0)
+            lib.bsofi_device_set_batch_pipelined(1)
 
     Ag, tg = run(3)
     Au, tu = run(0)
@@ -172,12 +174,12 @@ def test_chain_gate_gives_the_same_results(cuda_device, precision):
 
 @pytest.mark.parametrize("precision", [0, 1])
 def test_pipelined_batch_matches_default(cuda_device, precision):
-    """bsofi_device_set_batch_pipelined(1) runs the chains on high-priority
-    streams and BSTRI/BSOI as per-step launches: each instance's inverse
-    matches the default batch's within the FP64 tolerance (the per-step and
-    persistent GEMMs may differ in rounding), tau bitwise (the same BSOF);
-    and the pipelined batch captured into a CUDA graph replays to the same
-    results."""
+    """Pipelined batches (the default: chains on high-priority streams,
+    BSTRI/BSOI as per-step launches) against bsofi_device_set_batch_pipelined(0)
+    (each instance on one stream, persistent GEMMs): each instance's inverse
+    agrees within the FP64 tolerance (the per-step and persistent GEMMs may
+    differ in rounding), tau bitwise (the same BSOF); and the pipelined batch
+    captured into a CUDA graph replays to the same results."""
     import torch
     from gpu_util import from_device_colmajor, to_device_colmajor
     lib = api.load()
@@ -207,7 +209,7 @@ def test_pipelined_batch_matches_default(cuda_device, precision):
             assert rc == 0
             return dA, dtau
         finally:
-            lib.bsofi_device_set_batch_pipelined(0)
+            lib.bsofi_device_set_batch_pipelined(1)
 
     Ap, tp = run(1)
     Ad, td = run(0)
@@ -225,7 +227,7 @@ def test_pipelined_batch_matches_default(cuda_device, precision):
             g = api.BatchGraph(ns, Ls, [t.data_ptr() for t in dA], lds,
                                [t.data_ptr() for t in dtau], ws.data_ptr(), streams=8)
         finally:
-            lib.bsofi_device_set_batch_pipelined(0)
+            lib.bsofi_device_set_batch_pipelined(1)
         stream = torch.cuda.Stream()
         for w, p0 in zip(dA, pristine):
             w.copy_(p0)
