@@ -70,7 +70,7 @@ def parse():
     p.add_argument("--serve", type=int, default=1000,
                    help="requests in the served Poisson stream (0 = skip; 10000 = the full "
                         "serving configuration)")
-    p.add_argument("--serve-rate", type=float, default=16.0, help="mean arrivals per second")
+    p.add_argument("--serve-rate", type=float, default=12.0, help="mean arrivals per second")
     p.add_argument("--serve-mixed", type=float, default=0.5,
                    help="fraction of served requests at mixed precision")
     p.add_argument("--serve-only", action="store_true",
