@@ -90,19 +90,19 @@ static size_t inst_ws(int n, int L, int ldda, int precision) {
                         : bsofi_dev_ws_bytes(n, L, ldda);
 }
 
-/* FP64 batches run each instance's BSOI as its own launch on the instance's
- * stream (0, the default: it overlaps the other instances' latency-bound
- * factorization chains) or all BSOI as one grouped persistent launch per tile
- * shape after every factorization (1: no wave tails between instances, but no
- * overlap with the chains; measured slower on a 256-instance batch of mixed
- * sizes, 227.8 against 248.5 inversions/s). */
+/* FP64 batches run each instance's BSOI as its own launch (0, the default:
+ * it overlaps the other instances' latency-bound factorization chains) or all
+ * BSOI as one grouped persistent launch per tile shape after every
+ * factorization (1: no wave tails between instances, but no overlap with the
+ * chains; measured slower on a 256-instance batch of mixed sizes, 227.8
+ * against 248.5 inversions/s). */
 static int g_grouped = 0;
 void bsofi_device_set_batch_grouped(int on) { g_grouped = on ? 1 : 0; }
 
-/* At most this many instances' factorization chains run at once (0: as many
- * as there are streams).  A BSOF launch holds its SMs (one CTA each) for the
- * whole latency-bound chain, so chains beyond a few only take SMs from the
- * other instances' GEMM phases. */
+/* At most this many instances' factorization chains run at once in
+ * one-stream-per-instance batches (0, the default: as many as there are
+ * streams).  Every bound measured slower (the batch is held by the chains'
+ * latency, not by the SMs their launches occupy); kept for diagnostics. */
 static int g_chains = 0;
 void bsofi_device_set_batch_chains(int k) {
   g_chains = k < 0 ? 0 : (k > MAX_GATE ? MAX_GATE : k);

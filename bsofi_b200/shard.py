@@ -19,14 +19,15 @@ whole, so N can exceed one GPU's memory:
      diagonal inverses, the row multipliers W_i and the last-column terms Z_i;
   2. rank r computes block columns cols[r] = [c0, c1) of X = R^{-1} (rows
      0 .. c1 n - 1; BSTRI's row recurrence, src/bsofi_cpu.c:146-177, read by
-     columns: X_{i,c} = W_i X_{i+1,c}, plus Z_i in the last column), with
-     the column ranges balanced by the area of the block upper triangle;
+     columns: X_{i,c} = W_i X_{i+1,c}, plus Z_i in the last column), the
+     column ranges chosen to minimise the largest stored slab;
   3. one all-to-all turns the column slabs into row bands (rows below c1 n
      of a slab are zero and are not sent);
   4. rank r finishes rows bands[r] of M^{-1} with bsofi_shard_bsoi_rows,
      the bands balanced by BSOI's work (the top rows cost twice the bottom).
-Per rank the device holds the state, its slab (about N^2 / (2 P) doubles)
-and its band (N^2 / P), plus the exchange buffers of the same sizes.
+Per rank the device holds the state, its slab (at most about 0.6 N^2 / P
+doubles at P = 8) and its band (about N^2 / P), plus the exchange buffers of
+the same sizes.
 """
 import collections
 
