@@ -1177,4 +1177,6 @@ void bsofi_device_set_bstri_overlap(int on) { bsofi_dev_set_bstri_overlap(on); }
 
 void bsofi_device_set_bsof_factor_warps(int warps) { bsofi_dev_set_bsof_factor_warps(warps); }
 
+void bsofi_device_set_gemm_k16(int on) { bsofi_dev_set_gemm_k16(on); }
+
 void bsofi_device_set_wait_test(int on) { bsofi_dev_set_wait_test(on); }

@@ -54,6 +54,18 @@ BSOFI_DEVINL void dmma_16x8x8(double (&d)[4], double a0, double a1, double a2, d
       : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
 }
 
+// D = A(16x16, row) * B(16x8, col) + D, FP64 (the sm_90+ shape with twice
+// the K of m16n8k8): a[2q+h] = A[g+8h][t+4q], b[q] = B[t+4q][g] (q = 0..3),
+// d as for m16n8k8.
+BSOFI_DEVINL void dmma_16x8x16(double (&d)[4], const double (&a)[8], const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 "
+      "{%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, {%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]),
+        "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
 // D = A(8x4, row) * B(4x8, col) + D, FP64.  a0 = A[g][t]; b0 = B[t][g];
 // d0, d1 = D[g][2t], D[g][2t+1].
 BSOFI_DEVINL void dmma_8x8x4(double (&d)[2], double a0, double b0) {

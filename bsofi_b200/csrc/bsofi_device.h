@@ -110,6 +110,8 @@ int bsofi_dev_invert_two_streams(int n, int L, double *dA, int ldd, double *dtau
 /* Launch plans of the calling thread without persistent GEMM kernels (BSOI
  * and the BSTRI recurrence as per-step launches) while on != 0. */
 void bsofi_dev_set_nonpersistent(int on);
+/* FP64 tile engine steps: mma.sync m16n8k8 (0) or m16n8k16 (1). */
+void bsofi_dev_set_gemm_k16(int on);
 
 /* Storage-sharded inversion (one inversion over several GPUs, none holding M
  * or M^{-1} whole).  The state (bsofi_dev_shard_state_bytes) holds the

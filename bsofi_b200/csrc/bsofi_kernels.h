@@ -120,6 +120,10 @@ cudaError_t launch_trtri_blocks(double* A, long long ld, int n, long long bstrid
                                 int nblk, int* info, double* tmp, cudaStream_t st, int boff = 0);
 
 // cfg: 0 = choose by tile count, 1 = 128x128 (K stage 16), 2 = 64x64, 3 = 128x128 (K stage 32).
+// Tile engine steps of every later launch: m16n8k8 (0, the default) or
+// m16n8k16 (1); process-wide.
+void gemm_set_k16(int on);
+bool gemm_k16();
 cudaError_t launch_gemm(const GemmDims& d, const GemmA& a, const GemmB& b,
                         const GemmC& c, int batch, int cfg, cudaStream_t st);
 cudaError_t gemm_init_attributes();

@@ -52,9 +52,14 @@ struct GemmDims {
   int M, N, K;
 };
 
-template <int BM_, int BN_, int WARPS_M_, int WARPS_N_, int STAGES_, int BK_ = 16>
+// K16: the inner product steps use mma.sync m16n8k16 (16-deep K per
+// instruction) instead of m16n8k8.
+template <int BM_, int BN_, int WARPS_M_, int WARPS_N_, int STAGES_, int BK_ = 16,
+          bool K16_ = false>
 struct TileCfg {
   static constexpr int BM = BM_, BN = BN_, BK = BK_;
+  static constexpr bool K16 = K16_;
+  static_assert(!K16_ || BK_ % 16 == 0, "K16 needs 16-deep stages");
   static constexpr int WARPS_M = WARPS_M_, WARPS_N = WARPS_N_;
   static constexpr int THREADS = 32 * WARPS_M * WARPS_N;
   static constexpr int STAGES = STAGES_;
@@ -72,6 +77,10 @@ struct TileCfg {
 using CfgL = TileCfg<128, 128, 2, 4, 3>;  // 256 threads, warp tile 64x32
 using CfgM = TileCfg<128, 128, 2, 4, 3, 32>;  // 256 threads, warp tile 64x32, K stage 32
 using CfgS = TileCfg<64, 64, 2, 2, 3>;    // 128 threads, warp tile 32x32
+// The same tiles with m16n8k16 steps.
+using CfgL16 = TileCfg<128, 128, 2, 4, 3, 16, true>;
+using CfgM16 = TileCfg<128, 128, 2, 4, 3, 32, true>;
+using CfgS16 = TileCfg<64, 64, 2, 2, 3, 16, true>;
 
 BSOFI_DEVINL int clamp02(long long v) { return v < 0 ? 0 : (v > 2 ? 2 : (int)v); }
 
@@ -208,49 +217,83 @@ BSOFI_DEVINL void gemm_tile(const GemmDims& d, const GemmA& a, const GemmB& b,
     __syncthreads();
     const double* tA = sA + (it % Cfg::STAGES) * Cfg::A_STAGE + wm * Cfg::WTM + g;
     const double* tB = sB + (it % Cfg::STAGES) * Cfg::B_STAGE + (wn * Cfg::WTN + g) * Cfg::SB + t;
+    if constexpr (Cfg::K16) {
 #pragma unroll
-    for (int k8 = 0; k8 < Cfg::BK / 8; k8++) {
-      // With 32-deep stages the next stage's B loads are issued after the
-      // first k8 step's DMMAs and its A loads after the second, so the tensor
-      // pipe has work queued while the warp computes addresses (measured: -6%
-      // on 128x128 K32 tiles; with 16-deep stages issuing them first is
-      // faster).
-      {
-        // One commit group per iteration holding both of the stage's loads:
-        // the group is committed after the later of the two.
-        constexpr int KA = Cfg::BK >= 32 ? 2 : 0, KB = Cfg::BK >= 32 ? 1 : 0;
-        constexpr int KC = KA > KB ? KA : KB;
-        int nx = it + Cfg::STAGES - 1;
-        if (k8 == KA && nx < nkt) {
-          int s = nx % Cfg::STAGES;
-          int k0 = (kt0 + nx) * Cfg::BK;
-          load_a_tile<Cfg, ALIGNED>(sA + s * Cfg::A_STAGE, a, pa0, pa1, d.M, d.K, m0, k0);
+      for (int k16 = 0; k16 < Cfg::BK / 16; k16++) {
+        // Next stage's loads: after the first 16-deep step's DMMAs when a
+        // stage holds two, else first.
+        if (k16 == (Cfg::BK >= 32 ? 1 : 0)) {
+          const int nx = it + Cfg::STAGES - 1;
+          if (nx < nkt) {
+            const int s = nx % Cfg::STAGES;
+            const int k0 = (kt0 + nx) * Cfg::BK;
+            load_b_tile<Cfg, ALIGNED>(sB + s * Cfg::B_STAGE, b, pb, d.N, d.K, k0, n0);
+            load_a_tile<Cfg, ALIGNED>(sA + s * Cfg::A_STAGE, a, pa0, pa1, d.M, d.K, m0, k0);
+          }
+          cp_async_commit();
         }
-        if (k8 == KB && nx < nkt) {
-          int s = nx % Cfg::STAGES;
-          int k0 = (kt0 + nx) * Cfg::BK;
-          load_b_tile<Cfg, ALIGNED>(sB + s * Cfg::B_STAGE, b, pb, d.N, d.K, k0, n0);
-        }
-        if (k8 == KC) cp_async_commit();
-      }
-      double af[Cfg::MT][4], bf[Cfg::NT][2];
-#pragma unroll
-      for (int i = 0; i < Cfg::MT; i++) {
-        af[i][0] = tA[(k8 * 8 + t) * Cfg::SA + i * 16];
-        af[i][1] = tA[(k8 * 8 + t) * Cfg::SA + i * 16 + 8];
-        af[i][2] = tA[(k8 * 8 + t + 4) * Cfg::SA + i * 16];
-        af[i][3] = tA[(k8 * 8 + t + 4) * Cfg::SA + i * 16 + 8];
-      }
-#pragma unroll
-      for (int j = 0; j < Cfg::NT; j++) {
-        bf[j][0] = tB[j * 8 * Cfg::SB + k8 * 8];
-        bf[j][1] = tB[j * 8 * Cfg::SB + k8 * 8 + 4];
-      }
-#pragma unroll
-      for (int i = 0; i < Cfg::MT; i++)
+        double bf[Cfg::NT][4];
 #pragma unroll
         for (int j = 0; j < Cfg::NT; j++)
-          dmma_16x8x8(acc[i][j], af[i][0], af[i][1], af[i][2], af[i][3], bf[j][0], bf[j][1]);
+#pragma unroll
+          for (int q = 0; q < 4; q++) bf[j][q] = tB[j * 8 * Cfg::SB + k16 * 16 + 4 * q];
+#pragma unroll
+        for (int i = 0; i < Cfg::MT; i++) {
+          double af[8];
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            af[2 * q] = tA[(k16 * 16 + t + 4 * q) * Cfg::SA + i * 16];
+            af[2 * q + 1] = tA[(k16 * 16 + t + 4 * q) * Cfg::SA + i * 16 + 8];
+          }
+#pragma unroll
+          for (int j = 0; j < Cfg::NT; j++) dmma_16x8x16(acc[i][j], af, bf[j]);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k8 = 0; k8 < Cfg::BK / 8; k8++) {
+        // With 32-deep stages the next stage's B loads are issued after the
+        // first k8 step's DMMAs and its A loads after the second, so the tensor
+        // pipe has work queued while the warp computes addresses (measured: -6%
+        // on 128x128 K32 tiles; with 16-deep stages issuing them first is
+        // faster).
+        {
+          // One commit group per iteration holding both of the stage's loads:
+          // the group is committed after the later of the two.
+          constexpr int KA = Cfg::BK >= 32 ? 2 : 0, KB = Cfg::BK >= 32 ? 1 : 0;
+          constexpr int KC = KA > KB ? KA : KB;
+          int nx = it + Cfg::STAGES - 1;
+          if (k8 == KA && nx < nkt) {
+            int s = nx % Cfg::STAGES;
+            int k0 = (kt0 + nx) * Cfg::BK;
+            load_a_tile<Cfg, ALIGNED>(sA + s * Cfg::A_STAGE, a, pa0, pa1, d.M, d.K, m0, k0);
+          }
+          if (k8 == KB && nx < nkt) {
+            int s = nx % Cfg::STAGES;
+            int k0 = (kt0 + nx) * Cfg::BK;
+            load_b_tile<Cfg, ALIGNED>(sB + s * Cfg::B_STAGE, b, pb, d.N, d.K, k0, n0);
+          }
+          if (k8 == KC) cp_async_commit();
+        }
+        double af[Cfg::MT][4], bf[Cfg::NT][2];
+#pragma unroll
+        for (int i = 0; i < Cfg::MT; i++) {
+          af[i][0] = tA[(k8 * 8 + t) * Cfg::SA + i * 16];
+          af[i][1] = tA[(k8 * 8 + t) * Cfg::SA + i * 16 + 8];
+          af[i][2] = tA[(k8 * 8 + t + 4) * Cfg::SA + i * 16];
+          af[i][3] = tA[(k8 * 8 + t + 4) * Cfg::SA + i * 16 + 8];
+        }
+#pragma unroll
+        for (int j = 0; j < Cfg::NT; j++) {
+          bf[j][0] = tB[j * 8 * Cfg::SB + k8 * 8];
+          bf[j][1] = tB[j * 8 * Cfg::SB + k8 * 8 + 4];
+        }
+#pragma unroll
+        for (int i = 0; i < Cfg::MT; i++)
+#pragma unroll
+          for (int j = 0; j < Cfg::NT; j++)
+            dmma_16x8x8(acc[i][j], af[i][0], af[i][1], af[i][2], af[i][3], bf[j][0], bf[j][1]);
+      }
     }
   }
   cp_async_wait<0>();

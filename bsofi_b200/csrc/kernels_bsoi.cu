@@ -171,6 +171,10 @@ cudaError_t launch_bsoi_persistent(double* A, long long ld, double* carry0, doub
   const bool al = ((uintptr_t)A % 16 == 0) && ((uintptr_t)carry0 % 16 == 0) &&
                   ((uintptr_t)carry1 % 16 == 0) && ((uintptr_t)G % 16 == 0) && ld % 2 == 0 &&
                   ldc % 2 == 0 && n % 2 == 0;
+  if (gemm_k16()) {
+    if (small) return al ? launch_al<CfgS16, true>(s, st) : launch_al<CfgS16, false>(s, st);
+    return al ? launch_al<CfgM16, true>(s, st) : launch_al<CfgM16, false>(s, st);
+  }
   if (small) return al ? launch_al<CfgS, true>(s, st) : launch_al<CfgS, false>(s, st);
   return al ? launch_al<CfgM, true>(s, st) : launch_al<CfgM, false>(s, st);
 }
@@ -307,7 +311,11 @@ cudaError_t preload_bsoi(size_t* local) {
   if ((e = preload_one(bsoi_persistent_kernel<CfgM, true>, local)) != cudaSuccess) return e;
   if ((e = preload_one(bsoi_persistent_kernel<CfgM, false>, local)) != cudaSuccess) return e;
   if ((e = preload_one(bsoi_persistent_kernel<CfgS, true>, local)) != cudaSuccess) return e;
-  return preload_one(bsoi_persistent_kernel<CfgS, false>, local);
+  if ((e = preload_one(bsoi_persistent_kernel<CfgS, false>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(bsoi_persistent_kernel<CfgM16, true>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(bsoi_persistent_kernel<CfgM16, false>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(bsoi_persistent_kernel<CfgS16, true>, local)) != cudaSuccess) return e;
+  return preload_one(bsoi_persistent_kernel<CfgS16, false>, local);
 }
 
 }  // namespace bsofi

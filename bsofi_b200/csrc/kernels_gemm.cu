@@ -1,7 +1,14 @@
 // Launch wrappers for the FP64 DMMA tile engine (gemm.cuh).
+#include <atomic>
+
 #include "bsofi_kernels.h"
 
 namespace bsofi {
+
+// Tile engine steps: m16n8k8 (0, the default) or m16n8k16 (1); process-wide.
+static std::atomic<int> g_k16{0};
+void gemm_set_k16(int on) { g_k16.store(on ? 1 : 0); }
+bool gemm_k16() { return g_k16.load() != 0; }
 
 template <class Cfg, bool ALIGNED>
 __global__ void __launch_bounds__(Cfg::THREADS) gemm_kernel(GemmDims d, GemmA a, GemmB b,
@@ -28,6 +35,12 @@ cudaError_t gemm_init_attributes() {
   if ((e = set_attr<CfgM, false>()) != cudaSuccess) return e;
   if ((e = set_attr<CfgS, true>()) != cudaSuccess) return e;
   if ((e = set_attr<CfgS, false>()) != cudaSuccess) return e;
+  if ((e = set_attr<CfgL16, true>()) != cudaSuccess) return e;
+  if ((e = set_attr<CfgL16, false>()) != cudaSuccess) return e;
+  if ((e = set_attr<CfgM16, true>()) != cudaSuccess) return e;
+  if ((e = set_attr<CfgM16, false>()) != cudaSuccess) return e;
+  if ((e = set_attr<CfgS16, true>()) != cudaSuccess) return e;
+  if ((e = set_attr<CfgS16, false>()) != cudaSuccess) return e;
   once.mark(dev);
   return cudaSuccess;
 }
@@ -58,6 +71,11 @@ cudaError_t launch_gemm(const GemmDims& d, const GemmA& a, const GemmB& b, const
     long long tilesL = (long long)((d.M + 127) / 128) * ((d.N + 127) / 128) * batch;
     cfg = (tilesL >= 148) ? 3 : 2;
   }
+  if (gemm_k16()) {
+    if (cfg == 1) return run<CfgL16>(d, a, b, c, batch, st);
+    if (cfg == 3) return run<CfgM16>(d, a, b, c, batch, st);
+    return run<CfgS16>(d, a, b, c, batch, st);
+  }
   if (cfg == 1) return run<CfgL>(d, a, b, c, batch, st);
   if (cfg == 3) return run<CfgM>(d, a, b, c, batch, st);
   return run<CfgS>(d, a, b, c, batch, st);
@@ -70,7 +88,13 @@ cudaError_t preload_gemm(size_t* local) {
   if ((e = preload_one(gemm_kernel<CfgM, true>, local)) != cudaSuccess) return e;
   if ((e = preload_one(gemm_kernel<CfgM, false>, local)) != cudaSuccess) return e;
   if ((e = preload_one(gemm_kernel<CfgS, true>, local)) != cudaSuccess) return e;
-  return preload_one(gemm_kernel<CfgS, false>, local);
+  if ((e = preload_one(gemm_kernel<CfgS, false>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(gemm_kernel<CfgL16, true>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(gemm_kernel<CfgL16, false>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(gemm_kernel<CfgM16, true>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(gemm_kernel<CfgM16, false>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(gemm_kernel<CfgS16, true>, local)) != cudaSuccess) return e;
+  return preload_one(gemm_kernel<CfgS16, false>, local);
 }
 
 }  // namespace bsofi

@@ -1107,6 +1107,8 @@ int bsofi_dev_invert_two_streams(int n, int L, double* dA, int ldd, double* dtau
 
 void bsofi_dev_set_nonpersistent(int on) { g_nonpersistent = on != 0; }
 
+void bsofi_dev_set_gemm_k16(int on) { gemm_set_k16(on); }
+
 int bsofi_dev_bsoftri_q_ex(int n, int L, double* dA, int ldd, double* dtau, void* dws,
                            void* stream, int workers) {
   g_launches = 0;

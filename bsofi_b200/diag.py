@@ -326,6 +326,11 @@ def main(argv):
         if a.startswith("--pipelined="):
             _lib.load().bsofi_device_set_batch_pipelined(int(a.split("=", 1)[1]))
             argv = [x for x in argv if x != a]
+    # --k16=1: the FP64 tile engine with mma.sync m16n8k16 steps.
+    for a in list(argv):
+        if a.startswith("--k16="):
+            _lib.load().bsofi_device_set_gemm_k16(int(a.split("=", 1)[1]))
+            argv = [x for x in argv if x != a]
     # --chains=K: at most K factorization chains of a batch in flight.
     for a in list(argv):
         if a.startswith("--chains="):

@@ -486,6 +486,11 @@ void bsofi_device_set_bstri_overlap(int on);
  * next leaf's tile meanwhile) or 8 (the tile is staged after the
  * factorization).  Results are the same either way to rounding.  Process-wide. */
 void bsofi_device_set_bsof_factor_warps(int warps);
+/* FP64 tile engine instruction shape (diagnostics, no reference
+ * counterpart; process-wide): mma.sync m16n8k8 steps (0, the default) or
+ * m16n8k16 (1: half the instructions, each 16 deep in K), for every GEMM
+ * launch and persistent BSOI launch that follows. */
+void bsofi_device_set_gemm_k16(int on);
 /* Diagnostics (no reference counterpart): with on = 1, the persistent BSOI
  * launches made by this thread wait, in every step after the first, on a
  * zeroed workspace word that nothing writes, under a short poll limit (about

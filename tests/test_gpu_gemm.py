@@ -37,3 +37,54 @@ def test_gemm_engine(cuda_device, M, N, K, lda, ldb, ldc, ua, ub, tile):
     out = Ct[:, :M].T
     err = float((out - ref).abs().max() / ref.abs().max())
     assert err < 1e-14, err
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("M,N,K,lda,ldb,ldc,ua,ub,tile", [
+    (128, 128, 128, 128, 128, 128, 0, 0, 1),
+    (128, 128, 128, 128, 128, 128, 0, 0, 3),
+    (64, 64, 64, 64, 64, 64, 0, 0, 2),
+    (257, 129, 300, 260, 302, 258, 0, 0, 3),
+    (513, 200, 96, 513, 97, 513, 0, 0, 2),      # odd leading dimensions
+    (256, 256, 256, 256, 256, 256, 1, 0, 3),    # upper-triangular A
+    (192, 320, 192, 192, 192, 192, 0, 1, 2),    # upper-triangular B
+    (150, 150, 150, 151, 151, 151, 1, 1, 0),
+])
+def test_gemm_engine_k16(cuda_device, M, N, K, lda, ldb, ldc, ua, ub, tile):
+    """The tile engine with mma.sync m16n8k16 steps
+    (bsofi_device_set_gemm_k16(1)) against torch FP64 matmul."""
+    lib = api.load()
+    lib.bsofi_device_set_gemm_k16(1)
+    try:
+        test_gemm_engine(cuda_device, M, N, K, lda, ldb, ldc, ua, ub, tile)
+    finally:
+        lib.bsofi_device_set_gemm_k16(0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,L", [(256, 8), (100, 12), (400, 6), (33, 7)])
+def test_inversion_with_k16_steps(cuda_device, n, L):
+    """A whole inversion with m16n8k16 steps in every GEMM and BSOI launch
+    against the default engine: within the FP64 tolerance, residual at the
+    FP64 level."""
+    import torch
+    from bsofi_b200.hubbard import random_pcyclic
+    from conftest import inverse_tolerance, rel_fro, residual
+    from gpu_util import from_device_colmajor, to_device_colmajor
+    lib = api.load()
+    N = n * L
+    M = random_pcyclic(n, L, seed=41 + n)
+    out = []
+    for k16 in (1, 0):
+        lib.bsofi_device_set_gemm_k16(k16)
+        try:
+            dA = to_device_colmajor(torch, M, device=cuda_device)
+            dtau = torch.zeros(N, dtype=torch.float64, device=cuda_device)
+            ws = torch.empty(api.workspace_bytes(n, L, N), dtype=torch.uint8, device=cuda_device)
+            assert api.device_invert(n, L, dA.data_ptr(), N, dtau.data_ptr(), ws.data_ptr()) == 0
+            torch.cuda.synchronize()
+            out.append(from_device_colmajor(dA, N))
+        finally:
+            lib.bsofi_device_set_gemm_k16(0)
+    assert rel_fro(out[0], out[1]) < inverse_tolerance(M, out[1])
+    assert residual(M, out[0]) < 1e-13
