@@ -566,7 +566,7 @@ BSOFI_DEVINL void apply_qt_mma(double* sV, double* sC, const double (&a)[R][16],
       __syncthreads();
     }
     constexpr int RW = PR / BW;
-#pragma unroll 1
+#pragma unroll
     for (int m0 = warp * RW; m0 < (warp + 1) * RW; m0 += 16) {
 #pragma unroll
       for (int j = 0; j < 2; j++) {
@@ -634,13 +634,18 @@ BSOFI_DEVINL void apply_qt_mma8(double* sV, double* sC, const double (&a)[R][8],
   }
   __syncthreads();
   {
-    double acc[2] = {0.0, 0.0};
+    // Four independent accumulators over interleaved 4-deep K steps, so the
+    // DMMAs of a warp do not wait on each other's results.
+    static_assert(KW % 16 == 0, "8-wide W split");
+    double acc[4][2] = {};
     const int k1 = warp * KW;
-#pragma unroll 4
-    for (int k0 = k1; k0 < k1 + KW; k0 += 4)
-      dmma_8x8x4(acc, sV[g * S8 + k0 + t], sC[g * S8 + k0 + t]);
-    sm.redW[warp][g][2 * t] = acc[0];
-    sm.redW[warp][g][2 * t + 1] = acc[1];
+#pragma unroll
+    for (int k0 = k1; k0 < k1 + KW; k0 += 16)
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        dmma_8x8x4(acc[q], sV[g * S8 + k0 + 4 * q + t], sC[g * S8 + k0 + 4 * q + t]);
+    sm.redW[warp][g][2 * t] = (acc[0][0] + acc[1][0]) + (acc[2][0] + acc[3][0]);
+    sm.redW[warp][g][2 * t + 1] = (acc[0][1] + acc[1][1]) + (acc[2][1] + acc[3][1]);
   }
   __syncthreads();
   if (tid < 64) {
@@ -659,7 +664,7 @@ BSOFI_DEVINL void apply_qt_mma8(double* sV, double* sC, const double (&a)[R][8],
     sm.redW[0][ai][cc] = -s2;
   }
   __syncthreads();
-#pragma unroll 1
+#pragma unroll 4
   for (int m0 = warp * KW; m0 < (warp + 1) * KW; m0 += 8) {
     double d[2] = {sC[(2 * t) * S8 + m0 + g], sC[(2 * t + 1) * S8 + m0 + g]};
 #pragma unroll

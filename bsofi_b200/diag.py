@@ -71,6 +71,19 @@ def bsof_timeline(n, L, reps=3):
             "update_publish_us": (has[:, 2] - has[:, 3]).mean() / 1e3,
             "to_next_leaf_us": (t[1:, 0] - t[:-1, 2]).mean() / 1e3,
         }
+        wait = (t[:, 1] - t[:, 0]) / 1e3
+        nl = (n + (16 if n <= 256 else 8) - 1) // (16 if n <= 256 else 8)
+        first = np.arange(S) % nl == 0  # the first leaf of each regular panel
+        first[(L - 2) * nl:] = False
+        out.update({
+            "wait_total_ms": wait.sum() / 1e3,
+            "wait_first_leaf_ms": wait[first].sum() / 1e3,
+            "wait_p50_us": float(np.percentile(wait, 50)),
+            "wait_p90_us": float(np.percentile(wait, 90)),
+            "wait_max_us": float(wait.max()),
+            "factor_total_ms": (has[:, 3] - has[:, 1]).sum() / 1e6,
+            "update_total_ms": (has[:, 2] - has[:, 3]).sum() / 1e6,
+        })
     return out
 
 
@@ -336,6 +349,11 @@ def main(argv):
         if a.startswith("--chains="):
             _lib.load().bsofi_device_set_batch_chains(int(a.split("=", 1)[1]))
             argv = [x for x in argv if x != a]
+    # --workers=W: BSOF worker CTAs of single inversions (the plan's otherwise).
+    for a in list(argv):
+        if a.startswith("--workers="):
+            _lib.load().bsofi_device_set_bsof_workers(int(a.split("=", 1)[1]))
+            argv = [x for x in argv if x != a]
     # --factor-warps=8: 16-wide BSOF leaves factored by all eight warps.
     for a in list(argv):
         if a.startswith("--factor-warps="):
@@ -350,6 +368,10 @@ def main(argv):
         print("per leaf: wait for tile %.2f us, factor (tile ready -> next-tile update) %.2f us, "
               "next-tile update + publish %.2f us, publish -> next leaf %.2f us" %
               (r["wait_tile_us"], r["factor_us"], r["update_publish_us"], r["to_next_leaf_us"]))
+        print("totals: wait %.2f ms (first leaf of a panel %.2f ms; per leaf p50 %.2f us, p90 %.2f us,"
+              " max %.1f us), factor %.2f ms, next-tile update + publish %.2f ms" %
+              (r["wait_total_ms"], r["wait_first_leaf_ms"], r["wait_p50_us"], r["wait_p90_us"],
+               r["wait_max_us"], r["factor_total_ms"], r["update_total_ms"]))
         return 0
     if len(argv) >= 3 and argv[0] == "invert":
         n, L = int(argv[1]), int(argv[2])
