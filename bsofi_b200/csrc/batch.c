@@ -119,6 +119,18 @@ void bsofi_device_set_batch_chains(int k) {
 static int g_pipelined = 1;
 void bsofi_device_set_batch_pipelined(int on) { g_pipelined = on ? 1 : 0; }
 
+/* BSOF worker CTAs per instance of a batch (0: by block size).  Measured on
+ * pipelined batches: 16 x (n = 256, p = 32) ran 134 inversions/s with 6
+ * workers and 142 with 12; the 256 instances of mixed sizes (n = 64..256)
+ * ran 268.5/s with 6 for all, 253/s with 12 for all, 251/s with 3.  So the
+ * largest 16-wide instances take 12, smaller ones 6, 8-wide ones 24. */
+static int g_batch_workers = 0;
+void bsofi_device_set_batch_workers(int w) { g_batch_workers = w < 0 ? 0 : w; }
+static int batch_workers(int n) {
+  if (g_batch_workers > 0) return g_batch_workers;
+  return n > 256 ? 24 : (n >= 224 ? 12 : 6);
+}
+
 unsigned long long bsofi_batch_workspace_bytes_ex(int count, const int *n, const int *L,
                                                   const int *ldda, int precision) {
   unsigned long long tot = 0;
@@ -177,7 +189,7 @@ static int grouped_fp64(stream_pool *p, int used, int count, const int *n, const
   }
   for (i = 0; i < count && !r; i++) {
     const int k = ord[i].i;
-    const int workers = n[k] <= 256 ? 6 : 24;
+    const int workers = batch_workers(n[k]);
     r = bsofi_dev_bsoftri_q_ex(n[k], L[k], dA[k], ldda[k], dtau[k], ws[k], p->s[i % used],
                                workers);
     *launches += bsofi_dev_launch_count();
@@ -264,7 +276,7 @@ int bsofi_device_invert_batched_ex(int count, const int *n, const int *L, double
     bsofi_dev_set_nonpersistent(1);
     for (i = 0; i < count && !r; i++) {
       const int k = ord[i].i, slot = i % used;
-      const int workers = n[k] <= 256 ? 6 : 24;
+      const int workers = batch_workers(n[k]);
       r = bsofi_dev_invert_two_streams(n[k], L[k], dA[k], ldda[k], dtau[k],
                                        (char *)dwork + off[k], p->hi[slot], p->s[slot],
                                        p->gate[slot], workers,
@@ -280,7 +292,7 @@ int bsofi_device_invert_batched_ex(int count, const int *n, const int *L, double
   for (i = 0; i < count && !(precision == 0 && g_grouped) && !g_pipelined; i++) {
     const int k = ord[i].i;
     /* Few BSOF workers per instance: the batch supplies the parallelism. */
-    const int workers = n[k] <= 256 ? 6 : 24;
+    const int workers = batch_workers(n[k]);
     /* Gate: instance i waits for the chain of instance i - K (ring slot
      * i % K, recorded by that instance after its BSOF) and records the slot
      * after its own; the host issues them in that order. */

@@ -344,6 +344,11 @@ def main(argv):
         if a.startswith("--k16="):
             _lib.load().bsofi_device_set_gemm_k16(int(a.split("=", 1)[1]))
             argv = [x for x in argv if x != a]
+    # --batch-workers=W: BSOF worker CTAs per batch instance.
+    for a in list(argv):
+        if a.startswith("--batch-workers="):
+            _lib.load().bsofi_device_set_batch_workers(int(a.split("=", 1)[1]))
+            argv = [x for x in argv if x != a]
     # --chains=K: at most K factorization chains of a batch in flight.
     for a in list(argv):
         if a.startswith("--chains="):

@@ -323,6 +323,9 @@ void bsofi_device_set_batch_chains(int k);
  * not start).  on = 0: each instance's whole pipeline on one stream.  The two
  * agree to the launch plans' rounding (tau bitwise). */
 void bsofi_device_set_batch_pipelined(int on);
+/* BSOF worker CTAs per batch instance (diagnostics; 0, the default: 6 for
+ * n < 224, 12 for 224 <= n <= 256, 24 above); process-wide. */
+void bsofi_device_set_batch_workers(int workers);
 /* The same batch at a chosen precision: 0 FP64 (as above), 1 mixed (every
  * instance as bsofi_device_invert_mixed with BSOFI_MIXED_SLICES slices).  The
  * workspace query returns 0 for an unknown precision. */
