@@ -131,6 +131,10 @@ static int batch_workers(int n) {
   return n > 256 ? 24 : (n >= 224 ? 12 : 6);
 }
 
+/* The same settings for the server's requests (server.c). */
+int bsofi_batch_pipelined_now(void) { return g_pipelined; }
+int bsofi_batch_workers_for(int n) { return batch_workers(n); }
+
 unsigned long long bsofi_batch_workspace_bytes_ex(int count, const int *n, const int *L,
                                                   const int *ldda, int precision) {
   unsigned long long tot = 0;

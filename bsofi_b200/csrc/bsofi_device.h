@@ -110,6 +110,10 @@ int bsofi_dev_invert_two_streams(int n, int L, double *dA, int ldd, double *dtau
 /* Launch plans of the calling thread without persistent GEMM kernels (BSOI
  * and the BSTRI recurrence as per-step launches) while on != 0. */
 void bsofi_dev_set_nonpersistent(int on);
+/* batch.c: whether batches (and the server's requests) run pipelined, and
+ * the BSOF worker count of an instance of block size n. */
+int bsofi_batch_pipelined_now(void);
+int bsofi_batch_workers_for(int n);
 /* FP64 tile engine steps: mma.sync m16n8k8 (0) or m16n8k16 (1). */
 void bsofi_dev_set_gemm_k16(int on);
 

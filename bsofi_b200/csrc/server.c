@@ -58,6 +58,8 @@ typedef struct {
   size_t moff, mlen;       /* server-owned matrix + tau in the pool (mlen 0: none) */
   int ldda, n, L;
   cudaStream_t stream;
+  cudaStream_t hi;       /* highest priority: the request's factorization chain */
+  cudaEvent_t handoff;   /* chain done on hi -> BSTRI and BSOI on stream */
   cudaEvent_t done;
   int *hinfo; /* pinned: BSTRI info word, BSOF / BSOI / BSTRI wait error words */
 } slot;
@@ -164,7 +166,7 @@ static void queue_remove(bsofi_server *sv, int pos) {
 /* ------------------------------------------------------------ API */
 bsofi_server *bsofi_server_create(int slots, unsigned long long pool_bytes) {
   bsofi_server *sv;
-  int i;
+  int i, least = 0, greatest = 0;
   if (slots < 1 || slots > MAX_SLOTS || pool_bytes < 4096) return NULL;
   if (bsofi_dev_prepare() != 0) return NULL;
   sv = (bsofi_server *)calloc(1, sizeof(bsofi_server));
@@ -179,8 +181,13 @@ bsofi_server *bsofi_server_create(int slots, unsigned long long pool_bytes) {
   sv->free_list[0].off = 0;
   sv->free_list[0].len = sv->pool_bytes;
   sv->nfree = 1;
+  if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess) goto fail;
   for (i = 0; i < slots; i++) {
     if (cudaStreamCreateWithFlags(&sv->s[i].stream, cudaStreamNonBlocking) != cudaSuccess) goto fail;
+    if (cudaStreamCreateWithPriority(&sv->s[i].hi, cudaStreamNonBlocking, greatest) != cudaSuccess)
+      goto fail;
+    if (cudaEventCreateWithFlags(&sv->s[i].handoff, cudaEventDisableTiming) != cudaSuccess)
+      goto fail;
     if (cudaEventCreateWithFlags(&sv->s[i].done, cudaEventDisableTiming) != cudaSuccess) goto fail;
     if (cudaMallocHost((void **)&sv->s[i].hinfo, 4 * sizeof(int)) != cudaSuccess) goto fail;
   }
@@ -198,6 +205,11 @@ void bsofi_server_destroy(bsofi_server *sv) {
       cudaStreamSynchronize(sv->s[i].stream);
       cudaStreamDestroy(sv->s[i].stream);
     }
+    if (sv->s[i].hi) {
+      cudaStreamSynchronize(sv->s[i].hi);
+      cudaStreamDestroy(sv->s[i].hi);
+    }
+    if (sv->s[i].handoff) cudaEventDestroy(sv->s[i].handoff);
     if (sv->s[i].done) cudaEventDestroy(sv->s[i].done);
     if (sv->s[i].hinfo) cudaFreeHost(sv->s[i].hinfo);
   }
@@ -301,18 +313,31 @@ int bsofi_server_release(bsofi_server *sv, long long id) {
   return 0;
 }
 
+/* A request runs pipelined like a batch instance (bsofi_device_set_batch_
+ * pipelined): the assembly and the factorization chain on the slot's
+ * highest-priority stream, then BSTRI and BSOI as per-step launches on its
+ * ordinary stream, so the other slots' chains are never held back by a
+ * persistent GEMM kernel; otherwise the whole pipeline on the ordinary one. */
 static int launch(bsofi_server *sv, slot *sl, const request *r) {
-  int e = 0, workers = r->n <= 256 ? 6 : 24;
+  const int pipelined = bsofi_batch_pipelined_now();
+  int e = 0, workers = bsofi_batch_workers_for(r->n);
   void *ws = sv->pool + sl->off;
   double *dA = r->dA, *dtau = r->dtau;
+  cudaStream_t first = pipelined ? sl->hi : sl->stream;
   if (r->owned) {
     dA = (double *)(sv->pool + sl->moff);
     dtau = (double *)(sv->pool + sl->moff +
                       align256(sizeof(double) * (size_t)r->ldda * r->n * r->L));
-    e = bsofi_device_assemble(r->n, r->L, r->dD, r->dS, dA, r->ldda, sl->stream);
+    e = bsofi_device_assemble(r->n, r->L, r->dD, r->dS, dA, r->ldda, first);
     if (e) return e <= BSOFI_INFO_CUDA ? BSOFI_INFO_CUDA - e : (int)cudaErrorInvalidValue;
   }
-  if (r->precision == 1)
+  if (pipelined) {
+    bsofi_dev_set_nonpersistent(1);
+    e = bsofi_dev_invert_two_streams(r->n, r->L, dA, r->ldda, dtau, ws, sl->hi, sl->stream,
+                                     sl->handoff, workers,
+                                     r->precision == 1 ? BSOFI_MIXED_SLICES : 0);
+    bsofi_dev_set_nonpersistent(0);
+  } else if (r->precision == 1)
     e = bsofi_dev_invert_mixed(r->n, r->L, dA, r->ldda, dtau, ws, sl->stream, workers,
                                BSOFI_MIXED_SLICES);
   else

@@ -314,8 +314,8 @@ void bsofi_device_set_batch_grouped(int on);
  * reference counterpart.  Results are unchanged.  (Measured: every bound
  * slowed the batch; the chains' latency, not their SMs, limits it.) */
 void bsofi_device_set_batch_chains(int k);
-/* Pipelined batches (on = 1, the default; process-wide, no reference
- * counterpart): each instance's factorization chain runs on a
+/* Pipelined batches and server requests (on = 1, the default; process-wide,
+ * no reference counterpart): each instance's factorization chain runs on a
  * highest-priority stream of the pool, the chains dealt to one stream back
  * to back, and hands over by an event to an ordinary stream for BSTRI and
  * BSOI, which then run as per-step launches instead of persistent kernels (a
