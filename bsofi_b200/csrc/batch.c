@@ -90,6 +90,10 @@ static size_t inst_ws(int n, int L, int ldda, int precision) {
                         : bsofi_dev_ws_bytes(n, L, ldda);
 }
 
+/* Process-wide switches, set and read from any thread. */
+static void flag_set(int *f, int v) { __atomic_store_n(f, v, __ATOMIC_RELAXED); }
+static int flag_get(int *f) { return __atomic_load_n(f, __ATOMIC_RELAXED); }
+
 /* FP64 batches run each instance's BSOI as its own launch (0, the default:
  * it overlaps the other instances' latency-bound factorization chains) or all
  * BSOI as one grouped persistent launch per tile shape after every
@@ -97,7 +101,7 @@ static size_t inst_ws(int n, int L, int ldda, int precision) {
  * chains; measured slower on a 256-instance batch of mixed sizes, 227.8
  * against 248.5 inversions/s). */
 static int g_grouped = 0;
-void bsofi_device_set_batch_grouped(int on) { g_grouped = on ? 1 : 0; }
+void bsofi_device_set_batch_grouped(int on) { flag_set(&g_grouped, on ? 1 : 0); }
 
 /* At most this many instances' factorization chains run at once in
  * one-stream-per-instance batches (0, the default: as many as there are
@@ -105,7 +109,7 @@ void bsofi_device_set_batch_grouped(int on) { g_grouped = on ? 1 : 0; }
  * latency, not by the SMs their launches occupy); kept for diagnostics. */
 static int g_chains = 0;
 void bsofi_device_set_batch_chains(int k) {
-  g_chains = k < 0 ? 0 : (k > MAX_GATE ? MAX_GATE : k);
+  flag_set(&g_chains, k < 0 ? 0 : (k > MAX_GATE ? MAX_GATE : k));
 }
 
 /* Pipelined batches (1, the default): each instance's factorization chain
@@ -117,7 +121,7 @@ void bsofi_device_set_batch_chains(int k) {
  * 265.4 against 249.5 inversions/s (16 streams); 16 instances of one size
  * unchanged.  0: each instance's whole pipeline on one stream. */
 static int g_pipelined = 1;
-void bsofi_device_set_batch_pipelined(int on) { g_pipelined = on ? 1 : 0; }
+void bsofi_device_set_batch_pipelined(int on) { flag_set(&g_pipelined, on ? 1 : 0); }
 
 /* BSOF worker CTAs per instance of a batch (0: by block size).  Measured on
  * pipelined batches: 16 x (n = 256, p = 32) ran 134 inversions/s with 6
@@ -125,14 +129,15 @@ void bsofi_device_set_batch_pipelined(int on) { g_pipelined = on ? 1 : 0; }
  * ran 268.5/s with 6 for all, 253/s with 12 for all, 251/s with 3.  So the
  * largest 16-wide instances take 12, smaller ones 6, 8-wide ones 24. */
 static int g_batch_workers = 0;
-void bsofi_device_set_batch_workers(int w) { g_batch_workers = w < 0 ? 0 : w; }
+void bsofi_device_set_batch_workers(int w) { flag_set(&g_batch_workers, w < 0 ? 0 : w); }
 static int batch_workers(int n) {
-  if (g_batch_workers > 0) return g_batch_workers;
+  const int w = flag_get(&g_batch_workers);
+  if (w > 0) return w;
   return n > 256 ? 24 : (n >= 224 ? 12 : 6);
 }
 
 /* The same settings for the server's requests (server.c). */
-int bsofi_batch_pipelined_now(void) { return g_pipelined; }
+int bsofi_batch_pipelined_now(void) { return flag_get(&g_pipelined); }
 int bsofi_batch_workers_for(int n) { return batch_workers(n); }
 
 unsigned long long bsofi_batch_workspace_bytes_ex(int count, const int *n, const int *L,
@@ -233,7 +238,7 @@ int bsofi_device_invert_batched_ex(int count, const int *n, const int *L, double
   order_t *ord;
   size_t *off;
   cudaError_t e;
-  int i, used, r = 0;
+  int i, used, r = 0, grouped, pipelined, chains;
   long long launches = 0;
   if (count < 0 || (count > 0 && (!n || !L || !dA || !ldda || !dtau || !dwork))) return -1;
   if (precision != 0 && precision != 1) return -1;
@@ -242,6 +247,9 @@ int bsofi_device_invert_batched_ex(int count, const int *n, const int *L, double
         !dtau[i])
       return -1;
   if (count == 0) return 0;
+  grouped = flag_get(&g_grouped);
+  pipelined = flag_get(&g_pipelined);
+  chains = flag_get(&g_chains);
   if ((e = (cudaError_t)bsofi_dev_prepare()) != cudaSuccess) return BSOFI_INFO_CUDA - (int)e;
   if (streams < 1) streams = 8;
   if (streams > MAX_STREAMS) streams = MAX_STREAMS;
@@ -267,14 +275,14 @@ int bsofi_device_invert_batched_ex(int count, const int *n, const int *L, double
   if ((e = cudaEventRecord(p->ev[0], (cudaStream_t)stream)) != cudaSuccess) goto fail;
   for (i = 0; i < used; i++)
     if ((e = cudaStreamWaitEvent(p->s[i], p->ev[0], 0)) != cudaSuccess) goto fail;
-  if (precision == 0 && g_grouped) {
+  if (precision == 0 && grouped) {
     r = grouped_fp64(p, used, count, n, L, dA, ldda, dtau, dwork, ord, off, &launches);
     if (r) {
       e = (cudaError_t)r;
       goto fail;
     }
   }
-  if (g_pipelined && !(precision == 0 && g_grouped)) {
+  if (pipelined && !(precision == 0 && grouped)) {
     for (i = 0; i < used; i++)
       if ((e = cudaStreamWaitEvent(p->hi[i], p->ev[0], 0)) != cudaSuccess) goto fail;
     bsofi_dev_set_nonpersistent(1);
@@ -293,14 +301,14 @@ int bsofi_device_invert_batched_ex(int count, const int *n, const int *L, double
       goto fail;
     }
   }
-  for (i = 0; i < count && !(precision == 0 && g_grouped) && !g_pipelined; i++) {
+  for (i = 0; i < count && !(precision == 0 && grouped) && !pipelined; i++) {
     const int k = ord[i].i;
     /* Few BSOF workers per instance: the batch supplies the parallelism. */
     const int workers = batch_workers(n[k]);
     /* Gate: instance i waits for the chain of instance i - K (ring slot
      * i % K, recorded by that instance after its BSOF) and records the slot
      * after its own; the host issues them in that order. */
-    const int K = (g_chains > 0 && g_chains < used) ? g_chains : 0;
+    const int K = (chains > 0 && chains < used) ? chains : 0;
     if (K > 0)
       r = bsofi_dev_invert_gated(n[k], L[k], dA[k], ldda[k], dtau[k], (char *)dwork + off[k],
                                  p->s[i % used], workers, precision == 1 ? BSOFI_MIXED_SLICES : 0,
@@ -323,7 +331,7 @@ int bsofi_device_invert_batched_ex(int count, const int *n, const int *L, double
     /* The chain streams too (their last work is already ordered before the
      * ordinary streams' by the hand-over events; joining them as well keeps
      * a stream capture of the batch complete). */
-    if (g_pipelined && !(precision == 0 && g_grouped)) {
+    if (pipelined && !(precision == 0 && grouped)) {
       if ((e = cudaEventRecord(p->gate[i], p->hi[i])) != cudaSuccess) goto fail;
       if ((e = cudaStreamWaitEvent((cudaStream_t)stream, p->gate[i], 0)) != cudaSuccess)
         goto fail;
