@@ -141,6 +141,7 @@ _SIGS = {
     "bsofi_device_set_batch_pipelined": (None, [ctypes.c_int]),
     "bsofi_device_set_batch_workers": (None, [ctypes.c_int]),
     "bsofi_device_set_gemm_k16": (None, [ctypes.c_int]),
+    "bsofi_device_set_bsoi_tma": (None, [ctypes.c_int]),
     "bsofi_device_set_wait_test": (None, [ctypes.c_int]),
     "bsofi_device_set_bstri_overlap": (None, [ctypes.c_int]),
     "bsofi_device_timing": (None, [ctypes.c_int]),

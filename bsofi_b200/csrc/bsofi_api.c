@@ -1179,4 +1179,6 @@ void bsofi_device_set_bsof_factor_warps(int warps) { bsofi_dev_set_bsof_factor_w
 
 void bsofi_device_set_gemm_k16(int on) { bsofi_dev_set_gemm_k16(on); }
 
+void bsofi_device_set_bsoi_tma(int on) { bsofi_dev_set_bsoi_tma(on); }
+
 void bsofi_device_set_wait_test(int on) { bsofi_dev_set_wait_test(on); }

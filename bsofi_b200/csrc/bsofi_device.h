@@ -116,6 +116,8 @@ int bsofi_batch_pipelined_now(void);
 int bsofi_batch_workers_for(int n);
 /* FP64 tile engine steps: mma.sync m16n8k8 (0) or m16n8k16 (1). */
 void bsofi_dev_set_gemm_k16(int on);
+/* Persistent BSOI with TMA-loaded clean 128 x 128 tiles (1) or cp.async (0). */
+void bsofi_dev_set_bsoi_tma(int on);
 
 /* Storage-sharded inversion (one inversion over several GPUs, none holding M
  * or M^{-1} whole).  The state (bsofi_dev_shard_state_bytes) holds the

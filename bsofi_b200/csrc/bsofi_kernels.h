@@ -51,6 +51,8 @@ cudaError_t launch_wy_apply(const WyArgs& a, int batch, cudaStream_t st);
 // it is A's block column L-1.
 int bsof_leaf_width(int n);
 void bsof_set_factor_warps(int w);
+// TMA loading of the persistent BSOI's clean 128 x 128 tiles; process-wide.
+void bsoi_set_tma(int on);
 int bsof_tiles(int n);
 cudaError_t launch_bsof_persistent(double* A, long long ld, int n, int L, double* tau, double* T,
                                    double* G, int maxleaves, int* cnt, int* factored,

@@ -165,6 +165,47 @@ BSOFI_DEVINL void load_b_tile(double* sB, const GemmB& b, const double* pb,
   }
 }
 
+// K tiles [kt0, kt1) of tile (m0, n0) outside which its K range is
+// structurally zero (as gemm_tile computes it).
+template <class Cfg>
+BSOFI_DEVINL void tile_k_tiles(const GemmDims& d, const GemmA& a, const GemmB& b, int m0, int n0,
+                               int& kt0, int& kt1) {
+  long long kbeg = 0, kend = d.K;
+  if (m0 >= a.rlim0 && a.ksplit < d.K) kbeg = a.ksplit;
+  else if (a.ksplit > 0) {
+    long long first = (long long)m0 - a.roff0;
+    if (first > 0) kbeg = min(first, (long long)a.ksplit);
+  }
+  {
+    long long last = (long long)n0 + Cfg::BN + b.koff;
+    if (last < kend) kend = last > 0 ? last : 0;
+  }
+  kt0 = (int)(kbeg / Cfg::BK);
+  kt1 = (int)((kend + Cfg::BK - 1) / Cfg::BK);
+}
+
+// True when every element the K tiles [kt0, kt1) of tile (m0, n0) read is
+// taken as stored: the tile lies inside M and N, the K tiles inside K, and no
+// row limit or triangular mask of A or B reaches into what they load.
+template <class Cfg>
+BSOFI_DEVINL bool tile_clean(const GemmDims& d, const GemmA& a, const GemmB& b, int m0, int n0,
+                             int kt0, int kt1) {
+  if (m0 + Cfg::BM > d.M || n0 + Cfg::BN > d.N) return false;
+  const long long k_lo = (long long)kt0 * Cfg::BK, k_hi = (long long)kt1 * Cfg::BK;
+  if (k_hi > d.K) return false;
+  const long long rmax = (long long)m0 + Cfg::BM - 1;
+  if (k_lo < a.ksplit) {  // element (r, k) is zero when r >= rlim or r - roff > k
+    if (rmax >= a.rlim0) return false;
+    if (rmax - a.roff0 > k_lo) return false;
+  }
+  if (k_hi > a.ksplit) {
+    const long long kl = (k_lo > a.ksplit ? k_lo : a.ksplit) - a.ksplit;
+    if (rmax >= a.rlim1) return false;
+    if (rmax - a.roff1 > kl) return false;
+  }
+  return k_hi - 1 - b.koff <= n0;  // B element (k, j) is zero when k - koff > j
+}
+
 // One CTA computes the BM x BN tile (m0, n0) of batch entry `bz`.
 template <class Cfg, bool ALIGNED>
 BSOFI_DEVINL void gemm_tile(const GemmDims& d, const GemmA& a, const GemmB& b,

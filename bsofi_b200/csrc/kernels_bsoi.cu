@@ -15,9 +15,13 @@
 // restricted to the row bands [rb0, rb1): each of its tiles is then the tile a
 // launch over all rows computes (rows of X are independent in BSOI), which is
 // how one inversion's BSOI is split across GPUs by rows.
+#include <cuda.h>
+#include <atomic>
 #include <climits>
+#include <mutex>
 #include "bsofi_common.cuh"
 #include "bsofi_kernels.h"
+#include "tcgen05.cuh"
 
 namespace bsofi {
 
@@ -110,6 +114,281 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) bsoi_persistent_kernel(BsoiAr
   }
 }
 
+// ------------------------------------------------------------------ TMA
+// The same persistent BSOI with its tiles' operands loaded by TMA: per
+// 32-deep K stage, warp 0's lane 0 issues 16 boxes of 16 rows x 16 k for A
+// (from the matrix's block column k, or the carry, per 16 k) and 2 boxes of
+// 16 k x 128 columns for B = Q_k^T, all with the 128-byte swizzle, into a
+// 3-stage ring of full / empty mbarriers; the compute warps read their DMMA
+// fragments through the swizzle and never compute copy addresses.  Tiles
+// that need a zero-fill mask (the rows of the diagonal block of X(:,k)) take
+// the cp.async path on the same shared memory.  The tensor maps cover this
+// GPU's memory only; no load uses cluster multicast.
+struct BsoiTmaMaps {
+  CUtensorMap x;         // the matrix: rows N (inner) x columns N; 16 x 16 boxes
+  CUtensorMap carry[2];  // rows N x n; 16 x 16 boxes
+  CUtensorMap g;         // G: 2n (k, inner) x 2n (columns) x (L-1); 16 x 128 x 1 boxes
+};
+
+struct BsoiTmaParams {
+  BsoiTmaMaps m;
+  BsoiArgs s;
+};
+
+struct TmaRing {
+  uint64_t full[3];
+  uint64_t empty[3];
+};
+
+// Abort word of the bounded waits for loads still in flight (never set).
+static __device__ int g_tma_no_abort = 0;
+
+constexpr int TMA_STAGES = 3, TMA_A_BYTES = 32768, TMA_STAGE_BYTES = 65536;
+
+// Bounded wait for a ring phase; the (global) error word is read only every
+// 256 polls, so a wait whose data is there costs one poll.
+BSOFI_DEVINL bool tma_ring_wait(uint64_t* bar, uint32_t parity, const int* err) {
+  for (long long i = 0; i < (1ll << 20); i++) {
+    if (tc::mbar_try_wait(bar, parity)) return true;
+    if ((i & 255) == 255 && *(volatile const int*)err) return false;
+  }
+  return false;
+}
+
+// Byte offset of element (e, r) in a 128-byte-row box with the 128-byte
+// swizzle: row r of 128 bytes, its 16-byte chunks permuted by r mod 8.
+BSOFI_DEVINL int swz(int r, int e) { return r * 128 + (((e >> 1) ^ (r & 7)) << 4) + (e & 1) * 8; }
+
+// Stage of K tile kt into ring slot `slot` (lane 0 of warp 0).
+BSOFI_DEVINL void tma_issue(const BsoiTmaMaps& M, int k, int n, int src, int m0, int n0, int kt,
+                            char* sa, uint64_t* full) {
+  tc::mbar_arrive_expect_tx(full, TMA_STAGE_BYTES);
+  char* sb = sa + TMA_A_BYTES;
+#pragma unroll
+  for (int bk = 0; bk < 2; bk++) {
+    const int kk0 = kt * 32 + bk * 16;
+#pragma unroll
+    for (int bm = 0; bm < 8; bm++) {
+      char* dst = sa + (bk * 8 + bm) * 2048;
+      if (kk0 < n) tc::tma_load_2d(dst, &M.x, full, m0 + 16 * bm, k * n + kk0);
+      else tc::tma_load_2d(dst, &M.carry[src], full, m0 + 16 * bm, kk0 - n);
+    }
+    tc::tma_load_3d(sb + bk * 16384, &M.g, full, kk0, n0, k);
+  }
+}
+
+// One clean tile through the TMA ring; false when a wait gave up (error word
+// set).  gstage: stages this CTA has run through the ring (uniform).
+BSOFI_DEVINL bool bsoi_tma_tile(const BsoiTmaMaps& M, const BsoiArgs& s, int k, int src,
+                                const GemmC& c, int m0, int n0, int kt0, int kt1, char* tb,
+                                TmaRing& ring, unsigned& gstage) {
+  using Cfg = CfgM;
+  const int nkt = kt1 - kt0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm = warp % Cfg::WARPS_M, wn = warp / Cfg::WARPS_M;
+  const int g = lane >> 2, t = lane & 3;
+  bool ok = true;
+  int issued = 0, consumed = 0;
+  if (warp == 0) {
+    for (int i = 0; i < TMA_STAGES && i < nkt && ok; i++) {
+      const unsigned gs = gstage + i, slot = gs % TMA_STAGES;
+      if (gs >= (unsigned)TMA_STAGES)
+        ok = tma_ring_wait(&ring.empty[slot], ((gs / TMA_STAGES) - 1) & 1, s.err);
+      if (ok) {
+        if (lane == 0)
+          tma_issue(M, k, s.n, src, m0, n0, kt0 + i, tb + slot * TMA_STAGE_BYTES, &ring.full[slot]);
+        issued++;
+      } else {
+        atomicExch(s.err, 1);
+      }
+    }
+  }
+  double acc[Cfg::MT][Cfg::NT][4];
+#pragma unroll
+  for (int i = 0; i < Cfg::MT; i++)
+#pragma unroll
+    for (int j = 0; j < Cfg::NT; j++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[i][j][q] = 0.0;
+  for (int it = 0; it < nkt && ok; it++) {
+    const unsigned gs = gstage + it, slot = gs % TMA_STAGES;
+    ok = tma_ring_wait(&ring.full[slot], (gs / TMA_STAGES) & 1, s.err);
+    if (!ok) {
+      atomicExch(s.err, 1);
+      break;
+    }
+    const char* sa = tb + slot * TMA_STAGE_BYTES;
+    const char* sb = sa + TMA_A_BYTES;
+#pragma unroll
+    for (int k8 = 0; k8 < 4; k8++) {
+      double af[Cfg::MT][4], bf[Cfg::NT][2];
+#pragma unroll
+      for (int i = 0; i < Cfg::MT; i++) {
+        const int bm = wm * 4 + i;
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+          const int kk = k8 * 8 + t + 4 * q, bk = kk >> 4, r = kk & 15;
+#pragma unroll
+          for (int h = 0; h < 2; h++)
+            af[i][2 * q + h] =
+                *reinterpret_cast<const double*>(sa + (bk * 8 + bm) * 2048 + swz(r, g + 8 * h));
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < Cfg::NT; j++) {
+        const int jr = wn * Cfg::WTN + j * 8 + g;
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+          const int kk = k8 * 8 + t + 4 * q;
+          bf[j][q] = *reinterpret_cast<const double*>(sb + (kk >> 4) * 16384 + swz(jr, kk & 15));
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < Cfg::MT; i++)
+#pragma unroll
+        for (int j = 0; j < Cfg::NT; j++)
+          dmma_16x8x8(acc[i][j], af[i][0], af[i][1], af[i][2], af[i][3], bf[j][0], bf[j][1]);
+    }
+    __syncwarp();
+    if (lane == 0) tc::mbar_arrive(&ring.empty[slot]);
+    consumed = it + 1;
+    if (warp == 0 && it + TMA_STAGES < nkt) {
+      // Refill this slot once every warp has consumed it.
+      ok = tma_ring_wait(&ring.empty[slot], (gs / TMA_STAGES) & 1, s.err);
+      if (ok) {
+        if (lane == 0)
+          tma_issue(M, k, s.n, src, m0, n0, kt0 + it + TMA_STAGES, tb + slot * TMA_STAGE_BYTES,
+                    &ring.full[slot]);
+        issued++;
+      } else {
+        atomicExch(s.err, 1);
+      }
+    }
+  }
+  if (!ok) {
+    // Before the CTA leaves, its loads still in flight land (bounded wait).
+    if (warp == 0)
+      for (int i = consumed; i < issued; i++) {
+        const unsigned gs = gstage + i;
+        tma_ring_wait(&ring.full[gs % TMA_STAGES], (gs / TMA_STAGES) & 1, &g_tma_no_abort);
+      }
+    gstage += nkt;
+    return false;
+  }
+  gstage += nkt;
+#pragma unroll
+  for (int i = 0; i < Cfg::MT; i++) {
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int r = m0 + wm * Cfg::WTM + i * 16 + g + h * 8;
+#pragma unroll
+      for (int j = 0; j < Cfg::NT; j++) {
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+          const int col = n0 + wn * Cfg::WTN + j * 8 + 2 * t + q;
+          const double v = acc[i][j][h * 2 + q];
+          if (col < c.nsplit) c.p0[cm(r, col, c.ld0)] = v;
+          else c.p1[cm(r, col - c.nsplit, c.ld1)] = v;
+        }
+      }
+    }
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(CfgM::THREADS, 1)
+    bsoi_tma_kernel(const __grid_constant__ BsoiTmaParams P) {
+  using Cfg = CfgM;
+  const BsoiArgs& s = P.s;
+  extern __shared__ __align__(16) double smem_bsoi[];
+  __shared__ int s_tile, s_ok;
+  __shared__ TmaRing ring;
+  // The 128-byte swizzle wants 1024-byte aligned boxes.
+  char* tb = reinterpret_cast<char*>(((uintptr_t)smem_bsoi + 1023) & ~(uintptr_t)1023);
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < TMA_STAGES; i++) {
+      tc::mbar_init(&ring.full[i], 1);
+      tc::mbar_init(&ring.empty[i], Cfg::THREADS / 32);
+    }
+    tc::fence_barrier_init();
+    tc::prefetch_tmap(&P.m.x);
+    tc::prefetch_tmap(&P.m.carry[0]);
+    tc::prefetch_tmap(&P.m.carry[1]);
+    tc::prefetch_tmap(&P.m.g);
+  }
+  unsigned gstage = 0;
+  const int n2 = 2 * s.n;
+  const int RT = (s.N + Cfg::BM - 1) / Cfg::BM, CT = (n2 + Cfg::BN - 1) / Cfg::BN;
+  const long long total = (long long)(s.L - 1) * RT * CT;
+  for (;;) {
+    __syncthreads();  // the previous tile's shared memory is no longer read
+    if (threadIdx.x == 0) s_tile = atomicAdd(s.next, 1);
+    __syncthreads();
+    const long long tile = s_tile;
+    if (tile >= total) return;
+    const int step = (int)(tile / ((long long)RT * CT));  // 0 = k = L-2
+    const int rem = (int)(tile % ((long long)RT * CT));
+    const int rb = rem / CT, cb = rem % CT;
+    const int k = s.L - 2 - step;
+    if (step > 0) {
+      if (threadIdx.x == 0) {
+        const int* flag = s.done + (long long)(step - 1) * RT + rb;
+        long long it = 0;
+        int ok = 1;
+        while (ld_acq(flag) < CT) {
+          if (ld_acq(s.err) != 0 || ++it > s.spin_limit) {
+            atomicExch(s.err, 1);
+            ok = 0;
+            break;
+          }
+          __nanosleep(64);
+        }
+        s_ok = ok;
+      }
+      __syncthreads();
+      if (!s_ok) return;
+    }
+    const int src = (s.L - 2 - k) & 1;
+    GemmDims d = {s.N, n2, n2};
+    GemmA a;
+    a.p0 = s.A + cm(0, (long long)k * s.n, s.ld);
+    a.ld0 = s.ld;
+    a.p1 = s.carry[src];
+    a.ld1 = s.ldc;
+    a.bs0 = a.bs1 = 0;
+    a.ksplit = s.n;
+    a.rlim0 = (k + 1) * s.n;
+    a.roff0 = k * s.n;
+    a.rlim1 = INT_MAX;
+    a.roff1 = kNoMask;
+    GemmB b = {s.G + (long long)k * n2 * n2, n2, 0, kNoMask};
+    GemmC c = {};
+    c.p0 = s.carry[(s.L - 1 - k) & 1];
+    c.ld0 = s.ldc;
+    c.p1 = s.A + cm(0, (long long)(k + 1) * s.n, s.ld);
+    c.ld1 = s.ld;
+    c.nsplit = s.n;
+    c.alpha = 1.0;
+    const int m0 = rb * Cfg::BM, n0 = cb * Cfg::BN;
+    int kt0, kt1;
+    tile_k_tiles<Cfg>(d, a, b, m0, n0, kt0, kt1);
+    if (kt1 > kt0 && tile_clean<Cfg>(d, a, b, m0, n0, kt0, kt1)) {
+      const bool ok = bsoi_tma_tile(P.m, s, k, src, c, m0, n0, kt0, kt1, tb, ring, gstage);
+      // Every warp reaches this barrier; a wait that gave up in any warp
+      // (error word set) ends the whole CTA.
+      if (__syncthreads_or(!ok)) return;
+    } else {
+      gemm_tile<Cfg, true>(d, a, b, c, m0, n0, 0, smem_bsoi);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(s.done + (long long)step * RT + rb)
+                   : "memory");
+    }
+  }
+}
+
 // Row bands of the smallest tile height (sizes the done counters for every
 // tile configuration).
 int bsoi_row_bands(int N) { return (N + CfgS::BM - 1) / CfgS::BM; }
@@ -146,6 +425,97 @@ static cudaError_t launch_al(const BsoiArgs& s, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// TMA loading of the persistent BSOI's clean tiles (1, the default) or
+// cp.async for every tile (0); process-wide.  Measured at n = 256, p = 32:
+// BSOI 3.473 against 3.582 ms (29.1 against 28.2 TFLOP/s), bitwise the same.
+static std::atomic<int> g_tma{1};
+void bsoi_set_tma(int on) { g_tma.store(on ? 1 : 0); }
+
+namespace {
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn tma_encoder() {
+  static std::once_flag once;
+  static EncodeTiledFn fn = nullptr;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+// FP64 tensor map of rank 2 or 3 (dims[0] contiguous), 128-byte swizzle.
+bool encode_f64(CUtensorMap* m, const double* base, int rank, const cuuint64_t* dims,
+                const cuuint64_t* strides_bytes, const cuuint32_t* box) {
+  EncodeTiledFn f = tma_encoder();
+  if (!f) return false;
+  const cuuint32_t es[3] = {1, 1, 1};
+  return f(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, rank, const_cast<double*>(base), dims, strides_bytes,
+           box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The TMA launch for a full-range 128 x 128 BSOI; false when it does not
+// apply (the caller then launches the cp.async kernel).
+bool launch_tma(const BsoiArgs& s, cudaStream_t st, cudaError_t* err) {
+  const int n = s.n, L = s.L, N = s.N;
+  if (n % 16 != 0) return false;
+  BsoiTmaParams P;
+  P.s = s;
+  {
+    const cuuint64_t dims[2] = {(cuuint64_t)N, (cuuint64_t)N};
+    const cuuint64_t str[1] = {(cuuint64_t)s.ld * sizeof(double)};
+    const cuuint32_t box[2] = {16, 16};
+    if (!encode_f64(&P.m.x, s.A, 2, dims, str, box)) return false;
+  }
+  for (int i = 0; i < 2; i++) {
+    const cuuint64_t dims[2] = {(cuuint64_t)N, (cuuint64_t)n};
+    const cuuint64_t str[1] = {(cuuint64_t)s.ldc * sizeof(double)};
+    const cuuint32_t box[2] = {16, 16};
+    if (!encode_f64(&P.m.carry[i], s.carry[i], 2, dims, str, box)) return false;
+  }
+  {
+    const cuuint64_t n2 = 2ull * n;
+    const cuuint64_t dims[3] = {n2, n2, (cuuint64_t)(L - 1)};
+    const cuuint64_t str[2] = {n2 * sizeof(double), n2 * n2 * sizeof(double)};
+    const cuuint32_t box[3] = {16, 128, 1};
+    if (!encode_f64(&P.m.g, s.G, 3, dims, str, box)) return false;
+  }
+  const size_t smem = CfgM::SMEM + 1024;
+  static PerDevice once;
+  const int pend = once.pending();
+  if (pend >= 0) {
+    cudaError_t e = cudaFuncSetAttribute(bsoi_tma_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) {
+      *err = e;
+      return true;
+    }
+    once.mark(pend);
+  }
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bsoi_tma_kernel, CfgM::THREADS, smem);
+  const long long tiles = (long long)(L - 1) * ((N + CfgM::BM - 1) / CfgM::BM) *
+                          ((2 * n + CfgM::BN - 1) / CfgM::BN);
+  int grid = sms * (per > 0 ? per : 1);
+  if (tiles < grid) grid = (int)tiles;
+  bsoi_tma_kernel<<<grid, CfgM::THREADS, smem, st>>>(P);
+  *err = cudaGetLastError();
+  return true;
+}
+
+}  // namespace
+
 cudaError_t launch_bsoi_persistent(double* A, long long ld, double* carry0, double* carry1,
                                    long long ldc, const double* G, int n, int L, int* done,
                                    int* next, int* err, bool small, cudaStream_t st, int row0,
@@ -176,6 +546,10 @@ cudaError_t launch_bsoi_persistent(double* A, long long ld, double* carry0, doub
     return al ? launch_al<CfgM16, true>(s, st) : launch_al<CfgM16, false>(s, st);
   }
   if (small) return al ? launch_al<CfgS, true>(s, st) : launch_al<CfgS, false>(s, st);
+  if (al && g_tma.load() && never == nullptr && s.rb0 == 0 && s.rb1 == s.N) {
+    cudaError_t e = cudaSuccess;
+    if (launch_tma(s, st, &e)) return e;
+  }
   return al ? launch_al<CfgM, true>(s, st) : launch_al<CfgM, false>(s, st);
 }
 
@@ -312,6 +686,7 @@ cudaError_t preload_bsoi(size_t* local) {
   if ((e = preload_one(bsoi_persistent_kernel<CfgM, false>, local)) != cudaSuccess) return e;
   if ((e = preload_one(bsoi_persistent_kernel<CfgS, true>, local)) != cudaSuccess) return e;
   if ((e = preload_one(bsoi_persistent_kernel<CfgS, false>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(bsoi_tma_kernel, local)) != cudaSuccess) return e;
   if ((e = preload_one(bsoi_persistent_kernel<CfgM16, true>, local)) != cudaSuccess) return e;
   if ((e = preload_one(bsoi_persistent_kernel<CfgM16, false>, local)) != cudaSuccess) return e;
   if ((e = preload_one(bsoi_persistent_kernel<CfgS16, true>, local)) != cudaSuccess) return e;

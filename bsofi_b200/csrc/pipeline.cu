@@ -1109,6 +1109,8 @@ void bsofi_dev_set_nonpersistent(int on) { g_nonpersistent = on != 0; }
 
 void bsofi_dev_set_gemm_k16(int on) { gemm_set_k16(on); }
 
+void bsofi_dev_set_bsoi_tma(int on) { bsoi_set_tma(on); }
+
 int bsofi_dev_bsoftri_q_ex(int n, int L, double* dA, int ldd, double* dtau, void* dws,
                            void* stream, int workers) {
   g_launches = 0;

@@ -1,5 +1,5 @@
-// Blackwell (sm_100a) primitives for the integer tensor-core path: mbarriers,
-// TMA tile loads, and the tcgen05 tensor-memory instructions, as inline PTX.
+// Blackwell (sm_100a) primitives: mbarriers, TMA tile loads, and the tcgen05
+// tensor-memory instructions, as inline PTX.
 //
 // Every wait is bounded: a wait that gives up returns false and the caller
 // reports it through an error word instead of spinning on.
@@ -69,6 +69,17 @@ __device__ __forceinline__ void tma_load_3d(void* smem_dst, const void* tmap, ui
       "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
       " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(smem_dst)),
       "l"(tmap), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+      : "memory");
+}
+
+// 2-D tiled bulk tensor load global -> shared (no multicast), completion
+// counted in bytes on `bar`; x is the innermost coordinate.
+__device__ __forceinline__ void tma_load_2d(void* smem_dst, const void* tmap, uint64_t* bar,
+                                            int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(smem_dst)),
+      "l"(tmap), "r"(smem_u32(bar)), "r"(x), "r"(y)
       : "memory");
 }
 

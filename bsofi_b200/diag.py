@@ -339,6 +339,11 @@ def main(argv):
         if a.startswith("--pipelined="):
             _lib.load().bsofi_device_set_batch_pipelined(int(a.split("=", 1)[1]))
             argv = [x for x in argv if x != a]
+    # --tma=1|0: the persistent BSOI's clean tiles loaded by TMA, or cp.async.
+    for a in list(argv):
+        if a.startswith("--tma="):
+            _lib.load().bsofi_device_set_bsoi_tma(int(a.split("=", 1)[1]))
+            argv = [x for x in argv if x != a]
     # --k16=1: the FP64 tile engine with mma.sync m16n8k16 steps.
     for a in list(argv):
         if a.startswith("--k16="):
@@ -378,6 +383,16 @@ def main(argv):
               (r["wait_total_ms"], r["wait_first_leaf_ms"], r["wait_p50_us"], r["wait_p90_us"],
                r["wait_max_us"], r["factor_total_ms"], r["update_total_ms"]))
         return 0
+    # --bsoi-plan=P (invert): the size's BSOI launch form (0 persistent
+    # 128 x 128, 5 persistent 64 x 64, 1-4 one launch per step).
+    bsoi_plan = None
+    for a in list(argv):
+        if a.startswith("--bsoi-plan="):
+            bsoi_plan = int(a.split("=", 1)[1])
+            argv = [x for x in argv if x != a]
+    if bsoi_plan is not None and len(argv) >= 3:
+        n, L = int(argv[1]), int(argv[2])
+        api.plan_set(n, L, [bsoi_plan] + api.plan_get(n, L)[1][1:])
     if len(argv) >= 3 and argv[0] == "invert":
         n, L = int(argv[1]), int(argv[2])
         reps = int(argv[3]) if len(argv) > 3 else 3

@@ -494,6 +494,15 @@ void bsofi_device_set_bsof_factor_warps(int warps);
  * m16n8k16 (1: half the instructions, each 16 deep in K), for every GEMM
  * launch and persistent BSOI launch that follows. */
 void bsofi_device_set_gemm_k16(int on);
+/* Operand loading of the persistent 128 x 128 BSOI kernel (no reference
+ * counterpart; process-wide): on = 1, the default, loads every tile that
+ * needs no zero-fill mask by TMA (2-D and 3-D tensor maps of the matrix, the
+ * carries and Q_k^T, 16 x 16 and 16 x 128 boxes with the 128-byte swizzle, a
+ * 3-stage ring of mbarriers filled by one thread), the rest by cp.async;
+ * on = 0 loads every tile by cp.async.  Same products in the same order: the
+ * same results bit for bit.  Applies to full-range launches with even
+ * leading dimensions and n a multiple of 16. */
+void bsofi_device_set_bsoi_tma(int on);
 /* Diagnostics (no reference counterpart): with on = 1, the persistent BSOI
  * launches made by this thread wait, in every step after the first, on a
  * zeroed workspace word that nothing writes, under a short poll limit (about

@@ -88,3 +88,35 @@ def test_inversion_with_k16_steps(cuda_device, n, L):
             lib.bsofi_device_set_gemm_k16(0)
     assert rel_fro(out[0], out[1]) < inverse_tolerance(M, out[1])
     assert residual(M, out[0]) < 1e-13
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,L", [(256, 32), (256, 8), (128, 20), (64, 40), (320, 6), (192, 12)])
+def test_bsoi_tma_is_bitwise_the_same(cuda_device, n, L):
+    """The persistent BSOI with its clean tiles loaded by TMA (the default,
+    bsofi_device_set_bsoi_tma(1)) computes the same products in the same
+    order as with cp.async (0): the inverses are equal bit for bit
+    (persistent 128 x 128 plans, set explicitly)."""
+    import torch
+    from bsofi_b200.hubbard import random_pcyclic
+    from gpu_util import to_device_colmajor
+    lib = api.load()
+    N = n * L
+    M = random_pcyclic(n, L, seed=71 + n + L)
+    saved = api.plan_get(n, L)[1]
+    api.plan_set(n, L, [0] + list(saved[1:]))
+    out = []
+    try:
+        for tma in (1, 0):
+            lib.bsofi_device_set_bsoi_tma(tma)
+            dA = to_device_colmajor(torch, M, device=cuda_device)
+            dtau = torch.zeros(N, dtype=torch.float64, device=cuda_device)
+            ws = torch.zeros(api.workspace_bytes(n, L, N), dtype=torch.uint8, device=cuda_device)
+            assert api.device_invert(n, L, dA.data_ptr(), N, dtau.data_ptr(), ws.data_ptr()) == 0
+            torch.cuda.synchronize()
+            assert int(ws.view(torch.int32)[0].item()) >= 0x7f7f7f7f
+            out.append(dA)
+    finally:
+        lib.bsofi_device_set_bsoi_tma(1)
+        api.plan_set(n, L, list(saved))
+    assert torch.equal(out[0], out[1])
