@@ -363,9 +363,9 @@ def main():
 
     peak = measure_dgemm_peak(torch, dev)
     achieved = flops_bsoi(n, L) * args.steps / (gemm_ms * 1e-3) / 1e12 if gemm_ms > 0 else None
-    roofline = {"kernel": "bsoi_persistent_kernel (all p-1 BSOI steps in one ordinary "
-                          "persistent launch, FP64 DMMA m16n8k8); dominant by algorithmic work "
-                          "(79% of the flop model)",
+    roofline = {"kernel": "bsoi_tma_kernel (all p-1 BSOI steps in one ordinary persistent "
+                          "launch; clean 128x128 tiles loaded by TMA, FP64 DMMA m16n8k8); "
+                          "dominant by algorithmic work (79% of the flop model)",
                 "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if achieved else None,
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor)",

@@ -159,6 +159,18 @@ BSOFI_DEVINL bool tma_ring_wait(uint64_t* bar, uint32_t parity, const int* err) 
 // swizzle: row r of 128 bytes, its 16-byte chunks permuted by r mod 8.
 BSOFI_DEVINL int swz(int r, int e) { return r * 128 + (((e >> 1) ^ (r & 7)) << 4) + (e & 1) * 8; }
 
+// Fragment rows are relabelled so that every 64-bit A fragment read of a
+// half-warp meets 16 distinct 8-byte slots of a 128-byte row through the
+// swizzle: row g + 8h of a 16-row fragment is tile row frag_row(g, h) (lanes
+// 0-15 read rows {2a, 2a+1, 2a+8, 2a+9}).  This permutes output rows only:
+// every product and sum is the same, so the results are bitwise those of the
+// natural order.  Relabelling B's columns the same way (frag_col) removes
+// B's 2-way conflicts too, but measured slower together with the row map
+// (BSOI at n = 256, p = 32: 3.350 ms rows only, 3.411 columns only, 3.578
+// both, 3.467 neither), so B keeps the natural order.
+BSOFI_DEVINL int frag_row(int g, int h) { return (g & 1) + 8 * ((g >> 1) & 1) + 4 * (g >> 2) + 2 * h; }
+BSOFI_DEVINL int frag_col(int g) { return g; }
+
 // Stage of K tile kt into ring slot `slot` (lane 0 of warp 0).
 BSOFI_DEVINL void tma_issue(const BsoiTmaMaps& M, int k, int n, int src, int m0, int n0, int kt,
                             char* sa, uint64_t* full) {
@@ -230,13 +242,13 @@ BSOFI_DEVINL bool bsoi_tma_tile(const BsoiTmaMaps& M, const BsoiArgs& s, int k, 
           const int kk = k8 * 8 + t + 4 * q, bk = kk >> 4, r = kk & 15;
 #pragma unroll
           for (int h = 0; h < 2; h++)
-            af[i][2 * q + h] =
-                *reinterpret_cast<const double*>(sa + (bk * 8 + bm) * 2048 + swz(r, g + 8 * h));
+            af[i][2 * q + h] = *reinterpret_cast<const double*>(sa + (bk * 8 + bm) * 2048 +
+                                                                swz(r, frag_row(g, h)));
         }
       }
 #pragma unroll
       for (int j = 0; j < Cfg::NT; j++) {
-        const int jr = wn * Cfg::WTN + j * 8 + g;
+        const int jr = wn * Cfg::WTN + j * 8 + frag_col(g);
 #pragma unroll
         for (int q = 0; q < 2; q++) {
           const int kk = k8 * 8 + t + 4 * q;
@@ -280,12 +292,12 @@ BSOFI_DEVINL bool bsoi_tma_tile(const BsoiTmaMaps& M, const BsoiArgs& s, int k, 
   for (int i = 0; i < Cfg::MT; i++) {
 #pragma unroll
     for (int h = 0; h < 2; h++) {
-      const int r = m0 + wm * Cfg::WTM + i * 16 + g + h * 8;
+      const int r = m0 + wm * Cfg::WTM + i * 16 + frag_row(g, h);
 #pragma unroll
       for (int j = 0; j < Cfg::NT; j++) {
 #pragma unroll
         for (int q = 0; q < 2; q++) {
-          const int col = n0 + wn * Cfg::WTN + j * 8 + 2 * t + q;
+          const int col = n0 + wn * Cfg::WTN + j * 8 + frag_col(2 * t + q);
           const double v = acc[i][j][h * 2 + q];
           if (col < c.nsplit) c.p0[cm(r, col, c.ld0)] = v;
           else c.p1[cm(r, col - c.nsplit, c.ld1)] = v;
