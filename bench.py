@@ -210,7 +210,7 @@ def bsof_chain_ms(api, n, L, ldd, ws):
 
 def traffic_per_launch():
     """DRAM bytes per BSOI launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "bsoi_persistent_traffic.json")
+    path = os.path.join(ROOT, "profiles", "bsoi_tma_traffic.json")
     if os.path.exists(path):
         try:
             return json.load(open(path)).get("dram_bytes_per_launch")
