@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) bsoi_persistent_kernel(BsoiAr
 // The same persistent BSOI with its tiles' operands loaded by TMA: per
 // 32-deep K stage, warp 0's lane 0 issues 16 boxes of 16 rows x 16 k for A
 // (from the matrix's block column k, or the carry, per 16 k) and 2 boxes of
-// 16 k x 128 columns for B = Q_k^T, all with the 128-byte swizzle, into a
+// 16 k x BN columns for B = Q_k^T, all with the 128-byte swizzle, into a
 // 3-stage ring of full / empty mbarriers; the compute warps read their DMMA
 // fragments through the swizzle and never compute copy addresses.  Tiles
 // that need a zero-fill mask (the rows of the diagonal block of X(:,k)) take
@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) bsoi_persistent_kernel(BsoiAr
 struct BsoiTmaMaps {
   CUtensorMap x;         // the matrix: rows N (inner) x columns N; 16 x 16 boxes
   CUtensorMap carry[2];  // rows N x n; 16 x 16 boxes
-  CUtensorMap g;         // G: 2n (k, inner) x 2n (columns) x (L-1); 16 x 128 x 1 boxes
+  CUtensorMap g;         // G: 2n (k, inner) x 2n (columns) x (L-1); 16 x BN x 1 boxes
 };
 
 struct BsoiTmaParams {
@@ -143,7 +143,24 @@ struct TmaRing {
 // Abort word of the bounded waits for loads still in flight (never set).
 static __device__ int g_tma_no_abort = 0;
 
-constexpr int TMA_STAGES = 3, TMA_A_BYTES = 32768, TMA_STAGE_BYTES = 65536;
+constexpr int TMA_STAGES = 3, TMA_A_BYTES = 32768;
+
+// The tile of the TMA kernel: 128 rows x BN columns (BN = 128, or 160 when 2n
+// is a multiple of 160 but not of 128, e.g. n = 400), 8 warps of 64 x BN/4.
+template <int BN_>
+struct TmaTile {
+  static constexpr int BM = 128, BN = BN_, BK = 32;
+  static constexpr int WTN = BN / CfgM::WARPS_N, NT = WTN / 8;
+  // One 16-deep B box (16 k x BN columns) and one stage (A and two B boxes).
+  static constexpr int B_BOX_BYTES = 16 * BN * 8;
+  static constexpr int STAGE_BYTES = TMA_A_BYTES + 2 * B_BOX_BYTES;
+  // The ring, or the cp.async tile of the masked tiles if larger, and 1024
+  // bytes to align the swizzled boxes.
+  static constexpr size_t SMEM =
+      ((size_t)TMA_STAGES * STAGE_BYTES > CfgM::SMEM ? (size_t)TMA_STAGES * STAGE_BYTES
+                                                     : CfgM::SMEM) + 1024;
+  static_assert(WTN % 8 == 0 && B_BOX_BYTES % 1024 == 0, "TMA tile");
+};
 
 // Bounded wait for a ring phase; the (global) error word is read only every
 // 256 polls, so a wait whose data is there costs one poll.
@@ -171,10 +188,14 @@ BSOFI_DEVINL int swz(int r, int e) { return r * 128 + (((e >> 1) ^ (r & 7)) << 4
 BSOFI_DEVINL int frag_row(int g, int h) { return (g & 1) + 8 * ((g >> 1) & 1) + 4 * (g >> 2) + 2 * h; }
 BSOFI_DEVINL int frag_col(int g) { return g; }
 
-// Stage of K tile kt into ring slot `slot` (lane 0 of warp 0).
+// Stage of K tile kt into ring slot `slot` (lane 0 of warp 0).  below: the
+// tile's rows lie under the diagonal block of X(:,k), where X(:,k) is zero;
+// a stage that starts before the carry (n not a multiple of 32) then takes
+// those 16 k as the carry map's zero fill at column -16.
+template <int BN>
 BSOFI_DEVINL void tma_issue(const BsoiTmaMaps& M, int k, int n, int src, int m0, int n0, int kt,
-                            char* sa, uint64_t* full) {
-  tc::mbar_arrive_expect_tx(full, TMA_STAGE_BYTES);
+                            bool below, char* sa, uint64_t* full) {
+  tc::mbar_arrive_expect_tx(full, TmaTile<BN>::STAGE_BYTES);
   char* sb = sa + TMA_A_BYTES;
 #pragma unroll
   for (int bk = 0; bk < 2; bk++) {
@@ -182,20 +203,40 @@ BSOFI_DEVINL void tma_issue(const BsoiTmaMaps& M, int k, int n, int src, int m0,
 #pragma unroll
     for (int bm = 0; bm < 8; bm++) {
       char* dst = sa + (bk * 8 + bm) * 2048;
-      if (kk0 < n) tc::tma_load_2d(dst, &M.x, full, m0 + 16 * bm, k * n + kk0);
+      if (kk0 < n && !below) tc::tma_load_2d(dst, &M.x, full, m0 + 16 * bm, k * n + kk0);
       else tc::tma_load_2d(dst, &M.carry[src], full, m0 + 16 * bm, kk0 - n);
     }
-    tc::tma_load_3d(sb + bk * 16384, &M.g, full, kk0, n0, k);
+    tc::tma_load_3d(sb + bk * TmaTile<BN>::B_BOX_BYTES, &M.g, full, kk0, n0, k);
   }
+}
+
+// A tile the TMA ring loads: every element its K tiles read is taken as
+// stored (tile_clean), or its rows all lie at or below the diagonal block's
+// end, where segment 0 (X(:,k)) is zero and read as zero fill, and segment 1
+// (the carry) is taken as stored.
+template <class T>
+BSOFI_DEVINL bool tma_tile_ok(const GemmDims& d, const GemmA& a, const GemmB& b, int m0, int n0,
+                              int kt0, int kt1) {
+  if (kt1 <= kt0) return false;
+  if (tile_clean<T>(d, a, b, m0, n0, kt0, kt1)) return true;
+  if (m0 < a.rlim0) return false;
+  GemmA z = a;
+  z.rlim0 = INT_MAX;
+  z.roff0 = kNoMask;
+  return tile_clean<T>(d, z, b, m0, n0, kt0, kt1);
 }
 
 // One clean tile through the TMA ring; false when a wait gave up (error word
 // set).  gstage: stages this CTA has run through the ring (uniform).
+template <int BN>
 BSOFI_DEVINL bool bsoi_tma_tile(const BsoiTmaMaps& M, const BsoiArgs& s, int k, int src,
                                 const GemmC& c, int m0, int n0, int kt0, int kt1, char* tb,
                                 TmaRing& ring, unsigned& gstage) {
   using Cfg = CfgM;
+  using T = TmaTile<BN>;
+  constexpr int NT = T::NT, WTN = T::WTN, STAGE_BYTES = T::STAGE_BYTES;
   const int nkt = kt1 - kt0;
+  const bool below = m0 >= (k + 1) * s.n;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int wm = warp % Cfg::WARPS_M, wn = warp / Cfg::WARPS_M;
   const int g = lane >> 2, t = lane & 3;
@@ -208,18 +249,19 @@ BSOFI_DEVINL bool bsoi_tma_tile(const BsoiTmaMaps& M, const BsoiArgs& s, int k, 
         ok = tma_ring_wait(&ring.empty[slot], ((gs / TMA_STAGES) - 1) & 1, s.err);
       if (ok) {
         if (lane == 0)
-          tma_issue(M, k, s.n, src, m0, n0, kt0 + i, tb + slot * TMA_STAGE_BYTES, &ring.full[slot]);
+          tma_issue<BN>(M, k, s.n, src, m0, n0, kt0 + i, below, tb + slot * STAGE_BYTES,
+                        &ring.full[slot]);
         issued++;
       } else {
         atomicExch(s.err, 1);
       }
     }
   }
-  double acc[Cfg::MT][Cfg::NT][4];
+  double acc[Cfg::MT][NT][4];
 #pragma unroll
   for (int i = 0; i < Cfg::MT; i++)
 #pragma unroll
-    for (int j = 0; j < Cfg::NT; j++)
+    for (int j = 0; j < NT; j++)
 #pragma unroll
       for (int q = 0; q < 4; q++) acc[i][j][q] = 0.0;
   for (int it = 0; it < nkt && ok; it++) {
@@ -229,11 +271,11 @@ BSOFI_DEVINL bool bsoi_tma_tile(const BsoiTmaMaps& M, const BsoiArgs& s, int k, 
       atomicExch(s.err, 1);
       break;
     }
-    const char* sa = tb + slot * TMA_STAGE_BYTES;
+    const char* sa = tb + slot * STAGE_BYTES;
     const char* sb = sa + TMA_A_BYTES;
 #pragma unroll
     for (int k8 = 0; k8 < 4; k8++) {
-      double af[Cfg::MT][4], bf[Cfg::NT][2];
+      double af[Cfg::MT][4], bf[NT][2];
 #pragma unroll
       for (int i = 0; i < Cfg::MT; i++) {
         const int bm = wm * 4 + i;
@@ -247,18 +289,19 @@ BSOFI_DEVINL bool bsoi_tma_tile(const BsoiTmaMaps& M, const BsoiArgs& s, int k, 
         }
       }
 #pragma unroll
-      for (int j = 0; j < Cfg::NT; j++) {
-        const int jr = wn * Cfg::WTN + j * 8 + frag_col(g);
+      for (int j = 0; j < NT; j++) {
+        const int jr = wn * WTN + j * 8 + frag_col(g);
 #pragma unroll
         for (int q = 0; q < 2; q++) {
           const int kk = k8 * 8 + t + 4 * q;
-          bf[j][q] = *reinterpret_cast<const double*>(sb + (kk >> 4) * 16384 + swz(jr, kk & 15));
+          bf[j][q] = *reinterpret_cast<const double*>(sb + (kk >> 4) * T::B_BOX_BYTES +
+                                                      swz(jr, kk & 15));
         }
       }
 #pragma unroll
       for (int i = 0; i < Cfg::MT; i++)
 #pragma unroll
-        for (int j = 0; j < Cfg::NT; j++)
+        for (int j = 0; j < NT; j++)
           dmma_16x8x8(acc[i][j], af[i][0], af[i][1], af[i][2], af[i][3], bf[j][0], bf[j][1]);
     }
     __syncwarp();
@@ -269,7 +312,8 @@ BSOFI_DEVINL bool bsoi_tma_tile(const BsoiTmaMaps& M, const BsoiArgs& s, int k, 
       ok = tma_ring_wait(&ring.empty[slot], (gs / TMA_STAGES) & 1, s.err);
       if (ok) {
         if (lane == 0)
-          tma_issue(M, k, s.n, src, m0, n0, kt0 + it + TMA_STAGES, tb + slot * TMA_STAGE_BYTES,
+          tma_issue<BN>(M, k, s.n, src, m0, n0, kt0 + it + TMA_STAGES, below,
+                        tb + slot * STAGE_BYTES,
                     &ring.full[slot]);
         issued++;
       } else {
@@ -294,10 +338,10 @@ BSOFI_DEVINL bool bsoi_tma_tile(const BsoiTmaMaps& M, const BsoiArgs& s, int k, 
     for (int h = 0; h < 2; h++) {
       const int r = m0 + wm * Cfg::WTM + i * 16 + frag_row(g, h);
 #pragma unroll
-      for (int j = 0; j < Cfg::NT; j++) {
+      for (int j = 0; j < NT; j++) {
 #pragma unroll
         for (int q = 0; q < 2; q++) {
-          const int col = n0 + wn * Cfg::WTN + j * 8 + frag_col(2 * t + q);
+          const int col = n0 + wn * WTN + j * 8 + frag_col(2 * t + q);
           const double v = acc[i][j][h * 2 + q];
           if (col < c.nsplit) c.p0[cm(r, col, c.ld0)] = v;
           else c.p1[cm(r, col - c.nsplit, c.ld1)] = v;
@@ -308,9 +352,11 @@ BSOFI_DEVINL bool bsoi_tma_tile(const BsoiTmaMaps& M, const BsoiArgs& s, int k, 
   return true;
 }
 
+template <int BN>
 __global__ void __launch_bounds__(CfgM::THREADS, 1)
     bsoi_tma_kernel(const __grid_constant__ BsoiTmaParams P) {
   using Cfg = CfgM;
+  using T = TmaTile<BN>;
   const BsoiArgs& s = P.s;
   extern __shared__ __align__(16) double smem_bsoi[];
   __shared__ int s_tile, s_ok;
@@ -330,7 +376,7 @@ __global__ void __launch_bounds__(CfgM::THREADS, 1)
   }
   unsigned gstage = 0;
   const int n2 = 2 * s.n;
-  const int RT = (s.N + Cfg::BM - 1) / Cfg::BM, CT = (n2 + Cfg::BN - 1) / Cfg::BN;
+  const int RT = (s.N + T::BM - 1) / T::BM, CT = (n2 + BN - 1) / BN;
   const long long total = (long long)(s.L - 1) * RT * CT;
   for (;;) {
     __syncthreads();  // the previous tile's shared memory is no longer read
@@ -381,16 +427,26 @@ __global__ void __launch_bounds__(CfgM::THREADS, 1)
     c.ld1 = s.ld;
     c.nsplit = s.n;
     c.alpha = 1.0;
-    const int m0 = rb * Cfg::BM, n0 = cb * Cfg::BN;
+    const int m0 = rb * T::BM, n0 = cb * BN;
     int kt0, kt1;
-    tile_k_tiles<Cfg>(d, a, b, m0, n0, kt0, kt1);
-    if (kt1 > kt0 && tile_clean<Cfg>(d, a, b, m0, n0, kt0, kt1)) {
-      const bool ok = bsoi_tma_tile(P.m, s, k, src, c, m0, n0, kt0, kt1, tb, ring, gstage);
+    tile_k_tiles<T>(d, a, b, m0, n0, kt0, kt1);
+    if (tma_tile_ok<T>(d, a, b, m0, n0, kt0, kt1)) {
+      const bool ok = bsoi_tma_tile<BN>(P.m, s, k, src, c, m0, n0, kt0, kt1, tb, ring, gstage);
       // Every warp reaches this barrier; a wait that gave up in any warp
       // (error word set) ends the whole CTA.
       if (__syncthreads_or(!ok)) return;
     } else {
-      gemm_tile<Cfg, true>(d, a, b, c, m0, n0, 0, smem_bsoi);
+      // The cp.async engine in 128-column passes; the last pass's columns
+      // end at the tile's (its loads there are zero-filled, its stores
+      // skipped).
+      GemmDims dc = d;
+      dc.N = min(d.N, n0 + BN);
+      for (int c0 = 0; c0 < BN; c0 += Cfg::BN) {
+        if (c0 > 0) __syncthreads();  // the previous pass's shared memory is read
+        gemm_tile<Cfg, true>(dc, a, b, c, m0, n0 + c0, 0, smem_bsoi);
+      }
+      // The ring's next TMA writes land on bytes these passes wrote.
+      tc::fence_proxy_async_smem();
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -439,7 +495,7 @@ static cudaError_t launch_al(const BsoiArgs& s, cudaStream_t st) {
 
 // TMA loading of the persistent BSOI's clean tiles (1, the default) or
 // cp.async for every tile (0); process-wide.  Measured at n = 256, p = 32:
-// BSOI 3.473 against 3.582 ms (29.1 against 28.2 TFLOP/s), bitwise the same.
+// BSOI 3.350 against 3.574 ms (30.2 against 28.3 TFLOP/s), bitwise the same.
 static std::atomic<int> g_tma{1};
 void bsoi_set_tma(int on) { g_tma.store(on ? 1 : 0); }
 
@@ -475,11 +531,38 @@ bool encode_f64(CUtensorMap* m, const double* base, int rank, const cuuint64_t* 
            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// The TMA launch for a full-range 128 x 128 BSOI; false when it does not
-// apply (the caller then launches the cp.async kernel).
+template <int BN>
+cudaError_t launch_tma_bn(const BsoiTmaParams& P, int n, int L, int N, cudaStream_t st) {
+  const size_t smem = TmaTile<BN>::SMEM;
+  static PerDevice once;
+  const int pend = once.pending();
+  if (pend >= 0) {
+    cudaError_t e = cudaFuncSetAttribute(bsoi_tma_kernel<BN>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    once.mark(pend);
+  }
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bsoi_tma_kernel<BN>, CfgM::THREADS, smem);
+  const long long tiles = (long long)(L - 1) * ((N + 127) / 128) * ((2 * n + BN - 1) / BN);
+  int grid = sms * (per > 0 ? per : 1);
+  if (tiles < grid) grid = (int)tiles;
+  bsoi_tma_kernel<BN><<<grid, CfgM::THREADS, smem, st>>>(P);
+  return cudaGetLastError();
+}
+
+// The TMA launch for a full-range persistent BSOI; false when it does not
+// apply (the caller then launches the cp.async kernel): n a multiple of 16
+// (the 16-row boxes of A start on block boundaries) and 2n a multiple of 128
+// (128 x 128 tiles) or else of 160 (128 x 160 tiles: no ragged column tile
+// at n = 400, 2n = 800).
 bool launch_tma(const BsoiArgs& s, cudaStream_t st, cudaError_t* err) {
   const int n = s.n, L = s.L, N = s.N;
   if (n % 16 != 0) return false;
+  const int bn = (2 * n) % 128 == 0 ? 128 : ((2 * n) % 160 == 0 ? 160 : 0);
+  if (bn == 0) return false;
   BsoiTmaParams P;
   P.s = s;
   {
@@ -498,31 +581,10 @@ bool launch_tma(const BsoiArgs& s, cudaStream_t st, cudaError_t* err) {
     const cuuint64_t n2 = 2ull * n;
     const cuuint64_t dims[3] = {n2, n2, (cuuint64_t)(L - 1)};
     const cuuint64_t str[2] = {n2 * sizeof(double), n2 * n2 * sizeof(double)};
-    const cuuint32_t box[3] = {16, 128, 1};
+    const cuuint32_t box[3] = {16, (cuuint32_t)bn, 1};
     if (!encode_f64(&P.m.g, s.G, 3, dims, str, box)) return false;
   }
-  const size_t smem = CfgM::SMEM + 1024;
-  static PerDevice once;
-  const int pend = once.pending();
-  if (pend >= 0) {
-    cudaError_t e = cudaFuncSetAttribute(bsoi_tma_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) {
-      *err = e;
-      return true;
-    }
-    once.mark(pend);
-  }
-  int dev = 0, sms = 0, per = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bsoi_tma_kernel, CfgM::THREADS, smem);
-  const long long tiles = (long long)(L - 1) * ((N + CfgM::BM - 1) / CfgM::BM) *
-                          ((2 * n + CfgM::BN - 1) / CfgM::BN);
-  int grid = sms * (per > 0 ? per : 1);
-  if (tiles < grid) grid = (int)tiles;
-  bsoi_tma_kernel<<<grid, CfgM::THREADS, smem, st>>>(P);
-  *err = cudaGetLastError();
+  *err = bn == 128 ? launch_tma_bn<128>(P, n, L, N, st) : launch_tma_bn<160>(P, n, L, N, st);
   return true;
 }
 
@@ -698,7 +760,8 @@ cudaError_t preload_bsoi(size_t* local) {
   if ((e = preload_one(bsoi_persistent_kernel<CfgM, false>, local)) != cudaSuccess) return e;
   if ((e = preload_one(bsoi_persistent_kernel<CfgS, true>, local)) != cudaSuccess) return e;
   if ((e = preload_one(bsoi_persistent_kernel<CfgS, false>, local)) != cudaSuccess) return e;
-  if ((e = preload_one(bsoi_tma_kernel, local)) != cudaSuccess) return e;
+  if ((e = preload_one(bsoi_tma_kernel<128>, local)) != cudaSuccess) return e;
+  if ((e = preload_one(bsoi_tma_kernel<160>, local)) != cudaSuccess) return e;
   if ((e = preload_one(bsoi_persistent_kernel<CfgM16, true>, local)) != cudaSuccess) return e;
   if ((e = preload_one(bsoi_persistent_kernel<CfgM16, false>, local)) != cudaSuccess) return e;
   if ((e = preload_one(bsoi_persistent_kernel<CfgS16, true>, local)) != cudaSuccess) return e;

@@ -72,10 +72,16 @@ Plan default_plan(int n, int L) {
   // between 2048 and 20000 (256/32, 196/40, 100/64, 324/40); at 64/16 one
   // launch per group of 2 rows was best; at 400/64 no group size beat the
   // persistent one-row recurrence.
+  // When 2n is a multiple of 160 (and n of 16), the persistent launch runs
+  // 128 x 160 tiles loaded by TMA; its BSOI against the 64 x 64 plans: 50.5
+  // against 56.0 ms at 400/64, 53.7 against 57.5 ms at 560/40 (per step),
+  // 4.63 against 5.43 ms at 240/40 (persistent).
   const int N = n * L;
   const int tiles = ((N + 127) / 128) * ((2 * n + 127) / 128);
+  const int tiles160 = ((N + 127) / 128) * ((2 * n) / 160);
   int bsoi;
   if ((2 * n) % 128 == 0 && tiles >= 148) bsoi = 0;
+  else if ((2 * n) % 160 == 0 && n % 16 == 0 && tiles160 >= 148) bsoi = 0;
   else if (N >= 20000) bsoi = 2;
   else if (N >= 4000) bsoi = 5;
   else bsoi = 1;

@@ -91,12 +91,15 @@ def test_inversion_with_k16_steps(cuda_device, n, L):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n,L", [(256, 32), (256, 8), (128, 20), (64, 40), (320, 6), (192, 12)])
+@pytest.mark.parametrize("n,L", [(256, 32), (256, 8), (128, 20), (64, 40), (320, 6), (192, 12),
+                                 (80, 24), (240, 8), (400, 6)])
 def test_bsoi_tma_is_bitwise_the_same(cuda_device, n, L):
     """The persistent BSOI with its clean tiles loaded by TMA (the default,
     bsofi_device_set_bsoi_tma(1)) computes the same products in the same
     order as with cp.async (0): the inverses are equal bit for bit
-    (persistent 128 x 128 plans, set explicitly)."""
+    (persistent plans, set explicitly; 128 x 160 TMA tiles where 2n is a
+    multiple of 160 but not of 128: n = 80, 240, 400), with a residual at
+    the FP64 level."""
     import torch
     from bsofi_b200.hubbard import random_pcyclic
     from gpu_util import to_device_colmajor
@@ -120,3 +123,6 @@ def test_bsoi_tma_is_bitwise_the_same(cuda_device, n, L):
         lib.bsofi_device_set_bsoi_tma(1)
         api.plan_set(n, L, list(saved))
     assert torch.equal(out[0], out[1])
+    from conftest import residual
+    from gpu_util import from_device_colmajor
+    assert residual(M, from_device_colmajor(out[0], N)) < 1e-13

@@ -19,7 +19,12 @@ def test_default_plan_follows_the_tuned_sizes():
     assert api.plan_get(64, 16) == (False, [1, 2, 32, 2])
     # 2n = 392: 64x64 tiles, persistent for mid-size N, per step for N >= 20k.
     assert api.plan_get(196, 40) == (False, [5, 4, 32, 4])
-    assert api.plan_get(400, 64) == (False, [2, 4, 32, 0])
+    assert api.plan_get(324, 80) == (False, [2, 4, 32, 0])
+    # 2n a multiple of 160 (800 = 5 x 160, 480 = 3 x 160): persistent 128x160
+    # TMA tiles once a step has 148 tiles; below that the 64x64 plans.
+    assert api.plan_get(400, 64) == (False, [0, 4, 32, 0])
+    assert api.plan_get(240, 40) == (False, [0, 4, 32, 4])
+    assert api.plan_get(240, 8) == (False, [1, 2, 32, 2])
 
 
 def test_set_get_clear_roundtrip():
