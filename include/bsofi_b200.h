@@ -494,14 +494,17 @@ void bsofi_device_set_bsof_factor_warps(int warps);
  * m16n8k16 (1: half the instructions, each 16 deep in K), for every GEMM
  * launch and persistent BSOI launch that follows. */
 void bsofi_device_set_gemm_k16(int on);
-/* Operand loading of the persistent 128 x 128 BSOI kernel (no reference
- * counterpart; process-wide): on = 1, the default, loads every tile that
- * needs no zero-fill mask by TMA (2-D and 3-D tensor maps of the matrix, the
- * carries and Q_k^T, 16 x 16 and 16 x 128 boxes with the 128-byte swizzle, a
- * 3-stage ring of mbarriers filled by one thread), the rest by cp.async;
- * on = 0 loads every tile by cp.async.  Same products in the same order: the
- * same results bit for bit.  Applies to full-range launches with even
- * leading dimensions and n a multiple of 16. */
+/* Operand loading of the persistent 128-row BSOI kernel (no reference
+ * counterpart; process-wide): on = 1, the default, loads by TMA every tile
+ * that needs no zero-fill mask, and every tile under the diagonal block of
+ * X(:,k), whose zeros come from the tensor map's fill (2-D and 3-D tensor
+ * maps of the matrix, the carries and Q_k^T, 16 x 16 and 16 x BN boxes with
+ * the 128-byte swizzle, a 3-stage ring of mbarriers filled by one thread),
+ * the rest by cp.async; on = 0 loads every tile by cp.async in 128 x 128
+ * tiles.  Same products in the same order: the same results bit for bit.
+ * Applies to full-range launches with even leading dimensions, n a multiple
+ * of 16 and 2n a multiple of 128 (128 x 128 tiles) or of 160 (128 x 160
+ * tiles, which need TMA: with on = 0 such sizes run 128 x 128 tiles). */
 void bsofi_device_set_bsoi_tma(int on);
 /* Diagnostics (no reference counterpart): with on = 1, the persistent BSOI
  * launches made by this thread wait, in every step after the first, on a
