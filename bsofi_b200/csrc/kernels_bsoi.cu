@@ -313,8 +313,7 @@ BSOFI_DEVINL bool bsoi_tma_tile(const BsoiTmaMaps& M, const BsoiArgs& s, int k, 
       if (ok) {
         if (lane == 0)
           tma_issue<BN>(M, k, s.n, src, m0, n0, kt0 + it + TMA_STAGES, below,
-                        tb + slot * STAGE_BYTES,
-                    &ring.full[slot]);
+                        tb + slot * STAGE_BYTES, &ring.full[slot]);
         issued++;
       } else {
         atomicExch(s.err, 1);
